@@ -1,0 +1,158 @@
+/*
+ * mfcfd_b200 -- B200 (sm_100a) meshfree LSKUM 2-D Euler pseudo-time loop.
+ *
+ * C ABI.  Plain pointers and sizes; every function returns an int status
+ * (0 = MFCFD_OK, negative = error) and never exits, aborts or prints.
+ *
+ * This boundary replaces the reference's Fortran module procedures over
+ * module-global state (Nischay-Pro/mfcfd, src_mpi_primal):
+ *   meshfree_solver.F90:83     call q_lskum()          -> create/set_state/run
+ *   q_lskum.F90:16-79          the pseudo-time loop    -> mfcfd_run
+ *   fpi_solver.F90:13-83       one iteration           -> one step of mfcfd_run
+ *   compute_force_coeffs.F90:11-102  Cl, Cd, Cm, cp    -> mfcfd_forces
+ *   initial_conditions.F90:9-70      freestream/restart -> create / set_state
+ * The reference has no C ABI, plugin or operator registry; its Fortran host
+ * binds these entry points through ISO_C_BINDING (see the Fortran module
+ * shipped in fortran/mfcfd_b200.F90).
+ *
+ * Array conventions follow the Fortran arrays the reference keeps in
+ * `type(points) :: point` (src_mpi_primal/data_structure.F90:13-49):
+ *   prim(4,N)  -> double[N][4] (rho, u1, u2, pr per point, caller's order)
+ *   conn(N,20) -> int, column-major: slot r of point i at conn[(r-1)*ld_conn + i-1],
+ *                 values are 1-based point numbers.
+ * The library copies every input on create/set and writes only into
+ * caller-provided outputs; it keeps no host pointer past a call.  Points are
+ * renumbered internally; all inputs and outputs use the caller's order.
+ *
+ * Threading: one host thread per handle at a time; handles are independent.
+ */
+#ifndef MFCFD_B200_H
+#define MFCFD_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define MFCFD_OK             0
+#define MFCFD_ERR_ARG       -1  /* bad argument (null pointer, size, range)      */
+#define MFCFD_ERR_CUDA      -2  /* CUDA runtime error (see mfcfd_last_error)     */
+#define MFCFD_ERR_NONFINITE -3  /* residue became NaN; the loop stopped there     */
+#define MFCFD_ERR_TIMEOUT   -4  /* a bounded device wait gave up                  */
+#define MFCFD_ERR_OOM       -5  /* device allocation failed                       */
+#define MFCFD_ERR_GRID      -6  /* grid would give a singular least-squares system
+                                   (an empty split list) or bad connectivity     */
+#define MFCFD_ERR_NODEV     -7  /* no CUDA device / unsupported device            */
+#define MFCFD_ERR_STATE     -8  /* call not valid in the handle's current state   */
+
+/* precision of the pseudo-time loop */
+#define MFCFD_FP64        0
+#define MFCFD_FP32_MIXED  1
+
+/* point renumbering */
+#define MFCFD_ORDER_KIND  0   /* stable partition wall | outer | interior */
+#define MFCFD_ORDER_RCM   1   /* reverse Cuthill-McKee, then the partition */
+
+/* Grid as the reference reads it from point/point.h5 group /1 (or the legacy
+ * partGrid text file): src_mpi_primal/point_preprocessor.F90:353-371. */
+typedef struct mfcfd_grid {
+    int n;                      /* local points (single rank: max_points)  */
+    const double *x, *y;        /* coordinates                             */
+    const double *nx, *ny;      /* file normals (used for interior points
+                                   only when format == 2, quadtree)        */
+    const double *min_dist;     /* Venkatakrishnan length scale            */
+    const int *flag_1;          /* 0 wall, 1 interior, 2 outer             */
+    const int *flag_2;          /* shape number, 0 = not on a shape        */
+    const int *left, *right;    /* 1-based ring neighbours (boundary pts)  */
+    const int *nbhs;            /* stencil size, 0..20                     */
+    const int *conn;            /* Fortran conn(N,20), column-major, 1-based */
+    int ld_conn;                /* leading dimension of conn (>= n)        */
+    int shapes;                 /* number of shapes (-shapes)              */
+} mfcfd_grid;
+
+/* Case parameters: the reference's case.in keys (readcase.F90:12-125) plus
+ * Mach/aoa (parameter.F90:5-6; the CUDA tree reads them from input.nml). */
+typedef struct mfcfd_params {
+    double cfl;                 /* -cfl                                    */
+    double power;               /* -power: LSQ weights dist**power         */
+    double vl_const;            /* -vl_const: Venkatakrishnan constant     */
+    double mach;                /* freestream Mach number                  */
+    double aoa;                 /* angle of attack, degrees                */
+    int    rks;                 /* 4 (-tscheme ssprk43) or 1 (first)       */
+    double euler;               /* 1.0 (ssprk43) or 2.0 (first)            */
+    int    inner_iterations;    /* -inner_iterations                       */
+    int    interior_points_normal_flag; /* 0: (0,1), 1: (1,0)             */
+    int    format;              /* 1 legacy, 2 quadtree (-format_file)     */
+    int    restart;             /* 1: -restart_solution same (res_old given) */
+    double res_old;             /* residual norm of iteration 2 when restart */
+    int    precision;           /* MFCFD_FP64 or MFCFD_FP32_MIXED          */
+    int    ordering;            /* MFCFD_ORDER_KIND or MFCFD_ORDER_RCM     */
+} mfcfd_params;
+
+typedef struct mfcfd mfcfd_t;
+
+/* Sets the default parameters of the reference's readcase (cfl 0,
+ * power 0, vl_const 150, ssprk43, no inner iterations, legacy format) with
+ * Mach 0.63 and aoa 2 (parameter.F90:5-6). */
+int mfcfd_default_params(mfcfd_params *p);
+
+/* Builds a solver on the current CUDA device: normals (point_normals.F90),
+ * split connectivity (generate_connectivity.F90), renumbering, device
+ * arrays, and the freestream initial state (initial_conditions.F90:9-20). */
+int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **out);
+
+/* Frees every device and host resource of the handle.  NULL is a no-op. */
+int mfcfd_destroy(mfcfd_t *h);
+
+/* Loads prim(4,N) (restart_sol, initial_conditions.F90:44-70). */
+int mfcfd_set_state(mfcfd_t *h, const double *prim);
+
+/* Copies prim(4,N) out. */
+int mfcfd_get_state(mfcfd_t *h, double *prim);
+
+/* Runs iterations it_first .. it_first+n_iters-1 of the q_lskum loop
+ * (q_lskum.F90:59-73, fpi_solver.F90:13-83).  residue (n_iters entries, may
+ * be NULL) receives the reference's residue per iteration: 0 for it <= 2
+ * (no restart), else log10(res_new/res_old).  Like the reference, the loop
+ * stops after the first iteration whose residue is NaN; *n_done (may be
+ * NULL) is the number of iterations done and the return value is then
+ * MFCFD_ERR_NONFINITE. */
+int mfcfd_run(mfcfd_t *h, int it_first, int n_iters, double *residue, int *n_done);
+
+/* Cl, Cd, Cm per shape (`shapes` entries each, any may be NULL) and cp per
+ * shape point in grid order (flag_2 > 0, may be NULL) for the current state
+ * (compute_force_coeffs.F90:11-102). */
+int mfcfd_forces(mfcfd_t *h, double *cl, double *cd, double *cm, double *cp);
+
+/* Uses the given cudaStream_t (NULL = the handle's own stream). */
+int mfcfd_set_stream(mfcfd_t *h, void *stream);
+
+/* Copies an internal per-point array out in caller order, for stage-level
+ * checks: "q" (4/pt, the last stage's input), "dq" (8/pt: d/dx of q1..q4 then
+ * d/dy), "qm" (8/pt: max of q1..q4 then min), "delta" (1), "nx", "ny" (1),
+ * "flux_res" (4/pt, last stage; kept only when the handle was told to keep
+ * diagnostics by mfcfd_keep_diagnostics). */
+int mfcfd_get_array(mfcfd_t *h, const char *name, double *out);
+
+/* Whether the flux pass also stores flux_res for mfcfd_get_array (0/1). */
+int mfcfd_keep_diagnostics(mfcfd_t *h, int on);
+
+/* Number of points, and the number of split-list entries per point type. */
+int mfcfd_info(mfcfd_t *h, int *n, int *n_wall, int *n_outer, int *n_interior);
+
+/* Human-readable text of a status code (static storage). */
+const char *mfcfd_strerror(int status);
+
+/* The last error message recorded on the handle (static per handle; empty
+ * when none).  h may be NULL for errors of mfcfd_create. */
+const char *mfcfd_last_error(mfcfd_t *h);
+
+/* Device kernels launched by the handle since creation (all kinds). */
+long long mfcfd_launch_count(mfcfd_t *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MFCFD_B200_H */

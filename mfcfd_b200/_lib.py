@@ -1,0 +1,108 @@
+"""ctypes binding of the C ABI declared in include/mfcfd_b200.h.
+
+The product path has no fallback: if libmfcfd_b200.so is missing and cannot
+be built, or the CUDA device is absent, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import build as _build
+
+MFCFD_OK = 0
+MFCFD_ERR_ARG = -1
+MFCFD_ERR_CUDA = -2
+MFCFD_ERR_NONFINITE = -3
+MFCFD_ERR_TIMEOUT = -4
+MFCFD_ERR_OOM = -5
+MFCFD_ERR_GRID = -6
+MFCFD_ERR_NODEV = -7
+MFCFD_ERR_STATE = -8
+MFCFD_FP64 = 0
+MFCFD_FP32_MIXED = 1
+MFCFD_ORDER_KIND = 0
+MFCFD_ORDER_RCM = 1
+
+# every symbol include/mfcfd_b200.h declares
+EXPORTS = ("mfcfd_default_params", "mfcfd_create", "mfcfd_destroy", "mfcfd_set_state",
+           "mfcfd_get_state", "mfcfd_run", "mfcfd_forces", "mfcfd_set_stream",
+           "mfcfd_get_array", "mfcfd_keep_diagnostics", "mfcfd_info", "mfcfd_strerror",
+           "mfcfd_last_error", "mfcfd_launch_count")
+
+
+class Grid(C.Structure):
+    _fields_ = [("n", C.c_int), ("x", C.c_void_p), ("y", C.c_void_p), ("nx", C.c_void_p),
+                ("ny", C.c_void_p), ("min_dist", C.c_void_p), ("flag_1", C.c_void_p),
+                ("flag_2", C.c_void_p), ("left", C.c_void_p), ("right", C.c_void_p),
+                ("nbhs", C.c_void_p), ("conn", C.c_void_p), ("ld_conn", C.c_int),
+                ("shapes", C.c_int)]
+
+
+class Params(C.Structure):
+    _fields_ = [("cfl", C.c_double), ("power", C.c_double), ("vl_const", C.c_double),
+                ("mach", C.c_double), ("aoa", C.c_double), ("rks", C.c_int),
+                ("euler", C.c_double), ("inner_iterations", C.c_int),
+                ("interior_points_normal_flag", C.c_int), ("format", C.c_int),
+                ("restart", C.c_int), ("res_old", C.c_double), ("precision", C.c_int),
+                ("ordering", C.c_int)]
+
+
+_LIB = None
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = True) -> C.CDLL:
+    """Loads libmfcfd_b200.so (building it in-tree first if it is absent)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = _build.LIB
+    if not os.path.exists(path) or (build_if_missing and not _build.up_to_date()):
+        if not build_if_missing:
+            raise RuntimeError(f"{path} is missing")
+        _build.build()
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    D = C.POINTER(C.c_double)
+    I = C.POINTER(C.c_int)
+    lib.mfcfd_default_params.argtypes = [C.POINTER(Params)]
+    lib.mfcfd_create.argtypes = [C.POINTER(Grid), C.POINTER(Params), C.POINTER(P)]
+    lib.mfcfd_destroy.argtypes = [P]
+    lib.mfcfd_set_state.argtypes = [P, D]
+    lib.mfcfd_get_state.argtypes = [P, D]
+    lib.mfcfd_run.argtypes = [P, C.c_int, C.c_int, D, I]
+    lib.mfcfd_forces.argtypes = [P, D, D, D, D]
+    lib.mfcfd_set_stream.argtypes = [P, P]
+    lib.mfcfd_get_array.argtypes = [P, C.c_char_p, D]
+    lib.mfcfd_keep_diagnostics.argtypes = [P, C.c_int]
+    lib.mfcfd_info.argtypes = [P, I, I, I, I]
+    lib.mfcfd_strerror.argtypes = [C.c_int]
+    lib.mfcfd_strerror.restype = C.c_char_p
+    lib.mfcfd_last_error.argtypes = [P]
+    lib.mfcfd_last_error.restype = C.c_char_p
+    lib.mfcfd_launch_count.argtypes = [P]
+    lib.mfcfd_launch_count.restype = C.c_longlong
+    for name in EXPORTS:
+        if name not in ("mfcfd_strerror", "mfcfd_last_error", "mfcfd_launch_count"):
+            getattr(lib, name).restype = C.c_int
+    _LIB = lib
+    return lib
+
+
+class MfcfdError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+def check(status: int, handle=None, what: str = "") -> None:
+    if status == MFCFD_OK:
+        return
+    lib = load()
+    detail = lib.mfcfd_last_error(handle).decode(errors="replace")
+    text = lib.mfcfd_strerror(status).decode()
+    raise MfcfdError(status, f"{what}: {text}" + (f": {detail}" if detail else ""))

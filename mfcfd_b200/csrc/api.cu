@@ -1,0 +1,775 @@
+// C ABI of mfcfd_b200: handle, host-side set-up and the pseudo-time driver.
+//
+// Set-up restates the reference's once-per-run work on the host, in the
+// reference's arithmetic (this file is compiled without FMA contraction):
+//   point_normals.F90:8-105        wall/outer normals, interior (0,1)/(1,0)
+//   generate_connectivity.F90      xpos/xneg/ypos/yneg membership, kept as
+//                                  per-point bit masks over the stencil slots
+//   point_preprocessor.F90:374-435 wall/interior/outer/shape classification
+//   parameter.F90:16-34            theta and the freestream state
+// then renumbers the points (wall | outer | interior, optionally after RCM)
+// and uploads everything once.  mfcfd_run enqueues the iterations as CUDA
+// graphs (two iterations per graph, because the prim buffers alternate) with
+// no host synchronisation until the residue history is read back.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <deque>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "mfcfd_b200.h"
+#include "primal.h"
+
+using namespace lskum;
+
+namespace {
+
+constexpr int MAXNB = 20;
+thread_local std::string g_create_error;
+
+template <class T>
+cudaError_t dmalloc(T **p, size_t count) {
+    return cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T) + (count == 0 ? 16 : 0));
+}
+
+}  // namespace
+
+struct mfcfd {
+    int dev = 0;
+    int n = 0, kp = 1, nw = 0, no = 0, nint = 0, shapes = 1, nshape = 0;
+    mfcfd_params p{};
+    std::vector<int> perm;  // new index -> caller index
+    double pi = 0, theta = 0, cos_t = 0, sin_t = 0, q_inf[4] = {0, 0, 0, 0};
+
+    Geom geom{};
+    Consts consts{};
+    ShapeTab shape{};
+
+    // device buffers
+    double2 *d_xy = nullptr, *d_nrm = nullptr;
+    double *d_eps2 = nullptr, *d_obc = nullptr;
+    int *d_conn = nullptr, *d_nbhs = nullptr;
+    unsigned long long *d_mx = nullptr, *d_my = nullptr;
+    R4 *d_prim[2] = {nullptr, nullptr}, *d_q[2] = {nullptr, nullptr};
+    double *d_dq[2] = {nullptr, nullptr};
+    double *d_qm = nullptr, *d_delta = nullptr, *d_spd = nullptr, *d_res_part = nullptr;
+    double *d_flux_dbg = nullptr, *d_hist = nullptr, *d_forces = nullptr;
+    int hist_cap = 0;
+    Ctl *d_ctl = nullptr;
+    Ctl *h_ctl = nullptr;  // pinned
+    int *d_sh_idx = nullptr, *d_sh_shape = nullptr;
+    double *d_sh_geo = nullptr, *d_sh_my = nullptr;
+    double *h_stage = nullptr;  // pinned staging [n][4]
+
+    int cur = 0;   // prim buffer holding the state
+    int qcur = 0;  // q buffer holding q of the state
+    int iters_done_total = 0;
+    cudaStream_t own = nullptr, stream = nullptr;
+    cudaGraphExec_t pair_exec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [cur][qcur]
+    bool keep_diag = false;
+    long long launches = 0;
+    std::string err;
+    std::vector<double> shape_cp;
+};
+
+namespace {
+
+int fail(mfcfd_t *h, int code, const std::string &msg) {
+    if (h) h->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+int cuda_fail(mfcfd_t *h, cudaError_t e, const char *where) {
+    std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+    return fail(h, e == cudaErrorMemoryAllocation ? MFCFD_ERR_OOM : MFCFD_ERR_CUDA, m);
+}
+
+#define CK(call)                                                    \
+    do {                                                            \
+        cudaError_t e_ = (call);                                    \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, #call);      \
+    } while (0)
+
+void free_all(mfcfd_t *h) {
+    for (auto &row : h->pair_exec)
+        for (auto &g : row)
+            if (g) cudaGraphExecDestroy(g);
+    void *bufs[] = {h->d_xy, h->d_nrm, h->d_eps2, h->d_obc, h->d_conn, h->d_nbhs, h->d_mx,
+                    h->d_my, h->d_prim[0], h->d_prim[1], h->d_q[0], h->d_q[1], h->d_dq[0],
+                    h->d_dq[1], h->d_qm, h->d_delta, h->d_spd, h->d_res_part, h->d_flux_dbg,
+                    h->d_hist, h->d_forces, h->d_ctl, h->d_sh_idx, h->d_sh_shape, h->d_sh_geo,
+                    h->d_sh_my};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (h->h_ctl) cudaFreeHost(h->h_ctl);
+    if (h->h_stage) cudaFreeHost(h->h_stage);
+    if (h->own) cudaStreamDestroy(h->own);
+}
+
+// Reverse Cuthill-McKee over the symmetrised stencil graph.
+std::vector<int> rcm_order(int n, const std::vector<std::vector<int>> &adj) {
+    std::vector<int> order;
+    order.reserve(n);
+    std::vector<char> seen(n, 0);
+    std::vector<int> byDeg(n);
+    for (int i = 0; i < n; ++i) byDeg[i] = i;
+    std::stable_sort(byDeg.begin(), byDeg.end(),
+                     [&](int a, int b) { return adj[a].size() < adj[b].size(); });
+    for (int root : byDeg) {
+        if (seen[root]) continue;
+        std::deque<int> qq{root};
+        seen[root] = 1;
+        while (!qq.empty()) {
+            int v = qq.front();
+            qq.pop_front();
+            order.push_back(v);
+            std::vector<int> nb;
+            for (int w : adj[v])
+                if (!seen[w]) {
+                    seen[w] = 1;
+                    nb.push_back(w);
+                }
+            std::stable_sort(nb.begin(), nb.end(),
+                             [&](int a, int b) { return adj[a].size() < adj[b].size(); });
+            for (int w : nb) qq.push_back(w);
+        }
+    }
+    std::reverse(order.begin(), order.end());
+    return order;
+}
+
+int enqueue_iteration(mfcfd_t *h, cudaStream_t s) {
+    const int A = h->cur, B = h->cur ^ 1;
+    const int m = h->p.inner_iterations;
+    for (int rk = 1; rk <= h->p.rks; ++rk) {
+        const R4 *q_in = h->d_q[h->qcur];
+        R4 *q_out = h->d_q[h->qcur ^ 1];
+        launch_grad(h->geom, h->consts, q_in, h->d_spd, h->d_dq[0], h->d_qm, h->d_delta,
+                    rk == 1, h->d_ctl, s);
+        for (int t = 1; t <= m; ++t)
+            launch_inner(h->geom, h->consts, q_in, h->d_dq[(t - 1) & 1], h->d_dq[t & 1],
+                         h->d_ctl, s);
+        StageBufs b;
+        b.prim_in = rk == 1 ? h->d_prim[A] : h->d_prim[B];
+        b.prim_out = h->d_prim[B];
+        b.prim_old = h->d_prim[A];
+        b.q_in = q_in;
+        b.q_out = q_out;
+        b.dq = h->d_dq[m & 1];
+        b.qm = h->d_qm;
+        b.delta = h->d_delta;
+        b.spd = h->d_spd;
+        b.res_part = h->d_res_part;
+        b.flux_dbg = h->keep_diag ? h->d_flux_dbg : nullptr;
+        launch_flux(h->geom, h->consts, b, rk, rk == h->p.rks, h->d_ctl, s);
+        h->qcur ^= 1;
+        h->launches += 2 + m;
+    }
+    launch_residual(h->d_res_part, flux_blocks(h->n), h->d_ctl, h->d_hist, s);
+    h->launches += 1;
+    h->cur = B;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
+    return MFCFD_OK;
+}
+
+// Captures two consecutive iterations into one graph.  After two iterations
+// both the prim and the q buffer parity are back where they started.
+void drop_graphs(mfcfd_t *h) {
+    for (auto &row : h->pair_exec)
+        for (auto &g : row)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+}
+
+int build_pair_graph(mfcfd_t *h) {
+    int cur0 = h->cur, q0 = h->qcur;
+    cudaGraphExec_t &slot = h->pair_exec[cur0][q0];
+    if (slot) {
+        cudaGraphExecDestroy(slot);
+        slot = nullptr;
+    }
+    long long l0 = h->launches;
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(h->own, cudaStreamCaptureModeThreadLocal));
+    int st = enqueue_iteration(h, h->own);
+    if (st == MFCFD_OK) st = enqueue_iteration(h, h->own);
+    cudaError_t e = cudaStreamEndCapture(h->own, &graph);
+    h->cur = cur0;
+    h->qcur = q0;
+    h->launches = l0;
+    if (st != MFCFD_OK) return st;
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&slot, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
+    return MFCFD_OK;
+}
+
+int upload_state_aux(mfcfd_t *h) {
+    launch_init_state(h->geom, h->d_prim[h->cur], h->d_q[h->qcur], h->d_spd, h->stream);
+    h->launches += 1;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(h, e, "init_state launch");
+    return MFCFD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mfcfd_default_params(mfcfd_params *p) {
+    if (!p) return MFCFD_ERR_ARG;
+    memset(p, 0, sizeof(*p));
+    p->cfl = 0.0;
+    p->power = 0.0;
+    p->vl_const = 150.0;
+    p->mach = 0.63;
+    p->aoa = 2.0;
+    p->rks = 4;
+    p->euler = 1.0;
+    p->inner_iterations = 0;
+    p->interior_points_normal_flag = 0;
+    p->format = 1;
+    p->restart = 0;
+    p->res_old = 0.0;
+    p->precision = MFCFD_FP64;
+    p->ordering = MFCFD_ORDER_KIND;
+    return MFCFD_OK;
+}
+
+int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **out) {
+    mfcfd_t *h = nullptr;
+    if (!out) return fail(nullptr, MFCFD_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!grid || !params) return fail(nullptr, MFCFD_ERR_ARG, "grid or params is NULL");
+    const mfcfd_grid &G = *grid;
+    const int n = G.n;
+    if (n <= 0) return fail(nullptr, MFCFD_ERR_ARG, "grid.n must be positive");
+    if (!G.x || !G.y || !G.nx || !G.ny || !G.min_dist || !G.flag_1 || !G.flag_2 || !G.left ||
+        !G.right || !G.nbhs || !G.conn)
+        return fail(nullptr, MFCFD_ERR_ARG, "a grid array is NULL");
+    if (G.ld_conn < n) return fail(nullptr, MFCFD_ERR_ARG, "grid.ld_conn < grid.n");
+    if (G.shapes < 1) return fail(nullptr, MFCFD_ERR_ARG, "grid.shapes must be >= 1");
+    const mfcfd_params &P = *params;
+    if (!(P.rks == 1 || P.rks == 4))
+        return fail(nullptr, MFCFD_ERR_ARG, "params.rks must be 4 (ssprk43) or 1 (first)");
+    if (P.inner_iterations < 0 || P.inner_iterations > 64)
+        return fail(nullptr, MFCFD_ERR_ARG, "params.inner_iterations out of range");
+    if (!(P.cfl > 0.0) || !isfinite(P.mach) || !isfinite(P.aoa) || !isfinite(P.vl_const) ||
+        !isfinite(P.power) || !isfinite(P.euler))
+        return fail(nullptr, MFCFD_ERR_ARG, "params: cfl must be > 0 and all finite");
+    if (P.precision != MFCFD_FP64 && P.precision != MFCFD_FP32_MIXED)
+        return fail(nullptr, MFCFD_ERR_ARG, "params.precision unknown");
+    if (P.precision == MFCFD_FP32_MIXED)
+        return fail(nullptr, MFCFD_ERR_ARG, "params.precision FP32_MIXED is not built in this library");
+    if (P.ordering != MFCFD_ORDER_KIND && P.ordering != MFCFD_ORDER_RCM)
+        return fail(nullptr, MFCFD_ERR_ARG, "params.ordering unknown");
+
+    // grid checks (point_preprocessor.F90:32,73 reject bad partitions and shapes)
+    int nw = 0, no = 0, kp = 1;
+    for (int i = 0; i < n; ++i) {
+        int f = G.flag_1[i], nb = G.nbhs[i];
+        if (f < 0 || f > 2) return fail(nullptr, MFCFD_ERR_GRID, "flag_1 must be 0, 1 or 2");
+        if (G.flag_2[i] < 0 || G.flag_2[i] > G.shapes)
+            return fail(nullptr, MFCFD_ERR_GRID, "shapes value wrong, check again (flag_2)");
+        if (nb < 1 || nb > MAXNB)
+            return fail(nullptr, MFCFD_ERR_GRID, "nbhs out of range [1, 20]");
+        kp = std::max(kp, nb);
+        for (int r = 0; r < nb; ++r) {
+            int k = G.conn[(size_t)r * G.ld_conn + i];
+            if (k < 1 || k > n) return fail(nullptr, MFCFD_ERR_GRID, "conn index out of range");
+        }
+        if (f != 1) {
+            if (G.left[i] < 1 || G.left[i] > n || G.right[i] < 1 || G.right[i] > n)
+                return fail(nullptr, MFCFD_ERR_GRID, "left/right out of range on a boundary point");
+            (f == 0 ? nw : no) += 1;
+        }
+    }
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+        return fail(nullptr, MFCFD_ERR_NODEV, "no CUDA device");
+    {
+        cudaError_t e = init_kernels();
+        if (e != cudaSuccess) return fail(nullptr, MFCFD_ERR_CUDA, cudaGetErrorString(e));
+    }
+
+    h = new (std::nothrow) mfcfd();
+    if (!h) return fail(nullptr, MFCFD_ERR_OOM, "host allocation failed");
+    h->n = n;
+    h->kp = kp;
+    h->nw = nw;
+    h->no = no;
+    h->nint = n - nw - no;
+    h->shapes = G.shapes;
+    h->p = P;
+    cudaGetDevice(&h->dev);
+
+    // parameter.F90:16-34
+    h->pi = 4.0 * atan(1.0);
+    h->theta = P.aoa * h->pi / 180.0;
+    h->cos_t = cos(h->theta);
+    h->sin_t = sin(h->theta);
+    h->q_inf[0] = 1.0;
+    h->q_inf[1] = P.mach * cos(h->theta);
+    h->q_inf[2] = P.mach * sin(h->theta);
+    h->q_inf[3] = 1.0 / 1.4;
+
+    // point_normals.F90:8-105 (caller order)
+    std::vector<double> nx(n), ny(n);
+    for (int i = 0; i < n; ++i) {
+        int f = G.flag_1[i];
+        if (f == 1) {
+            if (P.interior_points_normal_flag == 0 && P.format != 2) {
+                nx[i] = 0.0;
+                ny[i] = 1.0;
+            } else if (P.interior_points_normal_flag == 1 && P.format != 2) {
+                nx[i] = 1.0;
+                ny[i] = 0.0;
+            } else {
+                nx[i] = G.nx[i];
+                ny[i] = G.ny[i];
+            }
+            continue;
+        }
+        int l = G.left[i] - 1, r = G.right[i] - 1;
+        double lx = G.x[l], ly = G.y[l], mx = G.x[i], my = G.y[i], rx = G.x[r], ry = G.y[r];
+        double nx1 = my - ly, nx2 = ry - my, ny1 = mx - lx, ny2 = rx - mx;
+        double vx = 0.5 * (nx1 + nx2), vy = 0.5 * (ny1 + ny2);
+        double det = sqrt(vx * vx + vy * vy);
+        nx[i] = -vx / det;
+        ny[i] = vy / det;
+    }
+
+    // generate_connectivity.F90:39-256 as bit masks (caller order, caller slots)
+    std::vector<unsigned long long> mx(n, 0), my(n, 0);
+    for (int i = 0; i < n; ++i) {
+        int f = G.flag_1[i];
+        double xi = G.x[i], yi = G.y[i], tx = ny[i], ty = -nx[i];
+        unsigned cnt[4] = {0, 0, 0, 0};
+        for (int r = 0; r < G.nbhs[i]; ++r) {
+            int k = G.conn[(size_t)r * G.ld_conn + i] - 1;
+            double delx = G.x[k] - xi, dely = G.y[k] - yi;
+            double dels = delx * tx + dely * ty;
+            double deln = delx * nx[i] + dely * ny[i];
+            if (dels <= 0.0) { mx[i] |= 1ull << r; ++cnt[0]; }
+            if (dels >= 0.0) { mx[i] |= 1ull << (32 + r); ++cnt[1]; }
+            if (f == 1) {
+                if (deln <= 0.0) { my[i] |= 1ull << r; ++cnt[2]; }
+                if (deln >= 0.0) { my[i] |= 1ull << (32 + r); ++cnt[3]; }
+            } else if (f == 0) {
+                my[i] |= 1ull << (32 + r);
+                ++cnt[3];
+            } else {
+                my[i] |= 1ull << r;
+                ++cnt[2];
+            }
+        }
+        bool bad = cnt[0] == 0 || cnt[1] == 0 || (f != 0 && cnt[2] == 0) || (f != 2 && cnt[3] == 0);
+        if (bad) {
+            char msg[160];
+            snprintf(msg, sizeof msg,
+                     "point %d (flag_1 %d) has an empty split list (xpos %u xneg %u ypos %u yneg %u)",
+                     i + 1, f, cnt[0], cnt[1], cnt[2], cnt[3]);
+            int st = fail(nullptr, MFCFD_ERR_GRID, msg);
+            delete h;
+            return st;
+        }
+    }
+
+    // renumbering: new -> caller index
+    std::vector<int> base(n);
+    if (P.ordering == MFCFD_ORDER_RCM) {
+        std::vector<std::vector<int>> adj(n);
+        for (int i = 0; i < n; ++i)
+            for (int r = 0; r < G.nbhs[i]; ++r) {
+                int k = G.conn[(size_t)r * G.ld_conn + i] - 1;
+                if (k == i) continue;
+                adj[i].push_back(k);
+                adj[k].push_back(i);
+            }
+        for (auto &a : adj) {
+            std::sort(a.begin(), a.end());
+            a.erase(std::unique(a.begin(), a.end()), a.end());
+        }
+        base = rcm_order(n, adj);
+    } else {
+        for (int i = 0; i < n; ++i) base[i] = i;
+    }
+    h->perm.reserve(n);
+    for (int want : {0, 2, 1})
+        for (int i : base)
+            if (G.flag_1[i] == want) h->perm.push_back(i);
+    std::vector<int> inv(n);
+    for (int p = 0; p < n; ++p) inv[h->perm[p]] = p;
+
+    // renumbered host arrays
+    std::vector<double2> hxy(n), hnrm(n);
+    std::vector<double> heps(n), hobc((size_t)8 * std::max(no, 1), 0.0);
+    std::vector<int> hconn((size_t)kp * n), hnb(n);
+    std::vector<unsigned long long> hmx(n), hmy(n);
+    for (int p = 0; p < n; ++p) {
+        int i = h->perm[p];
+        hxy[p] = make_double2(G.x[i], G.y[i]);
+        hnrm[p] = make_double2(nx[i], ny[i]);
+        double epsi = P.vl_const * G.min_dist[i];
+        epsi = pow(epsi, 3.0);  // limiters.F90:88-89
+        heps[p] = epsi * epsi;
+        hnb[p] = G.nbhs[i];
+        for (int r = 0; r < kp; ++r) {
+            int k = r < G.nbhs[i] ? inv[G.conn[(size_t)r * G.ld_conn + i] - 1] : p;
+            hconn[(size_t)r * n + p] = k;
+        }
+        hmx[p] = mx[i];
+        hmy[p] = my[i];
+        if (p >= nw && p < nw + no) {
+            // state_update.F90:248-263: the freestream half of Ubar
+            const double pr_inf = 1.0 / 1.4, rho_inf = 1.0, gamma = 1.4;
+            double u1_inf = h->q_inf[1], u2_inf = h->q_inf[2];
+            double tx = ny[i], ty = -nx[i];
+            double u1r = u1_inf * tx + u2_inf * ty;
+            double u2r = u1_inf * nx[i] + u2_inf * ny[i];
+            double temp1 = (u1r * u1r + u2r * u2r);
+            double e_inf = pr_inf / (rho_inf * (gamma - 1.0)) + 0.5 * (temp1);
+            double beta = (0.5 * rho_inf) / pr_inf;
+            double S2 = u2r * sqrt(beta);
+            double B2_inf = exp(-S2 * S2) / (2.0 * sqrt(h->pi * beta));
+            double A2n_inf = 0.5 * (1.0 - erf(S2));
+            double *o = &hobc[(size_t)8 * (p - nw)];
+            o[0] = u1r; o[1] = u2r; o[2] = e_inf; o[3] = A2n_inf; o[4] = B2_inf;
+        }
+    }
+    // shape points in grid order (compute_force_coeffs.F90:40-78)
+    std::vector<int> sidx, sshape;
+    std::vector<double> sgeo, smy;
+    for (int i = 0; i < n; ++i) {
+        if (G.flag_2[i] <= 0) continue;
+        int l = G.left[i] - 1, r = G.right[i] - 1;
+        if (G.flag_1[i] == 1 && (l < 0 || r < 0 || l >= n || r >= n)) {
+            int st = fail(nullptr, MFCFD_ERR_GRID, "shape point without left/right");
+            delete h;
+            return st;
+        }
+        double lx = G.x[l], ly = G.y[l], mxx = G.x[i], myy = G.y[i], rx = G.x[r], ry = G.y[r];
+        double ds1 = (mxx - lx) * (mxx - lx) + (myy - ly) * (myy - ly);
+        ds1 = sqrt(ds1);
+        double ds2 = (rx - mxx) * (rx - mxx) + (ry - myy) * (ry - myy);
+        ds2 = sqrt(ds2);
+        double ds = 0.5 * (ds1 + ds2);
+        sidx.push_back(inv[i]);
+        sshape.push_back(G.flag_2[i] - 1);
+        sgeo.insert(sgeo.end(), {nx[i], ny[i], ds, mxx});
+        smy.push_back(myy);
+    }
+    h->nshape = (int)sidx.size();
+
+    // device arrays
+    int st = MFCFD_OK;
+    auto up = [&](auto *d, const auto &v) -> int {
+        cudaError_t e = cudaMemcpy(d, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice);
+        return e == cudaSuccess ? MFCFD_OK : cuda_fail(h, e, "cudaMemcpy");
+    };
+#define ALLOC(ptr, cnt)                                                     \
+    do {                                                                    \
+        cudaError_t e_ = dmalloc(&(ptr), (size_t)(cnt));                    \
+        if (e_ != cudaSuccess) {                                            \
+            st = cuda_fail(h, e_, "cudaMalloc " #ptr);                      \
+            goto fail_create;                                               \
+        }                                                                   \
+    } while (0)
+    {
+        cudaError_t e = cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            st = cuda_fail(h, e, "cudaStreamCreate");
+            goto fail_create;
+        }
+        h->stream = h->own;
+    }
+    ALLOC(h->d_xy, n);
+    ALLOC(h->d_nrm, n);
+    ALLOC(h->d_eps2, n);
+    ALLOC(h->d_obc, hobc.size());
+    ALLOC(h->d_conn, (size_t)kp * n);
+    ALLOC(h->d_nbhs, n);
+    ALLOC(h->d_mx, n);
+    ALLOC(h->d_my, n);
+    for (int b = 0; b < 2; ++b) {
+        ALLOC(h->d_prim[b], n);
+        ALLOC(h->d_q[b], n);
+        ALLOC(h->d_dq[b], (size_t)8 * n);
+    }
+    ALLOC(h->d_qm, (size_t)8 * n);
+    ALLOC(h->d_delta, n);
+    ALLOC(h->d_spd, n);
+    ALLOC(h->d_res_part, flux_blocks(n));
+    ALLOC(h->d_forces, 3 * h->shapes + std::max(h->nshape, 1));
+    ALLOC(h->d_ctl, 1);
+    ALLOC(h->d_sh_idx, std::max(h->nshape, 1));
+    ALLOC(h->d_sh_shape, std::max(h->nshape, 1));
+    ALLOC(h->d_sh_geo, 4 * std::max(h->nshape, 1));
+    ALLOC(h->d_sh_my, std::max(h->nshape, 1));
+    {
+        cudaError_t e = cudaMallocHost(reinterpret_cast<void **>(&h->h_ctl), sizeof(Ctl));
+        if (e == cudaSuccess)
+            e = cudaMallocHost(reinterpret_cast<void **>(&h->h_stage), sizeof(double) * 4 * (size_t)n);
+        if (e != cudaSuccess) {
+            st = cuda_fail(h, e, "cudaMallocHost");
+            goto fail_create;
+        }
+    }
+    if ((st = up(h->d_xy, hxy)) || (st = up(h->d_nrm, hnrm)) || (st = up(h->d_eps2, heps)) ||
+        (st = up(h->d_obc, hobc)) || (st = up(h->d_conn, hconn)) || (st = up(h->d_nbhs, hnb)) ||
+        (st = up(h->d_mx, hmx)) || (st = up(h->d_my, hmy)))
+        goto fail_create;
+    if (h->nshape > 0) {
+        if ((st = up(h->d_sh_idx, sidx)) || (st = up(h->d_sh_shape, sshape)) ||
+            (st = up(h->d_sh_geo, sgeo)) || (st = up(h->d_sh_my, smy)))
+            goto fail_create;
+    }
+    h->geom = Geom{n, kp, nw, no, h->d_xy, h->d_nrm, h->d_eps2, h->d_conn, h->d_nbhs,
+                   h->d_mx, h->d_my, h->d_obc};
+    h->consts.cfl = P.cfl;
+    h->consts.power = P.power;
+    h->consts.euler = P.euler;
+    h->consts.pi = h->pi;
+    h->consts.gm1 = 1.4 - 1;
+    h->consts.power_zero = P.power == 0.0 ? 1 : 0;
+    h->consts.rks = P.rks;
+    h->shape = ShapeTab{h->nshape, h->shapes, h->d_sh_idx, h->d_sh_shape, h->d_sh_geo, h->d_sh_my};
+    {
+        Ctl c{};
+        c.it = 1;
+        c.it_first = 1;
+        c.restart = P.restart;
+        c.plen = n;
+        c.res_old = P.res_old;
+        *h->h_ctl = c;
+        cudaError_t e = cudaMemcpy(h->d_ctl, h->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            st = cuda_fail(h, e, "cudaMemcpy ctl");
+            goto fail_create;
+        }
+    }
+    // initial_conditions.F90:9-20: freestream everywhere
+    for (int p = 0; p < n; ++p)
+        for (int c = 0; c < 4; ++c) h->h_stage[4 * (size_t)p + c] = h->q_inf[c];
+    {
+        cudaError_t e = cudaMemcpy(h->d_prim[0], h->h_stage, sizeof(double) * 4 * (size_t)n,
+                                   cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            st = cuda_fail(h, e, "cudaMemcpy prim");
+            goto fail_create;
+        }
+    }
+    if ((st = upload_state_aux(h))) goto fail_create;
+    {
+        cudaError_t e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) {
+            st = cuda_fail(h, e, "create sync");
+            goto fail_create;
+        }
+    }
+    *out = h;
+    return MFCFD_OK;
+fail_create:
+    g_create_error = h->err;
+    free_all(h);
+    delete h;
+    return st;
+#undef ALLOC
+}
+
+int mfcfd_destroy(mfcfd_t *h) {
+    if (!h) return MFCFD_OK;
+    cudaStreamSynchronize(h->stream);
+    free_all(h);
+    delete h;
+    return MFCFD_OK;
+}
+
+int mfcfd_set_stream(mfcfd_t *h, void *stream) {
+    if (!h) return MFCFD_ERR_ARG;
+    h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own;
+    return MFCFD_OK;
+}
+
+int mfcfd_set_state(mfcfd_t *h, const double *prim) {
+    if (!h || !prim) return MFCFD_ERR_ARG;
+    CK(cudaStreamSynchronize(h->stream));
+    for (int p = 0; p < h->n; ++p) {
+        const double *src = prim + 4 * (size_t)h->perm[p];
+        double *dst = h->h_stage + 4 * (size_t)p;
+        dst[0] = src[0]; dst[1] = src[1]; dst[2] = src[2]; dst[3] = src[3];
+    }
+    CK(cudaMemcpyAsync(h->d_prim[h->cur], h->h_stage, sizeof(double) * 4 * (size_t)h->n,
+                       cudaMemcpyHostToDevice, h->stream));
+    int st = upload_state_aux(h);
+    if (st) return st;
+    CK(cudaStreamSynchronize(h->stream));
+    return MFCFD_OK;
+}
+
+int mfcfd_get_state(mfcfd_t *h, double *prim) {
+    if (!h || !prim) return MFCFD_ERR_ARG;
+    CK(cudaMemcpyAsync(h->h_stage, h->d_prim[h->cur], sizeof(double) * 4 * (size_t)h->n,
+                       cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int p = 0; p < h->n; ++p) {
+        const double *src = h->h_stage + 4 * (size_t)p;
+        double *dst = prim + 4 * (size_t)h->perm[p];
+        dst[0] = src[0]; dst[1] = src[1]; dst[2] = src[2]; dst[3] = src[3];
+    }
+    return MFCFD_OK;
+}
+
+int mfcfd_run(mfcfd_t *h, int it_first, int n_iters, double *residue, int *n_done) {
+    if (n_done) *n_done = 0;
+    if (!h || n_iters < 0) return MFCFD_ERR_ARG;
+    if (n_iters == 0) return MFCFD_OK;
+    if (n_iters > h->hist_cap) {
+        if (h->d_hist) cudaFree(h->d_hist);
+        h->d_hist = nullptr;
+        h->hist_cap = 0;
+        CK(dmalloc(&h->d_hist, (size_t)n_iters));
+        h->hist_cap = n_iters;
+        drop_graphs(h);  // the graphs hold the old history pointer
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    // reset it / it_first / halted / done; res_old stays on the device
+    h->h_ctl->it = it_first;
+    h->h_ctl->it_first = it_first;
+    h->h_ctl->halted = 0;
+    h->h_ctl->done = 0;
+    CK(cudaMemcpyAsync(h->d_ctl, h->h_ctl, 4 * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    int rem = n_iters;
+    if (rem & 1) {
+        int st = enqueue_iteration(h, h->stream);
+        if (st) return st;
+        --rem;
+    }
+    if (rem > 0) {
+        if (!h->pair_exec[h->cur][h->qcur]) {
+            // capture on the handle's own stream, ordered after the work above
+            CK(cudaStreamSynchronize(h->stream));
+            int st = build_pair_graph(h);
+            if (st) return st;
+        }
+        for (int k = 0; k < rem / 2; ++k) {
+            CK(cudaGraphLaunch(h->pair_exec[h->cur][h->qcur], h->stream));
+            h->launches += 2 * ((long long)h->p.rks * (2 + h->p.inner_iterations) + 1);
+        }
+    }
+    CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    int done = h->h_ctl->done;
+    if (residue && done > 0)
+        CK(cudaMemcpy(residue, h->d_hist, sizeof(double) * done, cudaMemcpyDeviceToHost));
+    if (n_done) *n_done = done;
+    h->iters_done_total += done;
+    if (h->h_ctl->halted) return fail(h, MFCFD_ERR_NONFINITE, "residue is NaN");
+    return MFCFD_OK;
+}
+
+int mfcfd_forces(mfcfd_t *h, double *cl, double *cd, double *cm, double *cp) {
+    if (!h) return MFCFD_ERR_ARG;
+    launch_forces(h->shape, h->d_prim[h->cur], h->p.mach, h->cos_t, h->sin_t, h->d_forces,
+                  h->stream);
+    h->launches += 1;
+    CK(cudaGetLastError());
+    std::vector<double> o(3 * h->shapes + h->nshape);
+    CK(cudaMemcpyAsync(o.data(), h->d_forces, o.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int s = 0; s < h->shapes; ++s) {
+        if (cl) cl[s] = o[s];
+        if (cd) cd[s] = o[h->shapes + s];
+        if (cm) cm[s] = o[2 * h->shapes + s];
+    }
+    if (cp)
+        for (int j = 0; j < h->nshape; ++j) cp[j] = o[3 * h->shapes + j];
+    return MFCFD_OK;
+}
+
+int mfcfd_keep_diagnostics(mfcfd_t *h, int on) {
+    if (!h) return MFCFD_ERR_ARG;
+    bool want = on != 0;
+    if (want && !h->d_flux_dbg) CK(dmalloc(&h->d_flux_dbg, (size_t)4 * h->n));
+    if (want != h->keep_diag) drop_graphs(h);
+    h->keep_diag = want;
+    return MFCFD_OK;
+}
+
+int mfcfd_get_array(mfcfd_t *h, const char *name, double *out) {
+    if (!h || !name || !out) return MFCFD_ERR_ARG;
+    const double *src = nullptr;
+    int w = 0;
+    std::string s(name);
+    if (s == "q") { src = reinterpret_cast<const double *>(h->d_q[h->qcur ^ 1]); w = 4; }
+    else if (s == "dq") { src = h->d_dq[h->p.inner_iterations & 1]; w = 8; }
+    else if (s == "qm") { src = h->d_qm; w = 8; }
+    else if (s == "delta") { src = h->d_delta; w = 1; }
+    else if (s == "flux_res") {
+        if (!h->d_flux_dbg) return fail(h, MFCFD_ERR_STATE, "flux_res needs mfcfd_keep_diagnostics");
+        src = h->d_flux_dbg; w = 4;
+    } else if (s == "nx" || s == "ny") {
+        src = reinterpret_cast<const double *>(h->d_nrm); w = 2;
+    } else {
+        return fail(h, MFCFD_ERR_ARG, "unknown array name");
+    }
+    std::vector<double> tmp((size_t)w * h->n);
+    CK(cudaMemcpyAsync(tmp.data(), src, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (s == "nx" || s == "ny") {
+        int off = s == "nx" ? 0 : 1;
+        for (int p = 0; p < h->n; ++p) out[h->perm[p]] = tmp[2 * (size_t)p + off];
+        return MFCFD_OK;
+    }
+    for (int p = 0; p < h->n; ++p)
+        for (int c = 0; c < w; ++c) {
+            int cc = c;
+            if (w == 8) cc = (c % 4) * 2 + c / 4;  // [dx1..4, dy1..4] -> Fortran (2,4)
+            out[(size_t)w * h->perm[p] + cc] = tmp[(size_t)w * p + c];
+        }
+    return MFCFD_OK;
+}
+
+int mfcfd_info(mfcfd_t *h, int *n, int *n_wall, int *n_outer, int *n_interior) {
+    if (!h) return MFCFD_ERR_ARG;
+    if (n) *n = h->n;
+    if (n_wall) *n_wall = h->nw;
+    if (n_outer) *n_outer = h->no;
+    if (n_interior) *n_interior = h->nint;
+    return MFCFD_OK;
+}
+
+long long mfcfd_launch_count(mfcfd_t *h) { return h ? h->launches : 0; }
+
+const char *mfcfd_strerror(int status) {
+    switch (status) {
+    case MFCFD_OK: return "ok";
+    case MFCFD_ERR_ARG: return "invalid argument";
+    case MFCFD_ERR_CUDA: return "CUDA runtime error";
+    case MFCFD_ERR_NONFINITE: return "residue became NaN";
+    case MFCFD_ERR_TIMEOUT: return "bounded device wait timed out";
+    case MFCFD_ERR_OOM: return "device out of memory";
+    case MFCFD_ERR_GRID: return "invalid or singular grid";
+    case MFCFD_ERR_NODEV: return "no usable CUDA device";
+    case MFCFD_ERR_STATE: return "call not valid in this state";
+    default: return "unknown status";
+    }
+}
+
+const char *mfcfd_last_error(mfcfd_t *h) {
+    return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+}  // extern "C"

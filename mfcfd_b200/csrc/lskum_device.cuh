@@ -1,0 +1,233 @@
+// Device-side building blocks of the LSKUM pseudo-time loop (FP64).
+//
+// Every function restates one reference routine of src_mpi_primal with the
+// same expression association as the Fortran source (which evaluates
+// a*b*c as (a*b)*c and a+b+c as (a+b)+c).  The split-flux routines are
+// written once with sign arguments: a - b == a + (-1)*b exactly in IEEE
+// arithmetic, so Gxp/Gxn (and GxI..GxIV) share one body.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace lskum {
+
+enum PointKind { KIND_WALL = 0, KIND_INTERIOR = 1, KIND_OUTER = 2 };
+
+// Limiter threshold: the literal 10e-6 in limiters.F90:78,81 is a
+// default-real (single precision) constant promoted to double.
+#define MFCFD_VENKAT_THR 9.99999974737875163555145263671875e-06
+
+struct __align__(32) R4 {
+    double a, b, c, d;
+};
+
+__device__ __forceinline__ R4 ld4(const R4 *p) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    double2 u = __ldg(q), v = __ldg(q + 1);
+    return R4{u.x, u.y, v.x, v.y};
+}
+__device__ __forceinline__ void st4(R4 *p, double a, double b, double c, double d) {
+    double2 *q = reinterpret_cast<double2 *>(p);
+    q[0] = make_double2(a, b);
+    q[1] = make_double2(c, d);
+}
+
+// Constant, renumbered geometry.  Wall points occupy [0, nw), outer points
+// [nw, nw + no), interior points [nw + no, n).
+struct Geom {
+    int n, kp, nw, no;
+    const double2 *xy;             // (x, y)
+    const double2 *nrm;            // (nx, ny) as the reference sets them
+    const double *eps2;            // (vl_const*min_dist)**3 squared
+    const int *conn;               // [kp][n], 0-based renumbered indices
+    const int *nbhs;               // [n]
+    const unsigned long long *mx;  // bit r: slot r in xpos; bit 32+r: in xneg
+    const unsigned long long *my;  // bit r: slot r in ypos; bit 32+r: in yneg
+    const double *obc;             // outer points: u1_inf_rot, u2_inf_rot, e_inf, A2n_inf, B2_inf, 0,0,0
+};
+
+struct Consts {
+    double cfl, power, euler, pi, gm1;  // gm1 = gamma - 1
+    int power_zero;                     // power == 0: weights are exactly 1
+    int rks;
+};
+
+// ---------------------------------------------------------------------------
+// q_variables.F90:8-37 eval_q_variables
+__device__ __forceinline__ void q_from_prim(double rho, double u1, double u2, double pr,
+                                            double q[4]) {
+    double beta = 0.5 * rho / pr;
+    q[0] = (log(rho) + (log(beta) * 2.5)) - beta * (u1 * u1 + u2 * u2);
+    double two_times_beta = 2.0 * beta;
+    q[1] = two_times_beta * u1;
+    q[2] = two_times_beta * u2;
+    q[3] = -two_times_beta;
+}
+
+// q_variables.F90:230-256 qtilde_to_primitive
+__device__ __forceinline__ void qtilde_to_primitive(const double qt[4], double gm1, double &u1,
+                                                    double &u2, double &rho, double &pr) {
+    double beta = -qt[3] * 0.5;
+    double temp = 0.5 / beta;
+    u1 = qt[1] * temp;
+    u2 = qt[2] * temp;
+    double temp1 = qt[0] + beta * (u1 * u1 + u2 * u2);
+    double temp2 = temp1 - (log(beta) / gm1);
+    rho = exp(temp2);
+    pr = rho * temp;
+}
+
+// limiters.F90:64-110 venkat_limiter, one component.
+__device__ __forceinline__ double venkat_phi(double qtilde, double q, double qmax, double qmin,
+                                             double eps2) {
+    double del_neg = qtilde - q;
+    if (fabs(del_neg) <= MFCFD_VENKAT_THR) return 1.0;
+    double del_pos = del_neg > 0.0 ? qmax - q : qmin - q;
+    double num = (del_pos * del_pos) + eps2;
+    num = num * del_neg + 2.0 * del_neg * del_neg * del_pos;
+    double den = del_pos * del_pos + 2.0 * del_neg * del_neg;
+    den = den + del_neg * del_pos + eps2;
+    den = den * del_neg;
+    double temp = num / den;
+    return temp < 1.0 ? temp : 1.0;
+}
+
+// Limited reconstruction of one point towards one neighbour direction,
+// straight to primitive variables (the qtilde lines of *_fluxes.F90, e.g.
+// interior_fluxes.F90:158-172).  t = delx*dq(1,:) + dely*dq(2,:) is formed
+// once and used for both the unlimited and the limited qtilde, exactly as the
+// reference recomputes it.
+__device__ __forceinline__ void reconstruct(const double q[4], const double dqx[4],
+                                            const double dqy[4], const double qmax[4],
+                                            const double qmin[4], double eps2, double delx,
+                                            double dely, double gm1, double &u1, double &u2,
+                                            double &rho, double &pr) {
+    double qt[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        double t = delx * dqx[r] + dely * dqy[r];
+        double phi = venkat_phi(q[r] - 0.5 * t, q[r], qmax[r], qmin[r], eps2);
+        qt[r] = q[r] - 0.5 * phi * t;
+    }
+    qtilde_to_primitive(qt, gm1, u1, u2, rho, pr);
+}
+
+// The per-state part shared by split_fluxes.F90 and quadrant_fluxes.F90: the
+// state in the point's (t, n) frame and the two Maxwellian half-moments.
+struct KState {
+    double rho, ut, un, pbr, usq, B1, B2, e1, e2;
+};
+
+__device__ __forceinline__ KState kstate(double u1, double u2, double rho, double pr, double nx,
+                                         double ny, double pi) {
+    KState s;
+    double tx = ny, ty = -nx;
+    s.ut = u1 * tx + u2 * ty;
+    s.un = u1 * nx + u2 * ny;
+    double beta = 0.5 * rho / pr;
+    double sb = sqrt(beta);
+    double S1 = s.ut * sb;
+    double S2 = s.un * sb;
+    double spb = sqrt(pi * beta);
+    s.B1 = 0.5 * exp(-S1 * S1) / spb;
+    s.B2 = 0.5 * exp(-S2 * S2) / spb;
+    s.e1 = erf(S1);
+    s.e2 = erf(S2);
+    s.pbr = pr / rho;
+    s.usq = s.ut * s.ut + s.un * s.un;
+    s.rho = rho;
+    return s;
+}
+
+// split_fluxes.F90:8-96 flux_Gxp (s1 = +1) / flux_Gxn (s1 = -1)
+__device__ __forceinline__ void flux_gx(const KState &s, double s1, double G[4]) {
+    double A1 = 0.5 * (1.0 + s1 * s.e1);
+    G[0] = s.rho * (s.ut * A1 + s1 * s.B1);
+    double temp1 = s.pbr + s.ut * s.ut;
+    double temp2 = temp1 * A1 + s1 * (s.ut * s.B1);
+    G[1] = s.rho * temp2;
+    temp1 = s.ut * s.un * A1 + s1 * (s.un * s.B1);
+    G[2] = s.rho * temp1;
+    temp1 = (7.0 * s.pbr) + s.usq;
+    temp2 = 0.5 * s.ut * temp1 * A1;
+    temp1 = (6.0 * s.pbr) + s.usq;
+    G[3] = s.rho * (temp2 + s1 * (0.5 * temp1 * s.B1));
+}
+
+// split_fluxes.F90:99-190 flux_Gyp (s2 = +1) / flux_Gyn (s2 = -1)
+__device__ __forceinline__ void flux_gy(const KState &s, double s2, double G[4]) {
+    double A2 = 0.5 * (1.0 + s2 * s.e2);
+    G[0] = s.rho * (s.un * A2 + s2 * s.B2);
+    double temp1 = s.pbr + s.un * s.un;
+    double temp2 = temp1 * A2 + s2 * (s.un * s.B2);
+    G[2] = s.rho * temp2;
+    temp1 = s.ut * s.un * A2 + s2 * (s.ut * s.B2);
+    G[1] = s.rho * temp1;
+    temp1 = (7.0 * s.pbr) + s.usq;
+    temp2 = 0.5 * s.un * temp1 * A2;
+    temp1 = (6.0 * s.pbr) + s.usq;
+    G[3] = s.rho * (temp2 + s2 * (0.5 * temp1 * s.B2));
+}
+
+// quadrant_fluxes.F90:12-248: GxI (s1=-1,s2=-1), GxII (+1,-1), GxIII (+1,+1),
+// GxIV (-1,+1).
+__device__ __forceinline__ void flux_quad(const KState &s, double s1, double s2, double G[4]) {
+    double A1 = 0.5 * (1.0 + s1 * s.e1);
+    double A2 = 0.5 * (1.0 + s2 * s.e2);
+    double rA2 = s.rho * A2;
+    double a1b = s.ut * A1 + s1 * s.B1;
+    G[0] = rA2 * a1b;
+    double temp1 = s.pbr + s.ut * s.ut;
+    double temp2 = temp1 * A1 + s1 * (s.ut * s.B1);
+    G[1] = rA2 * temp2;
+    temp2 = s.un * A2 + s2 * s.B2;
+    G[2] = s.rho * a1b * temp2;
+    temp1 = (7.0 * s.pbr) + s.usq;
+    temp2 = 0.5 * s.ut * temp1 * A1;
+    temp1 = (6.0 * s.pbr) + s.usq;
+    double temp3 = 0.5 * s.B1 * temp1;
+    double temp4 = 0.5 * s.rho * s.un * s.B2 * a1b;
+    G[3] = rA2 * (temp2 + s1 * temp3) + s2 * temp4;
+}
+
+// state_update.F90:144-163 primitive_to_conserved
+__device__ __forceinline__ void prim_to_conserved(double rho, double u1, double u2, double pr,
+                                                  double nx, double ny, double U[4]) {
+    U[0] = rho;
+    double temp1 = rho * u1;
+    double temp2 = rho * u2;
+    U[3] = 2.5 * pr + 0.5 * (temp1 * temp1 + temp2 * temp2) / rho;
+    U[1] = temp1 * ny - temp2 * nx;
+    U[2] = temp1 * nx + temp2 * ny;
+}
+
+// state_update.F90:239-294 conserved_vector_Ubar.  The freestream half
+// (inf[0..4] = u1_inf_rot, u2_inf_rot, e_inf, A2n_inf, B2_inf) depends only on
+// the geometry and is computed once on the host.
+__device__ __forceinline__ void conserved_ubar(double rho, double u1, double u2, double pr,
+                                               double nx, double ny, const double *inf,
+                                               double pi, double gm1, double Ubar[4]) {
+    const double rho_inf = 1.0;
+    double u1_inf_rot = inf[0], u2_inf_rot = inf[1], e_inf = inf[2], A2n_inf = inf[3],
+           B2_inf = inf[4];
+    double tx = ny, ty = -nx;
+    double u1_rot = u1 * tx + u2 * ty;
+    double u2_rot = u1 * nx + u2 * ny;
+    double temp1 = (u1_rot * u1_rot + u2_rot * u2_rot);
+    double e = pr / (rho * gm1) + 0.5 * (temp1);
+    double beta = (rho) / (2.0 * pr);
+    double S2 = u2_rot * sqrt(beta);
+    double B2 = exp(-S2 * S2) / (2.0 * sqrt(pi * beta));
+    double A2p = 0.5 * (1.0 + erf(S2));
+    Ubar[0] = (rho_inf * A2n_inf) + (rho * A2p);
+    Ubar[1] = (rho_inf * u1_inf_rot * A2n_inf) + (rho * u1_rot * A2p);
+    temp1 = rho_inf * (u2_inf_rot * A2n_inf - B2_inf);
+    double temp2 = rho * (u2_rot * A2p + B2);
+    Ubar[2] = temp1 + temp2;
+    temp1 = (rho_inf * A2n_inf * e_inf - 0.5 * rho_inf * u2_inf_rot * B2_inf);
+    temp2 = (rho * A2p * e + 0.5 * rho * u2_rot * B2);
+    Ubar[3] = temp1 + temp2;
+}
+
+}  // namespace lskum

@@ -1,0 +1,457 @@
+// FP64 kernels of the LSKUM pseudo-time loop on sm_100a.
+//
+// Per pseudo-time stage (fpi_solver.F90:27-53):
+//   k_grad   D pass  -- eval_q_derivatives (+ func_delta on the first stage)
+//   k_inner  I pass  -- eval_q_inner_loop + eval_update_innerloop (ping-pong)
+//   k_flux   F pass  -- cal_flux_residual + state_update + eval_q_variables of
+//                       the new state (+ res_sqr partials on the last stage)
+// and per iteration k_residual (fpi_solver.F90:57-70).
+//
+// Layout in HBM (renumbered points: wall | outer | interior): one 32-byte
+// row per point for prim and q, 64-byte rows for dq and qm, 16-byte rows for
+// (x, y) and (nx, ny); stencils as ELL columns conn[slot][point] so the
+// thread-per-point passes read them coalesced.
+#include <cuda_runtime.h>
+
+#include "primal.h"
+
+namespace lskum {
+
+namespace {
+
+constexpr int GRAD_BLOCK = 256;
+constexpr int LPP = 8;                   // lanes per point in the flux pass
+constexpr int FLUX_BLOCK = 128;          // 16 points per block
+constexpr int GROUPS = FLUX_BLOCK / LPP;
+constexpr int REC = 19;                  // dGxp[4] dGxn[4] dGyp[4] dGyn[4] dels deln w
+constexpr double OBT = 1.0 / 3.0;        // state_update.F90:19-20
+constexpr double TBT = 2.0 / 3.0;
+
+__device__ __forceinline__ void ld8(const double *p, double a[4], double b[4]) {
+    const double2 *v = reinterpret_cast<const double2 *>(p);
+    double2 t0 = __ldg(v), t1 = __ldg(v + 1), t2 = __ldg(v + 2), t3 = __ldg(v + 3);
+    a[0] = t0.x; a[1] = t0.y; a[2] = t1.x; a[3] = t1.y;
+    b[0] = t2.x; b[1] = t2.y; b[2] = t3.x; b[3] = t3.y;
+}
+
+__device__ __forceinline__ void st8(double *p, const double a[4], const double b[4]) {
+    double2 *v = reinterpret_cast<double2 *>(p);
+    v[0] = make_double2(a[0], a[1]);
+    v[1] = make_double2(a[2], a[3]);
+    v[2] = make_double2(b[0], b[1]);
+    v[3] = make_double2(b[2], b[3]);
+}
+
+// q_variables.F90:41-112 eval_q_derivatives, and state_update.F90:190-236
+// func_delta (spd[k] = |u_k| + 3 sqrt(p_k/rho_k) of the neighbour's state).
+__global__ void __launch_bounds__(GRAD_BLOCK)
+k_grad(Geom g, Consts c, const R4 *__restrict__ q, const double *__restrict__ spd,
+       double *__restrict__ dq, double *__restrict__ qm, double *__restrict__ delta,
+       int with_delta, const Ctl *__restrict__ ctl) {
+    if (ctl->halted) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.n) return;
+    double2 pi_ = g.xy[i];
+    R4 qv = ld4(q + i);
+    double qi[4] = {qv.a, qv.b, qv.c, qv.d};
+    double qmax[4] = {qi[0], qi[1], qi[2], qi[3]};
+    double qmin[4] = {qi[0], qi[1], qi[2], qi[3]};
+    double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
+    double sdxq[4] = {0.0, 0.0, 0.0, 0.0}, sdyq[4] = {0.0, 0.0, 0.0, 0.0};
+    double min_delt = 1.0;
+    int nb = g.nbhs[i];
+    for (int r = 0; r < nb; ++r) {
+        int k = g.conn[r * g.n + i];
+        R4 kv = ld4(q + k);
+        double qk[4] = {kv.a, kv.b, kv.c, kv.d};
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            if (qk[m] > qmax[m]) qmax[m] = qk[m];
+            if (qk[m] < qmin[m]) qmin[m] = qk[m];
+        }
+        double2 pk = g.xy[k];
+        double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
+        double dist = sqrt(delx * delx + dely * dely);
+        double w = c.power_zero ? 1.0 : pow(dist, c.power);
+        sdx2 = sdx2 + delx * delx * w;
+        sdy2 = sdy2 + dely * dely * w;
+        sdxy = sdxy + delx * dely * w;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            sdxq[m] = sdxq[m] + w * delx * (qk[m] - qi[m]);
+            sdyq[m] = sdyq[m] + w * dely * (qk[m] - qi[m]);
+        }
+        if (with_delta) {
+            double delta_t = dist / spd[k];
+            delta_t = c.cfl * delta_t;
+            if (min_delt > delta_t) min_delt = delta_t;
+        }
+    }
+    double det = sdx2 * sdy2 - sdxy * sdxy;
+    double one_by_det = 1.0 / det;
+    double dx[4], dy[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        dx[m] = (sdxq[m] * sdy2 - sdyq[m] * sdxy) * one_by_det;
+        dy[m] = (sdyq[m] * sdx2 - sdxq[m] * sdxy) * one_by_det;
+    }
+    st8(dq + 8 * (size_t)i, dx, dy);
+    st8(qm + 8 * (size_t)i, qmax, qmin);
+    if (with_delta) delta[i] = min_delt;
+}
+
+// q_variables.F90:115-227 eval_q_inner_loop + eval_update_innerloop: reads
+// dq_in, writes dq_out (the buffers swap instead of copying temp into dq).
+__global__ void __launch_bounds__(GRAD_BLOCK)
+k_inner(Geom g, Consts c, const R4 *__restrict__ q, const double *__restrict__ dq_in,
+        double *__restrict__ dq_out, const Ctl *__restrict__ ctl) {
+    if (ctl->halted) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.n) return;
+    double2 pi_ = g.xy[i];
+    R4 qv = ld4(q + i);
+    double qi[4] = {qv.a, qv.b, qv.c, qv.d};
+    double dxi[4], dyi[4];
+    ld8(dq_in + 8 * (size_t)i, dxi, dyi);
+    double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
+    double sdxq[4] = {0.0, 0.0, 0.0, 0.0}, sdyq[4] = {0.0, 0.0, 0.0, 0.0};
+    int nb = g.nbhs[i];
+    for (int r = 0; r < nb; ++r) {
+        int k = g.conn[r * g.n + i];
+        R4 kv = ld4(q + k);
+        double qk[4] = {kv.a, kv.b, kv.c, kv.d};
+        double dxk[4], dyk[4];
+        ld8(dq_in + 8 * (size_t)k, dxk, dyk);
+        double2 pk = g.xy[k];
+        double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
+        double dist = sqrt(delx * delx + dely * dely);
+        double w = c.power_zero ? 1.0 : pow(dist, c.power);
+        sdx2 = sdx2 + delx * delx * w;
+        sdy2 = sdy2 + dely * dely * w;
+        sdxy = sdxy + delx * dely * w;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            double temp1 = qi[m] - 0.5 * (delx * dxi[m] + dely * dyi[m]);
+            double temp2 = qk[m] - 0.5 * (delx * dxk[m] + dely * dyk[m]);
+            sdxq[m] = sdxq[m] + (w * delx * (temp2 - temp1));
+            sdyq[m] = sdyq[m] + (w * dely * (temp2 - temp1));
+        }
+    }
+    double det = sdx2 * sdy2 - sdxy * sdxy;
+    double one_by_det = 1.0 / det;
+    double dx[4], dy[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        dx[m] = one_by_det * (sdxq[m] * sdy2 - sdyq[m] * sdxy);
+        dy[m] = one_by_det * (sdyq[m] * sdx2 - sdxq[m] * sdxy);
+    }
+    st8(dq_out + 8 * (size_t)i, dx, dy);
+}
+
+// flux_residual.F90:14-73 cal_flux_residual + state_update.F90:10-141 +
+// q_variables.F90:8-37 on the new state.
+//
+// Eight lanes share one point; lane l takes stencil slots l, l+8, l+16.  For
+// its neighbour k a lane reconstructs both states once (limiter + qtilde ->
+// primitive; the reference repeats this per direction list with identical
+// inputs, so sharing it is exact), evaluates the split fluxes of every list
+// the neighbour belongs to, and stores G_k - G_i with the geometry in shared
+// memory.  Then lane pair (2L, 2L+1) sums list L in slot order -- the
+// reference's loop order -- for components (0,1) and (2,3), and lane 0
+// gathers the four list derivatives and updates the state.
+__global__ void __launch_bounds__(FLUX_BLOCK)
+k_flux(Geom g, Consts c, StageBufs b, int rk, int last, const Ctl *__restrict__ ctl) {
+    extern __shared__ double sm[];
+    __shared__ double sres[GROUPS];
+    if (ctl->halted) return;
+    const int grp = threadIdx.x / LPP, lane = threadIdx.x % LPP;
+    const int i = blockIdx.x * GROUPS + grp;
+    const bool valid = i < g.n;
+    double *rec = sm + (size_t)grp * g.kp * REC;
+
+    int nb = 0, kind = KIND_INTERIOR;
+    unsigned long long mx = 0, my = 0;
+    double nx = 0.0, ny = 1.0;
+    if (valid) {
+        nb = g.nbhs[i];
+        kind = i < g.nw ? KIND_WALL : (i < g.nw + g.no ? KIND_OUTER : KIND_INTERIOR);
+        mx = g.mx[i];
+        my = g.my[i];
+        double2 nn = g.nrm[i];
+        nx = nn.x;
+        ny = nn.y;
+        double2 pi_ = g.xy[i];
+        R4 qv = ld4(b.q_in + i);
+        double qi[4] = {qv.a, qv.b, qv.c, qv.d};
+        double dxi[4], dyi[4], qmaxi[4], qmini[4];
+        ld8(b.dq + 8 * (size_t)i, dxi, dyi);
+        ld8(b.qm + 8 * (size_t)i, qmaxi, qmini);
+        const double e2i = g.eps2[i];
+        const double tx = ny, ty = -nx;
+        // x-list flux signs: interior Gxp/Gxn; wall GxII/GxI (A2neg); outer
+        // GxIII/GxIV (A2pos).  y lists: Gyp (+1) / Gyn (-1).
+        const double s2q = kind == KIND_WALL ? -1.0 : 1.0;
+        for (int r = lane; r < nb; r += LPP) {
+            int k = g.conn[r * g.n + i];
+            double2 pk = g.xy[k];
+            double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
+            double dels = delx * tx + dely * ty;
+            double deln = delx * nx + dely * ny;
+            double w = 1.0;
+            if (!c.power_zero) w = pow(sqrt(dels * dels + deln * deln), c.power);
+            double u1, u2, rho, pr;
+            reconstruct(qi, dxi, dyi, qmaxi, qmini, e2i, delx, dely, c.gm1, u1, u2, rho, pr);
+            KState si = kstate(u1, u2, rho, pr, nx, ny, c.pi);
+            R4 kv = ld4(b.q_in + k);
+            double qk[4] = {kv.a, kv.b, kv.c, kv.d};
+            double dxk[4], dyk[4], qmaxk[4], qmink[4];
+            ld8(b.dq + 8 * (size_t)k, dxk, dyk);
+            ld8(b.qm + 8 * (size_t)k, qmaxk, qmink);
+            reconstruct(qk, dxk, dyk, qmaxk, qmink, g.eps2[k], delx, dely, c.gm1, u1, u2, rho,
+                        pr);
+            KState sk = kstate(u1, u2, rho, pr, nx, ny, c.pi);
+            double *e = rec + r * REC;
+            double Gi[4], Gk[4];
+#pragma unroll
+            for (int L = 0; L < 4; ++L) {
+                unsigned long long bits = (L < 2) ? mx : my;
+                if (!((bits >> (r + ((L & 1) ? 32 : 0))) & 1ull)) continue;
+                double sg = (L & 1) ? -1.0 : 1.0;
+                if (L < 2) {
+                    if (kind == KIND_INTERIOR) {
+                        flux_gx(si, sg, Gi);
+                        flux_gx(sk, sg, Gk);
+                    } else {
+                        flux_quad(si, sg, s2q, Gi);
+                        flux_quad(sk, sg, s2q, Gk);
+                    }
+                } else {
+                    flux_gy(si, sg, Gi);
+                    flux_gy(sk, sg, Gk);
+                }
+#pragma unroll
+                for (int m = 0; m < 4; ++m) e[4 * L + m] = Gk[m] - Gi[m];
+            }
+            e[16] = dels;
+            e[17] = deln;
+            e[18] = w;
+        }
+    }
+    __syncwarp();
+
+    // List sums in slot order: lane -> list L = lane/2, components c0, c0+1.
+    double Gv0 = 0.0, Gv1 = 0.0;
+    if (valid) {
+        const int L = lane >> 1, c0 = (lane & 1) * 2;
+        const bool used = !((kind == KIND_WALL && L == 2) || (kind == KIND_OUTER && L == 3));
+        const unsigned long long bits = ((L < 2) ? mx : my) >> ((L & 1) ? 32 : 0);
+        if (used) {
+            double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
+            double fx0 = 0.0, fx1 = 0.0, fy0 = 0.0, fy1 = 0.0;
+            for (int r = 0; r < nb; ++r) {
+                if (!((bits >> r) & 1ull)) continue;
+                const double *e = rec + r * REC;
+                double dels = e[16], deln = e[17], w = e[18];
+                double dels_w = dels * w, deln_w = deln * w;
+                sdx2 = sdx2 + dels * dels_w;
+                sdy2 = sdy2 + deln * deln_w;
+                sdxy = sdxy + dels * deln_w;
+                double d0 = e[4 * L + c0], d1 = e[4 * L + c0 + 1];
+                fx0 = fx0 + d0 * dels_w;
+                fy0 = fy0 + d0 * deln_w;
+                fx1 = fx1 + d1 * dels_w;
+                fy1 = fy1 + d1 * deln_w;
+            }
+            double det = sdx2 * sdy2 - sdxy * sdxy;
+            double one_by_det = 1.0 / det;
+            if (L < 2) {
+                Gv0 = (fx0 * sdy2 - fy0 * sdxy) * one_by_det;
+                Gv1 = (fx1 * sdy2 - fy1 * sdxy) * one_by_det;
+            } else {
+                Gv0 = (fy0 * sdx2 - fx0 * sdxy) * one_by_det;
+                Gv1 = (fy1 * sdx2 - fx1 * sdxy) * one_by_det;
+            }
+        }
+    }
+    double G[4][4];
+#pragma unroll
+    for (int L = 0; L < 4; ++L) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            G[L][2 * h] = __shfl_sync(0xffffffffu, Gv0, 2 * L + h, LPP);
+            G[L][2 * h + 1] = __shfl_sync(0xffffffffu, Gv1, 2 * L + h, LPP);
+        }
+    }
+
+    double res_sqr = 0.0;
+    if (valid && lane == 0) {
+        const double delta = b.delta[i];
+        double fr[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            if (kind == KIND_WALL) fr[m] = 2.0 * delta * (G[0][m] + G[1][m] + G[3][m]);
+            else if (kind == KIND_OUTER) fr[m] = delta * (G[0][m] + G[1][m] + G[2][m]);
+            else fr[m] = delta * (G[0][m] + G[1][m] + G[2][m] + G[3][m]);
+        }
+        if (b.flux_dbg) st4(reinterpret_cast<R4 *>(b.flux_dbg) + i, fr[0], fr[1], fr[2], fr[3]);
+        R4 P = ld4(b.prim_in + i);
+        double U[4], Uo[4] = {0.0, 0.0, 0.0, 0.0};
+        if (kind == KIND_OUTER) {
+            const double *inf = g.obc + 8 * (size_t)(i - g.nw);
+            conserved_ubar(P.a, P.b, P.c, P.d, nx, ny, inf, c.pi, c.gm1, U);
+            if (rk == 3) {
+                R4 O = ld4(b.prim_old + i);
+                conserved_ubar(O.a, O.b, O.c, O.d, nx, ny, inf, c.pi, c.gm1, Uo);
+            }
+        } else {
+            prim_to_conserved(P.a, P.b, P.c, P.d, nx, ny, U);
+            if (rk == 3) {
+                R4 O = ld4(b.prim_old + i);
+                prim_to_conserved(O.a, O.b, O.c, O.d, nx, ny, Uo);
+            }
+        }
+        double temp = U[0];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            if (rk != 3) U[m] = U[m] - (0.5 * c.euler * fr[m]);
+            else U[m] = TBT * Uo[m] + OBT * (U[m] - 0.5 * fr[m]);
+        }
+        if (kind == KIND_WALL) U[2] = 0.0;
+        double U2_rot = U[1], U3_rot = U[2];
+        U[1] = U2_rot * ny + U3_rot * nx;
+        U[2] = U3_rot * ny - U2_rot * nx;
+        if (kind != KIND_OUTER) res_sqr = (U[0] - temp) * (U[0] - temp);
+        double rho = U[0];
+        temp = 1.0 / U[0];
+        double u1 = U[1] * temp;
+        double u2 = U[2] * temp;
+        double pr = 0.4 * (U[3] - (0.5 * temp) * (U[1] * U[1] + U[2] * U[2]));
+        st4(b.prim_out + i, rho, u1, u2, pr);
+        double qn[4];
+        q_from_prim(rho, u1, u2, pr, qn);
+        st4(b.q_out + i, qn[0], qn[1], qn[2], qn[3]);
+        if (last) b.spd[i] = sqrt(u1 * u1 + u2 * u2) + 3.0 * sqrt(pr / rho);
+    }
+    if (last) {
+        if (lane == 0) sres[grp] = res_sqr;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s = 0.0;
+            for (int q = 0; q < GROUPS; ++q) s = s + sres[q];
+            b.res_part[blockIdx.x] = s;
+        }
+    }
+}
+
+// fpi_solver.F90:57-70: res_new = sqrt(sum res_sqr)/plen and the residue.
+// Partials are summed in a fixed order (deterministic).
+__global__ void __launch_bounds__(1024)
+k_residual(const double *__restrict__ part, int nparts, Ctl *ctl, double *hist) {
+    __shared__ double s[1024];
+    if (ctl->halted) return;
+    double acc = 0.0;
+    for (int t = threadIdx.x; t < nparts; t += blockDim.x) acc = acc + part[t];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) s[threadIdx.x] = s[threadIdx.x] + s[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double res_new = sqrt(s[0]) / ctl->plen;
+        int it = ctl->it;
+        double residue;
+        if (it <= 2 && ctl->restart == 0) {
+            ctl->res_old = res_new;
+            residue = 0.0;
+        } else {
+            residue = log10(res_new / ctl->res_old);
+        }
+        hist[it - ctl->it_first] = residue;
+        ctl->it = it + 1;
+        ctl->done = ctl->done + 1;
+        if (isnan(residue)) ctl->halted = 1;
+    }
+}
+
+__global__ void k_init_state(Geom g, const R4 *__restrict__ prim, R4 *__restrict__ q,
+                             double *__restrict__ spd) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.n) return;
+    R4 P = ld4(prim + i);
+    double qn[4];
+    q_from_prim(P.a, P.b, P.c, P.d, qn);
+    st4(q + i, qn[0], qn[1], qn[2], qn[3]);
+    spd[i] = sqrt(P.b * P.b + P.c * P.c) + 3.0 * sqrt(P.d / P.a);
+}
+
+// compute_force_coeffs.F90:11-102, one thread, shape points in grid order.
+__global__ void k_forces(ShapeTab t, const R4 *__restrict__ prim, double mach, double cos_t,
+                         double sin_t, double *out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double rho_inf = 1.0, pr_inf = 1.0 / 1.4;
+    double *H = out, *V = out + t.shapes, *PM = out + 2 * t.shapes;
+    double *cp_out = out + 3 * t.shapes;
+    for (int s = 0; s < t.shapes; ++s) H[s] = V[s] = PM[s] = 0.0;
+    double temp = 0.5 * rho_inf * mach * mach;
+    for (int j = 0; j < t.npts; ++j) {
+        int m = t.idx[j], s = t.shape[j];
+        double nx = t.geo[4 * j], ny = t.geo[4 * j + 1], ds = t.geo[4 * j + 2];
+        double mx = t.geo[4 * j + 3], my = t.my[j];
+        double cp = prim[m].d - pr_inf;
+        cp = -cp / temp;
+        cp_out[j] = cp;
+        H[s] = H[s] + cp * nx * ds;
+        V[s] = V[s] + cp * ny * ds;
+        PM[s] = PM[s] + (-cp * ny * ds * (mx - 0.25) + cp * nx * ds * (my));
+    }
+    for (int s = 0; s < t.shapes; ++s) {
+        double h = H[s], v = V[s];
+        H[s] = v * cos_t - h * sin_t;  // Cl
+        V[s] = h * cos_t + v * sin_t;  // Cd
+    }
+}
+
+inline int nblk(int n, int b) { return (n + b - 1) / b; }
+
+}  // namespace
+
+int flux_blocks(int n) { return nblk(n, GROUPS); }
+
+cudaError_t init_kernels() {
+    return cudaFuncSetAttribute(k_flux, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                GROUPS * 20 * REC * (int)sizeof(double));
+}
+
+void launch_grad(const Geom &g, const Consts &c, const R4 *q, const double *spd, double *dq,
+                 double *qm, double *delta, bool with_delta, const Ctl *ctl, cudaStream_t s) {
+    k_grad<<<nblk(g.n, GRAD_BLOCK), GRAD_BLOCK, 0, s>>>(g, c, q, spd, dq, qm, delta,
+                                                       with_delta ? 1 : 0, ctl);
+}
+
+void launch_inner(const Geom &g, const Consts &c, const R4 *q, const double *dq_in,
+                  double *dq_out, const Ctl *ctl, cudaStream_t s) {
+    k_inner<<<nblk(g.n, GRAD_BLOCK), GRAD_BLOCK, 0, s>>>(g, c, q, dq_in, dq_out, ctl);
+}
+
+void launch_flux(const Geom &g, const Consts &c, const StageBufs &b, int rk, bool last,
+                 const Ctl *ctl, cudaStream_t s) {
+    size_t smem = (size_t)GROUPS * g.kp * REC * sizeof(double);
+    k_flux<<<flux_blocks(g.n), FLUX_BLOCK, smem, s>>>(g, c, b, rk, last ? 1 : 0, ctl);
+}
+
+void launch_residual(const double *res_part, int nparts, Ctl *ctl, double *hist,
+                     cudaStream_t s) {
+    k_residual<<<1, 1024, 0, s>>>(res_part, nparts, ctl, hist);
+}
+
+void launch_init_state(const Geom &g, const R4 *prim, R4 *q, double *spd, cudaStream_t s) {
+    k_init_state<<<nblk(g.n, GRAD_BLOCK), GRAD_BLOCK, 0, s>>>(g, prim, q, spd);
+}
+
+void launch_forces(const ShapeTab &t, const R4 *prim, double mach, double cos_t, double sin_t,
+                   double *out, cudaStream_t s) {
+    k_forces<<<1, 32, 0, s>>>(t, prim, mach, cos_t, sin_t, out);
+}
+
+}  // namespace lskum

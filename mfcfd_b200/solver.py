@@ -1,0 +1,146 @@
+"""Host-side mirror of the reference's primal loop over the C ABI.
+
+``Solver`` holds one device-resident problem (one ``mfcfd_t`` handle); its
+methods follow the reference's call sequence in
+src_mpi_primal/meshfree_solver.F90:83 -> q_lskum.F90:16-79:
+
+* construction = read grid + allocate_soln + initial_conditions +
+  compute_normals + generate_connectivity,
+* ``run(n)`` = ``n`` passes of the ``do it = itr+1, itr+max_iters`` loop with
+  fpi_solver, returning the residue history (the loop stops at a NaN residue,
+  as q_lskum.F90:71 does),
+* ``forces()`` = compute_cl_cd_cm (Cl, Cd, Cm per shape, cp per shape point).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .grid import Grid
+
+_PREC = {"fp64": _lib.MFCFD_FP64, "fp32_mixed": _lib.MFCFD_FP32_MIXED}
+_ORDER = {"kind": _lib.MFCFD_ORDER_KIND, "rcm": _lib.MFCFD_ORDER_RCM}
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def make_params(cfl=0.2, power=0.0, vl_const=150.0, mach=0.63, aoa=2.0, tscheme="ssprk43",
+                inner_iterations=0, interior_points_normal_flag=0, format=1, restart=0,
+                res_old=0.0, precision="fp64", ordering="kind") -> _lib.Params:
+    """Case parameters with the reference's readcase defaults (readcase.F90)."""
+    if tscheme == "ssprk43":
+        rks, euler = 4, 1.0
+    elif tscheme == "first":
+        rks, euler = 1, 2.0
+    else:
+        raise ValueError(f"unknown tscheme {tscheme!r}")
+    return _lib.Params(cfl, power, vl_const, mach, aoa, rks, euler, inner_iterations,
+                       interior_points_normal_flag, format, restart, res_old,
+                       _PREC[precision], _ORDER[ordering])
+
+
+class Solver:
+    """Device-resident LSKUM primal solver for one grid (FP64 path)."""
+
+    def __init__(self, grid: Grid, **params):
+        self.lib = _lib.load()
+        self.grid = grid
+        self.n = grid.n
+        self.params = make_params(**params)
+        self.it = 0 if self.params.restart == 0 else None
+        g = grid
+        self._arrays = [np.ascontiguousarray(a) for a in
+                        (g.x, g.y, g.nx, g.ny, g.min_dist, g.flag_1, g.flag_2, g.left, g.right,
+                         g.nbhs, g.conn)]
+        a = self._arrays
+        self._grid = _lib.Grid(self.n, *[_ptr(v) for v in a], self.n, g.shapes)
+        h = C.c_void_p()
+        st = self.lib.mfcfd_create(C.byref(self._grid), C.byref(self.params), C.byref(h))
+        _lib.check(st, None, "mfcfd_create")
+        self.h = h
+        self.halted = False
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mfcfd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # state -------------------------------------------------------------
+    def set_state(self, prim: np.ndarray) -> None:
+        prim = np.ascontiguousarray(prim, dtype=np.float64)
+        if prim.shape != (self.n, 4):
+            raise ValueError(f"prim must be ({self.n}, 4)")
+        _lib.check(self.lib.mfcfd_set_state(self.h, _dptr(prim)), self.h, "mfcfd_set_state")
+
+    def get_state(self) -> np.ndarray:
+        out = np.empty((self.n, 4))
+        _lib.check(self.lib.mfcfd_get_state(self.h, _dptr(out)), self.h, "mfcfd_get_state")
+        return out
+
+    prim = get_state
+
+    # loop ----------------------------------------------------------------
+    def run(self, n_iters: int, it_first: int | None = None) -> np.ndarray:
+        """Runs ``n_iters`` iterations; returns the residue of each one done."""
+        if it_first is None:
+            it_first = (self.it or 0) + 1
+        res = np.zeros(max(n_iters, 1))
+        done = C.c_int(0)
+        st = self.lib.mfcfd_run(self.h, int(it_first), int(n_iters), _dptr(res), C.byref(done))
+        self.it = it_first + done.value - 1
+        if st == _lib.MFCFD_ERR_NONFINITE:
+            self.halted = True
+        else:
+            _lib.check(st, self.h, "mfcfd_run")
+        return res[:done.value].copy()
+
+    def forces(self):
+        """(Cl, Cd, Cm) per shape and cp per shape point (grid order)."""
+        s = self.grid.shapes
+        cl, cd, cm = np.zeros(s), np.zeros(s), np.zeros(s)
+        cp = np.zeros(int((self.grid.flag_2 > 0).sum()))
+        _lib.check(self.lib.mfcfd_forces(self.h, _dptr(cl), _dptr(cd), _dptr(cm), _dptr(cp)),
+                   self.h, "mfcfd_forces")
+        return cl, cd, cm, cp
+
+    # diagnostics -----------------------------------------------------------
+    def keep_diagnostics(self, on: bool = True) -> None:
+        _lib.check(self.lib.mfcfd_keep_diagnostics(self.h, 1 if on else 0), self.h,
+                   "mfcfd_keep_diagnostics")
+
+    _WIDTH = {"q": 4, "dq": 8, "qm": 8, "delta": 1, "flux_res": 4, "nx": 1, "ny": 1}
+
+    def get_array(self, name: str) -> np.ndarray:
+        w = self._WIDTH[name]
+        out = np.empty(self.n * w)
+        _lib.check(self.lib.mfcfd_get_array(self.h, name.encode(), _dptr(out)), self.h,
+                   f"mfcfd_get_array({name})")
+        return out.reshape(self.n, w) if w > 1 else out
+
+    def launch_count(self) -> int:
+        return int(self.lib.mfcfd_launch_count(self.h))
+
+    def info(self):
+        v = [C.c_int() for _ in range(4)]
+        _lib.check(self.lib.mfcfd_info(self.h, *[C.byref(x) for x in v]), self.h, "mfcfd_info")
+        return tuple(x.value for x in v)
