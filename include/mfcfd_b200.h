@@ -139,7 +139,7 @@ int mfcfd_get_array(mfcfd_t *h, const char *name, double *out);
 /* Whether the flux pass also stores flux_res for mfcfd_get_array (0/1). */
 int mfcfd_keep_diagnostics(mfcfd_t *h, int on);
 
-/* Number of points, and the number of split-list entries per point type. */
+/* Number of points and of wall, outer and interior points. */
 int mfcfd_info(mfcfd_t *h, int *n, int *n_wall, int *n_outer, int *n_interior);
 
 /* Human-readable text of a status code (static storage). */
@@ -151,6 +151,13 @@ const char *mfcfd_last_error(mfcfd_t *h);
 
 /* Device kernels launched by the handle since creation (all kinds). */
 long long mfcfd_launch_count(mfcfd_t *h);
+
+/* Runs iteration `it` with a CUDA event after every kernel on the handle's
+ * stream and returns the mean duration per launch in ms of the gradient,
+ * inner-iteration, flux and residual kernels (ms[0..3]) and of the whole
+ * iteration (ms[4]).  The state advances by that iteration, as mfcfd_run
+ * would advance it (no CUDA graph). */
+int mfcfd_profile_iteration(mfcfd_t *h, int it, double *ms);
 
 #ifdef __cplusplus
 }

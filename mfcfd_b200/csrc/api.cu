@@ -294,34 +294,11 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
             (f == 0 ? nw : no) += 1;
         }
     }
-    int dev_count = 0;
-    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
-        return fail(nullptr, MFCFD_ERR_NODEV, "no CUDA device");
-    {
-        cudaError_t e = init_kernels();
-        if (e != cudaSuccess) return fail(nullptr, MFCFD_ERR_CUDA, cudaGetErrorString(e));
-    }
-
-    h = new (std::nothrow) mfcfd();
-    if (!h) return fail(nullptr, MFCFD_ERR_OOM, "host allocation failed");
-    h->n = n;
-    h->kp = kp;
-    h->nw = nw;
-    h->no = no;
-    h->nint = n - nw - no;
-    h->shapes = G.shapes;
-    h->p = P;
-    cudaGetDevice(&h->dev);
 
     // parameter.F90:16-34
-    h->pi = 4.0 * atan(1.0);
-    h->theta = P.aoa * h->pi / 180.0;
-    h->cos_t = cos(h->theta);
-    h->sin_t = sin(h->theta);
-    h->q_inf[0] = 1.0;
-    h->q_inf[1] = P.mach * cos(h->theta);
-    h->q_inf[2] = P.mach * sin(h->theta);
-    h->q_inf[3] = 1.0 / 1.4;
+    const double pi = 4.0 * atan(1.0);
+    const double theta = P.aoa * pi / 180.0;
+    const double q_inf[4] = {1.0, P.mach * cos(theta), P.mach * sin(theta), 1.0 / 1.4};
 
     // point_normals.F90:8-105 (caller order)
     std::vector<double> nx(n), ny(n);
@@ -379,11 +356,37 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
             snprintf(msg, sizeof msg,
                      "point %d (flag_1 %d) has an empty split list (xpos %u xneg %u ypos %u yneg %u)",
                      i + 1, f, cnt[0], cnt[1], cnt[2], cnt[3]);
-            int st = fail(nullptr, MFCFD_ERR_GRID, msg);
-            delete h;
-            return st;
+            return fail(nullptr, MFCFD_ERR_GRID, msg);
         }
     }
+    // shape points need ring neighbours for ds (compute_force_coeffs.F90:43-62)
+    for (int i = 0; i < n; ++i)
+        if (G.flag_2[i] > 0 && (G.left[i] < 1 || G.left[i] > n || G.right[i] < 1 || G.right[i] > n))
+            return fail(nullptr, MFCFD_ERR_GRID, "shape point without valid left/right");
+
+    // host checks done: now the device
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+        return fail(nullptr, MFCFD_ERR_NODEV, "no CUDA device");
+    {
+        cudaError_t e = init_kernels();
+        if (e != cudaSuccess) return fail(nullptr, MFCFD_ERR_CUDA, cudaGetErrorString(e));
+    }
+    h = new (std::nothrow) mfcfd();
+    if (!h) return fail(nullptr, MFCFD_ERR_OOM, "host allocation failed");
+    h->n = n;
+    h->kp = kp;
+    h->nw = nw;
+    h->no = no;
+    h->nint = n - nw - no;
+    h->shapes = G.shapes;
+    h->p = P;
+    cudaGetDevice(&h->dev);
+    h->pi = pi;
+    h->theta = theta;
+    h->cos_t = cos(theta);
+    h->sin_t = sin(theta);
+    for (int c = 0; c < 4; ++c) h->q_inf[c] = q_inf[c];
 
     // renumbering: new -> caller index
     std::vector<int> base(n);
@@ -453,11 +456,6 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
     for (int i = 0; i < n; ++i) {
         if (G.flag_2[i] <= 0) continue;
         int l = G.left[i] - 1, r = G.right[i] - 1;
-        if (G.flag_1[i] == 1 && (l < 0 || r < 0 || l >= n || r >= n)) {
-            int st = fail(nullptr, MFCFD_ERR_GRID, "shape point without left/right");
-            delete h;
-            return st;
-        }
         double lx = G.x[l], ly = G.y[l], mxx = G.x[i], myy = G.y[i], rx = G.x[r], ry = G.y[r];
         double ds1 = (mxx - lx) * (mxx - lx) + (myy - ly) * (myy - ly);
         ds1 = sqrt(ds1);
@@ -752,6 +750,79 @@ int mfcfd_info(mfcfd_t *h, int *n, int *n_wall, int *n_outer, int *n_interior) {
 }
 
 long long mfcfd_launch_count(mfcfd_t *h) { return h ? h->launches : 0; }
+
+int mfcfd_profile_iteration(mfcfd_t *h, int it, double *ms) {
+    if (!h || !ms) return MFCFD_ERR_ARG;
+    const int m = h->p.inner_iterations;
+    const int nev = h->p.rks * (2 + m) + 2;
+    std::vector<cudaEvent_t> ev(nev);
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    CK(cudaStreamSynchronize(h->stream));
+    h->h_ctl->it = it;
+    h->h_ctl->it_first = it;
+    h->h_ctl->halted = 0;
+    h->h_ctl->done = 0;
+    if (h->hist_cap < 1) {
+        CK(dmalloc(&h->d_hist, 1));
+        h->hist_cap = 1;
+    }
+    CK(cudaMemcpyAsync(h->d_ctl, h->h_ctl, 4 * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    const int A = h->cur, B = h->cur ^ 1;
+    int e = 0;
+    CK(cudaEventRecord(ev[e++], h->stream));
+    for (int rk = 1; rk <= h->p.rks; ++rk) {
+        const R4 *q_in = h->d_q[h->qcur];
+        launch_grad(h->geom, h->consts, q_in, h->d_spd, h->d_dq[0], h->d_qm, h->d_delta,
+                    rk == 1, h->d_ctl, h->stream);
+        CK(cudaEventRecord(ev[e++], h->stream));
+        for (int t = 1; t <= m; ++t) {
+            launch_inner(h->geom, h->consts, q_in, h->d_dq[(t - 1) & 1], h->d_dq[t & 1],
+                         h->d_ctl, h->stream);
+            CK(cudaEventRecord(ev[e++], h->stream));
+        }
+        StageBufs b;
+        b.prim_in = rk == 1 ? h->d_prim[A] : h->d_prim[B];
+        b.prim_out = h->d_prim[B];
+        b.prim_old = h->d_prim[A];
+        b.q_in = q_in;
+        b.q_out = h->d_q[h->qcur ^ 1];
+        b.dq = h->d_dq[m & 1];
+        b.qm = h->d_qm;
+        b.delta = h->d_delta;
+        b.spd = h->d_spd;
+        b.res_part = h->d_res_part;
+        b.flux_dbg = h->keep_diag ? h->d_flux_dbg : nullptr;
+        launch_flux(h->geom, h->consts, b, rk, rk == h->p.rks, h->d_ctl, h->stream);
+        CK(cudaEventRecord(ev[e++], h->stream));
+        h->qcur ^= 1;
+    }
+    launch_residual(h->d_res_part, flux_blocks(h->n), h->d_ctl, h->d_hist, h->stream);
+    CK(cudaEventRecord(ev[e++], h->stream));
+    h->launches += nev - 1;
+    h->cur = B;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    double sum[4] = {0, 0, 0, 0};
+    int cnt[4] = {0, 0, 0, 0};
+    e = 1;
+    auto span = [&](int k) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, ev[k - 1], ev[k]);
+        return (double)t;
+    };
+    for (int rk = 1; rk <= h->p.rks; ++rk) {
+        sum[0] += span(e++); cnt[0]++;
+        for (int t = 1; t <= m; ++t) { sum[1] += span(e++); cnt[1]++; }
+        sum[2] += span(e++); cnt[2]++;
+    }
+    sum[3] += span(e++); cnt[3]++;
+    for (int k = 0; k < 4; ++k) ms[k] = cnt[k] ? sum[k] / cnt[k] : 0.0;
+    float tot = 0.f;
+    cudaEventElapsedTime(&tot, ev[0], ev[nev - 1]);
+    ms[4] = tot;
+    for (auto &x : ev) cudaEventDestroy(x);
+    return MFCFD_OK;
+}
 
 const char *mfcfd_strerror(int status) {
     switch (status) {

@@ -24,15 +24,11 @@ constexpr int LPP = 8;                   // lanes per point in the flux pass
 constexpr int FLUX_BLOCK = 128;          // 16 points per block
 constexpr int GROUPS = FLUX_BLOCK / LPP;
 constexpr int REC = 19;                  // dGxp[4] dGxn[4] dGyp[4] dGyn[4] dels deln w
+#ifndef FLUX_MIN_BLOCKS
+#define FLUX_MIN_BLOCKS 5                // <= 102 registers: 20 warps per SM
+#endif
 constexpr double OBT = 1.0 / 3.0;        // state_update.F90:19-20
 constexpr double TBT = 2.0 / 3.0;
-
-__device__ __forceinline__ void ld8(const double *p, double a[4], double b[4]) {
-    const double2 *v = reinterpret_cast<const double2 *>(p);
-    double2 t0 = __ldg(v), t1 = __ldg(v + 1), t2 = __ldg(v + 2), t3 = __ldg(v + 3);
-    a[0] = t0.x; a[1] = t0.y; a[2] = t1.x; a[3] = t1.y;
-    b[0] = t2.x; b[1] = t2.y; b[2] = t3.x; b[3] = t3.y;
-}
 
 __device__ __forceinline__ void st8(double *p, const double a[4], const double b[4]) {
     double2 *v = reinterpret_cast<double2 *>(p);
@@ -40,6 +36,13 @@ __device__ __forceinline__ void st8(double *p, const double a[4], const double b
     v[1] = make_double2(a[2], a[3]);
     v[2] = make_double2(b[0], b[1]);
     v[3] = make_double2(b[2], b[3]);
+}
+
+__device__ __forceinline__ void ld8(const double *p, double a[4], double b[4]) {
+    const double2 *v = reinterpret_cast<const double2 *>(p);
+    double2 t0 = __ldg(v), t1 = __ldg(v + 1), t2 = __ldg(v + 2), t3 = __ldg(v + 3);
+    a[0] = t0.x; a[1] = t0.y; a[2] = t1.x; a[3] = t1.y;
+    b[0] = t2.x; b[1] = t2.y; b[2] = t3.x; b[3] = t3.y;
 }
 
 // q_variables.F90:41-112 eval_q_derivatives, and state_update.F90:190-236
@@ -124,8 +127,8 @@ k_inner(Geom g, Consts c, const R4 *__restrict__ q, const double *__restrict__ d
         ld8(dq_in + 8 * (size_t)k, dxk, dyk);
         double2 pk = g.xy[k];
         double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
-        double dist = sqrt(delx * delx + dely * dely);
-        double w = c.power_zero ? 1.0 : pow(dist, c.power);
+        double w = 1.0;
+        if (!c.power_zero) w = pow(sqrt(delx * delx + dely * dely), c.power);
         sdx2 = sdx2 + delx * delx * w;
         sdy2 = sdy2 + dely * dely * w;
         sdxy = sdxy + delx * dely * w;
@@ -159,7 +162,7 @@ k_inner(Geom g, Consts c, const R4 *__restrict__ q, const double *__restrict__ d
 // memory.  Then lane pair (2L, 2L+1) sums list L in slot order -- the
 // reference's loop order -- for components (0,1) and (2,3), and lane 0
 // gathers the four list derivatives and updates the state.
-__global__ void __launch_bounds__(FLUX_BLOCK)
+__global__ void __launch_bounds__(FLUX_BLOCK, FLUX_MIN_BLOCKS)
 k_flux(Geom g, Consts c, StageBufs b, int rk, int last, const Ctl *__restrict__ ctl) {
     extern __shared__ double sm[];
     __shared__ double sres[GROUPS];
@@ -177,46 +180,55 @@ k_flux(Geom g, Consts c, StageBufs b, int rk, int last, const Ctl *__restrict__ 
         kind = i < g.nw ? KIND_WALL : (i < g.nw + g.no ? KIND_OUTER : KIND_INTERIOR);
         mx = g.mx[i];
         my = g.my[i];
-        double2 nn = g.nrm[i];
+        const double2 nn = g.nrm[i];
         nx = nn.x;
         ny = nn.y;
-        double2 pi_ = g.xy[i];
-        R4 qv = ld4(b.q_in + i);
-        double qi[4] = {qv.a, qv.b, qv.c, qv.d};
-        double dxi[4], dyi[4], qmaxi[4], qmini[4];
-        ld8(b.dq + 8 * (size_t)i, dxi, dyi);
-        ld8(b.qm + 8 * (size_t)i, qmaxi, qmini);
-        const double e2i = g.eps2[i];
-        const double tx = ny, ty = -nx;
         // x-list flux signs: interior Gxp/Gxn; wall GxII/GxI (A2neg); outer
         // GxIII/GxIV (A2pos).  y lists: Gyp (+1) / Gyn (-1).
         const double s2q = kind == KIND_WALL ? -1.0 : 1.0;
         for (int r = lane; r < nb; r += LPP) {
-            int k = g.conn[r * g.n + i];
-            double2 pk = g.xy[k];
-            double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
-            double dels = delx * tx + dely * ty;
-            double deln = delx * nx + dely * ny;
+            const int k = g.conn[r * g.n + i];
+            const double2 pi_ = g.xy[i];
+            const double2 pk = g.xy[k];
+            const double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
+            // neighbour state first (its gathers are the long-latency loads),
+            // then the point's own state, re-read per slot from L1 so nothing
+            // but the neighbour's kinetic state stays live across the two
+            KState sk, si;
+            {
+                const R4 kv = ld4(b.q_in + k);
+                const double qk[4] = {kv.a, kv.b, kv.c, kv.d};
+                double dxk[4], dyk[4], qmaxk[4], qmink[4];
+                ld8(b.dq + 8 * (size_t)k, dxk, dyk);
+                ld8(b.qm + 8 * (size_t)k, qmaxk, qmink);
+                double u1, u2, rho, pr;
+                reconstruct(qk, dxk, dyk, qmaxk, qmink, g.eps2[k], delx, dely, c.gm1, u1, u2, rho,
+                            pr);
+                sk = kstate(u1, u2, rho, pr, nx, ny, c.pi);
+            }
+            {
+                const R4 qv = ld4(b.q_in + i);
+                const double qi[4] = {qv.a, qv.b, qv.c, qv.d};
+                double dxi[4], dyi[4], qmaxi[4], qmini[4];
+                ld8(b.dq + 8 * (size_t)i, dxi, dyi);
+                ld8(b.qm + 8 * (size_t)i, qmaxi, qmini);
+                double u1, u2, rho, pr;
+                reconstruct(qi, dxi, dyi, qmaxi, qmini, g.eps2[i], delx, dely, c.gm1, u1, u2, rho,
+                            pr);
+                si = kstate(u1, u2, rho, pr, nx, ny, c.pi);
+            }
+            const double tx = ny, ty = -nx;
+            const double dels = delx * tx + dely * ty;
+            const double deln = delx * nx + dely * ny;
             double w = 1.0;
             if (!c.power_zero) w = pow(sqrt(dels * dels + deln * deln), c.power);
-            double u1, u2, rho, pr;
-            reconstruct(qi, dxi, dyi, qmaxi, qmini, e2i, delx, dely, c.gm1, u1, u2, rho, pr);
-            KState si = kstate(u1, u2, rho, pr, nx, ny, c.pi);
-            R4 kv = ld4(b.q_in + k);
-            double qk[4] = {kv.a, kv.b, kv.c, kv.d};
-            double dxk[4], dyk[4], qmaxk[4], qmink[4];
-            ld8(b.dq + 8 * (size_t)k, dxk, dyk);
-            ld8(b.qm + 8 * (size_t)k, qmaxk, qmink);
-            reconstruct(qk, dxk, dyk, qmaxk, qmink, g.eps2[k], delx, dely, c.gm1, u1, u2, rho,
-                        pr);
-            KState sk = kstate(u1, u2, rho, pr, nx, ny, c.pi);
             double *e = rec + r * REC;
             double Gi[4], Gk[4];
 #pragma unroll
             for (int L = 0; L < 4; ++L) {
-                unsigned long long bits = (L < 2) ? mx : my;
+                const unsigned long long bits = (L < 2) ? mx : my;
                 if (!((bits >> (r + ((L & 1) ? 32 : 0))) & 1ull)) continue;
-                double sg = (L & 1) ? -1.0 : 1.0;
+                const double sg = (L & 1) ? -1.0 : 1.0;
                 if (L < 2) {
                     if (kind == KIND_INTERIOR) {
                         flux_gx(si, sg, Gi);

@@ -1,0 +1,66 @@
+"""Host driver of a run: the reference's meshfree_solver + q_lskum sequence
+(src_mpi_primal/meshfree_solver.F90:18-103, q_lskum.F90:16-79) over the C ABI.
+
+    python -m mfcfd_b200.driver CASE_DIR
+
+reads CASE_DIR/case.in (or input.nml), the grid CASE_DIR/point/partGrid,
+optionally CASE_DIR/restart/sol.dat, runs max_iters iterations on the GPU and
+writes CASE_DIR/residue, CASE_DIR/cp/cp-file and, every nsave iterations,
+CASE_DIR/solution/sol.dat, in the reference's formats.
+"""
+from __future__ import annotations
+
+import os
+import sys
+import time
+
+from . import io
+from .solver import Solver
+
+
+def run_case(case_dir: str, grid=None, quiet: bool = False, chunk: int = 100) -> dict:
+    case = os.path.join(case_dir, "case.in")
+    opts = io.read_case(case) if os.path.exists(case) else io.read_nml(
+        os.path.join(case_dir, "input.nml"))
+    params = io.solver_params(opts)
+    if grid is None:
+        grid = io.read_partgrid(os.path.join(case_dir, "point", "partGrid"),
+                                shapes=int(opts["shapes"]))
+    itr, res_old = 0, 0.0
+    prim0 = None
+    if params["restart"]:
+        itr, res_old, prim0 = io.read_restart(os.path.join(case_dir, "restart", "sol.dat"), grid.n)
+        params["res_old"] = res_old
+    log = (lambda *a: None) if quiet else print
+    t0 = time.perf_counter()
+    its, res = [], []
+    with Solver(grid, **params) as s:
+        if prim0 is not None:
+            s.set_state(prim0)
+        max_iters, nsave = int(opts["max_iters"]), int(opts["nsave"])
+        it = itr
+        while it < itr + max_iters and not s.halted:
+            # stop at each multiple of nsave to write the solution file
+            n = min(chunk, itr + max_iters - it, nsave - it % nsave)
+            r = s.run(n, it_first=it + 1)
+            for k, v in enumerate(r):
+                log(f"  iterations:{it + 1 + k:8d}       residue:{v:30.20e}")
+            its.extend(range(it + 1, it + 1 + len(r)))
+            res.extend(r.tolist())
+            it += len(r)
+            if it % nsave == 0 and not s.halted:
+                io.write_solution(os.path.join(case_dir, "solution", "sol.dat"), grid,
+                                  s.get_state(), it + 1, res_old)
+        cl, cd, cm, cp = s.forces()
+        prim = s.get_state()
+    run_time = time.perf_counter() - t0
+    io.write_residue(os.path.join(case_dir, "residue"), its, res)
+    io.write_cp(os.path.join(case_dir, "cp", "cp-file"), grid, cp)
+    log(f" Vector function is {cd[0]:.17g}")
+    log(f" Run time: {run_time:.6f} seconds")
+    return dict(iterations=len(res), residue=res, cl=cl, cd=cd, cm=cm, cp=cp, prim=prim,
+                run_time=run_time)
+
+
+if __name__ == "__main__":
+    run_case(sys.argv[1] if len(sys.argv) > 1 else ".")

@@ -250,6 +250,12 @@ def naca_ogrid(ni: int, nj: int, thickness: float = 0.12, radius: float = 20.0,
     yw[0] = 0.0
     xo = 0.5 + radius * np.cos(phi)
     yo = -radius * np.sin(phi)
+    # the trailing- and leading-edge rays lie exactly on y = 0 (sin(pi) is
+    # not 0 in floating point; a 1e-15 tilt would put their on-ray neighbours
+    # in one y split list instead of both)
+    on_axis = (np.arange(ni) == 0) | (2 * np.arange(ni) == ni)
+    yo[on_axis] = 0.0
+    yw[on_axis] = 0.0
     dxr, dyr = xo - xw, yo - yw
     length = np.hypot(dxr, dyr)
     r = _stretch_ratio(length, first_spacing, nj - 1)
@@ -280,6 +286,15 @@ def naca_ogrid(ni: int, nj: int, thickness: float = 0.12, radius: float = 20.0,
     else:
         raise ValueError(f"unknown rays {rays!r}")
     X[-1, :], Y[-1, :] = xo, yo
+    if ni % 2 == 0:
+        # exact mirror symmetry about y = 0 before jitter: points that are
+        # aligned in exact arithmetic stay aligned (their dels/deln tie at 0
+        # and they enter both split lists on both sides)
+        h = ni // 2
+        X[:, h + 1:] = X[:, 1:h][:, ::-1]
+        Y[:, h + 1:] = -Y[:, 1:h][:, ::-1]
+        Y[:, 0] = 0.0
+        Y[:, h] = 0.0
 
     if jitter > 0 and nj > 2:
         def dist(ax, ay, bx, by):
@@ -361,6 +376,9 @@ CONFIGS = {
                seed=3000, first_spacing=1e-3),
     "C5": dict(ni=2560, nj=1600, mach=0.8, aoa=1.25, inner_iterations=0, iters=5000,
                seed=5000, first_spacing=1e-3),
+    # profiling case: the C2 flow on half the points (working set still > L2)
+    "P": dict(ni=1024, nj=512, mach=0.85, aoa=1.0, inner_iterations=3, iters=100,
+              seed=9000, first_spacing=1e-3),
 }
 FLOW_DEFAULTS = dict(cfl=0.2, vl_const=5.0, power=0.0, tscheme="ssprk43")
 

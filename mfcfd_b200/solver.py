@@ -137,6 +137,20 @@ class Solver:
                    f"mfcfd_get_array({name})")
         return out.reshape(self.n, w) if w > 1 else out
 
+    def profile_iteration(self) -> dict:
+        """Runs the next iteration with CUDA events around every kernel; mean
+        ms per launch of each kernel kind and of the whole iteration."""
+        it = (self.it or 0) + 1
+        ms = np.zeros(5)
+        _lib.check(self.lib.mfcfd_profile_iteration(self.h, it, _dptr(ms)), self.h,
+                   "mfcfd_profile_iteration")
+        self.it = it
+        return dict(grad=ms[0], inner=ms[1], flux=ms[2], residual=ms[3], iteration=ms[4])
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        _lib.check(self.lib.mfcfd_set_stream(self.h, C.c_void_p(stream_ptr or 0)), self.h,
+                   "mfcfd_set_stream")
+
     def launch_count(self) -> int:
         return int(self.lib.mfcfd_launch_count(self.h))
 
