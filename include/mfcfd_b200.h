@@ -13,7 +13,7 @@
  *   initial_conditions.F90:9-70      freestream/restart -> create / set_state
  * The reference has no C ABI, plugin or operator registry; its Fortran host
  * binds these entry points through ISO_C_BINDING (see the Fortran module
- * shipped in fortran/mfcfd_b200.F90).
+ * include/mfcfd_b200_mod.F90).
  *
  * Array conventions follow the Fortran arrays the reference keeps in
  * `type(points) :: point` (src_mpi_primal/data_structure.F90:13-49):
@@ -151,6 +151,24 @@ const char *mfcfd_last_error(mfcfd_t *h);
 
 /* Device kernels launched by the handle since creation (all kinds). */
 long long mfcfd_launch_count(mfcfd_t *h);
+
+/* Largest n_iters one mfcfd_run_noalloc call accepts. */
+#define MFCFD_NOALLOC_MAX_ITERS 65536
+
+/* mfcfd_run without any device allocation.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory while they run
+ * (a host whose device memory belongs to its own pool, a loop being
+ * captured into a CUDA graph, a service that allocates only at start-up):
+ * mfcfd_run may grow its residue-history buffer with cudaMalloc and
+ * instantiates CUDA graphs; this call keeps the history in a fixed
+ * per-device array of MFCFD_NOALLOC_MAX_ITERS doubles (512 KiB, held by every
+ * GPU that loads the library until exit), launches the kernels directly and
+ * allocates nothing.  Same arguments, results and status codes as mfcfd_run;
+ * n_iters above MFCFD_NOALLOC_MAX_ITERS gives MFCFD_ERR_ARG.  The first call
+ * on a device looks up the array's device address: make it before any
+ * stream capture.  All calls on a device share the array, so calls that
+ * overlap on the GPU (handles on concurrent streams) race on it. */
+int mfcfd_run_noalloc(mfcfd_t *h, int it_first, int n_iters, double *residue, int *n_done);
 
 /* Runs iteration `it` with a CUDA event after every kernel on the handle's
  * stream and returns the mean duration per launch in ms of the gradient,

@@ -844,3 +844,115 @@ const char *mfcfd_last_error(mfcfd_t *h) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// mfcfd_run_noalloc: the pseudo-time loop without any device allocation.
+//
+// mfcfd_run keeps each call's residue history in a device buffer that it
+// grows with cudaMalloc when a call asks for more iterations than any call
+// before, and it instantiates CUDA graphs.  Callers that must not allocate
+// device memory once they are running -- a Fortran/OpenACC host whose device
+// memory belongs to its own pool, a loop that is being captured into a CUDA
+// graph (cudaMalloc cannot be captured), a time-critical service that
+// allocates only at start-up -- use this entry point instead.  It keeps the
+// history in the fixed array below, launches the same kernels directly, and
+// calls no cudaMalloc, cudaFree or graph instantiation.
+//
+// The array is a host-side stand-in in host code: its device address is
+// taken with cudaGetSymbolAddress once per device, with that device current,
+// on the first call made on that device.  Make that first call before any
+// stream capture.  Every call on a device shares the array: each iteration
+// writes its history entry before anything reads it, and calls that overlap
+// on the GPU (two handles on concurrent streams) race on it.
+namespace {
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+__device__ __align__(256) double g_noalloc_hist[MFCFD_NOALLOC_MAX_ITERS];
+double *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+
+int noalloc_setup(mfcfd_t *h, double **out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGetDevice");
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+        return fail(h, MFCFD_ERR_NODEV, "mfcfd_run_noalloc: device index out of range");
+    if (!g_noalloc_ptr[dev]) {
+        double *p = nullptr;
+        e = cudaGetSymbolAddress(reinterpret_cast<void **>(&p), g_noalloc_hist);
+        if (e != cudaSuccess) return cuda_fail(h, e, "cudaGetSymbolAddress(g_noalloc_hist)");
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return MFCFD_OK;
+}
+
+// One iteration, as enqueue_iteration, with the history written to `hist`.
+int noalloc_iteration(mfcfd_t *h, cudaStream_t s, double *hist) {
+    const int A = h->cur, B = h->cur ^ 1;
+    const int m = h->p.inner_iterations;
+    for (int rk = 1; rk <= h->p.rks; ++rk) {
+        const R4 *q_in = h->d_q[h->qcur];
+        R4 *q_out = h->d_q[h->qcur ^ 1];
+        launch_grad(h->geom, h->consts, q_in, h->d_spd, h->d_dq[0], h->d_qm, h->d_delta,
+                    rk == 1, h->d_ctl, s);
+        for (int t = 1; t <= m; ++t)
+            launch_inner(h->geom, h->consts, q_in, h->d_dq[(t - 1) & 1], h->d_dq[t & 1],
+                         h->d_ctl, s);
+        StageBufs b;
+        b.prim_in = rk == 1 ? h->d_prim[A] : h->d_prim[B];
+        b.prim_out = h->d_prim[B];
+        b.prim_old = h->d_prim[A];
+        b.q_in = q_in;
+        b.q_out = q_out;
+        b.dq = h->d_dq[m & 1];
+        b.qm = h->d_qm;
+        b.delta = h->d_delta;
+        b.spd = h->d_spd;
+        b.res_part = h->d_res_part;
+        b.flux_dbg = h->keep_diag ? h->d_flux_dbg : nullptr;
+        launch_flux(h->geom, h->consts, b, rk, rk == h->p.rks, h->d_ctl, s);
+        h->qcur ^= 1;
+        h->launches += 2 + m;
+    }
+    launch_residual(h->d_res_part, flux_blocks(h->n), h->d_ctl, hist, s);
+    h->launches += 1;
+    h->cur = B;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
+    return MFCFD_OK;
+}
+
+}  // namespace
+
+extern "C" int mfcfd_run_noalloc(mfcfd_t *h, int it_first, int n_iters, double *residue,
+                                 int *n_done) {
+    if (n_done) *n_done = 0;
+    if (!h || n_iters < 0) return MFCFD_ERR_ARG;
+    if (n_iters > MFCFD_NOALLOC_MAX_ITERS)
+        return fail(h, MFCFD_ERR_ARG,
+                    "mfcfd_run_noalloc: n_iters exceeds MFCFD_NOALLOC_MAX_ITERS (65536); "
+                    "split the run into several calls");
+    if (n_iters == 0) return MFCFD_OK;
+    double *hist = nullptr;
+    int st = noalloc_setup(h, &hist);
+    if (st) return st;
+    CK(cudaStreamSynchronize(h->stream));
+    h->h_ctl->it = it_first;
+    h->h_ctl->it_first = it_first;
+    h->h_ctl->halted = 0;
+    h->h_ctl->done = 0;
+    CK(cudaMemcpyAsync(h->d_ctl, h->h_ctl, 4 * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    for (int k = 0; k < n_iters; ++k) {
+        st = noalloc_iteration(h, h->stream, hist);
+        if (st) return st;
+    }
+    CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const int done = h->h_ctl->done;
+    if (residue && done > 0)
+        CK(cudaMemcpy(residue, hist, sizeof(double) * done, cudaMemcpyDeviceToHost));
+    if (n_done) *n_done = done;
+    h->iters_done_total += done;
+    if (h->h_ctl->halted) return fail(h, MFCFD_ERR_NONFINITE, "residue is NaN");
+    return MFCFD_OK;
+}
