@@ -210,6 +210,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "mfcfd":
         args.warmup = 3
@@ -267,6 +268,39 @@ def main():
         dist.barrier()
     clocks = clk.summary()
     value = world * grid.n * args.steps / (ms / 1e3) / 1e6
+    cl64, cd64, _, _ = solver.forces()
+    it64 = solver.it
+
+    # FP32-mixed: same grid, same number of iterations, device-timed the same way
+    fp32 = None
+    if not args.no_fp32:
+        s32 = Solver(grid, precision="fp32_mixed", **f)
+        s32.set_stream(stream.cuda_stream)
+        s32.run(args.warmup)
+        torch.cuda.synchronize()
+        f_start = torch.cuda.Event(enable_timing=True)
+        f_end = torch.cuda.Event(enable_timing=True)
+        f_start.record(stream)
+        s32.run(args.steps)
+        f_end.record(stream)
+        torch.cuda.synchronize()
+        ms32 = f_start.elapsed_time(f_end)
+        if dist:
+            t = torch.tensor([ms32], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms32 = float(t.item())
+        cl32, cd32, _, _ = s32.forces()
+        kt32 = s32.profile_iteration()
+        s32.close()
+        v32 = world * grid.n * args.steps / (ms32 / 1e3) / 1e6
+        fp32 = {"value": v32, "unit": UNIT, "ms_per_step": ms32 / args.steps,
+                "speedup_vs_fp64": v32 / value, "iterations": it64,
+                "dCl": abs(float(cl32[0] - cl64[0])), "dCd": abs(float(cd32[0] - cd64[0])),
+                "Cl_fp64": float(cl64[0]), "Cd_fp64": float(cd64[0]),
+                "kernel_ms": {k: float(v) for k, v in kt32.items()},
+                "note": "FP32 state and per-neighbour flux work, FP64 least squares, "
+                        "update, residual and forces; dCl/dCd against the FP64 run after "
+                        "the same iterations"}
 
     # per-kernel CUDA-event durations on the same stream (extra iterations)
     prof = [solver.profile_iteration() for _ in range(3)]
@@ -332,7 +366,7 @@ def main():
             "gpu_launches": launches, "clocks": clocks,
             "kernel_ms": kt, "iteration_roofline": iteration_roof,
             "final_residue": float(res[-1]) if len(res) else None,
-            "fp32_mixed": None,
+            "fp32_mixed": fp32,
         }
         print(json.dumps(line), flush=True)
     solver.close()

@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libmfcfd_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("primal_fp64.cu", "api.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("primal_fp64.cu", "primal_fp32.cu", "api.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in ("primal.h", "lskum_device.cuh")] + [
     os.path.join(ROOT, "include", "mfcfd_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -26,11 +26,25 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found: cannot build libmfcfd_b200.so")
 
 
-def command(out: str = LIB, extra=()) -> list:
-    # -ffp-contract=off: the host-side set-up (normals, split masks, limiter
-    # epsilon) must round exactly like the reference's arithmetic.
-    return [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-I", os.path.join(ROOT, "include"),
-            "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared", *extra, "-o", out, *SOURCES]
+# Per-file device flags: the FP32-mixed kernels use approximate FP32 division
+# and square root with denormals flushed (their FP64 parts are unaffected).
+FILE_FLAGS = {"primal_fp32.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"]}
+
+
+def commands(out: str = LIB, extra=(), file_flags=None) -> list:
+    """nvcc commands: one object per source (with its own flags), then the link.
+    -ffp-contract=off: the host-side set-up (normals, split masks, limiter
+    epsilon) must round exactly like the reference's arithmetic."""
+    ff = FILE_FLAGS if file_flags is None else file_flags
+    base = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-I", os.path.join(ROOT, "include"),
+            "-Xcompiler", "-fPIC,-ffp-contract=off", *extra]
+    objs, cmds = [], []
+    for src in SOURCES:
+        obj = out + "." + os.path.basename(src) + ".o"
+        cmds.append(base + ff.get(os.path.basename(src), []) + ["-c", "-o", obj, src])
+        objs.append(obj)
+    cmds.append([nvcc(), *ARCH, "-shared", "-o", out, *objs])
+    return cmds
 
 
 def up_to_date(out: str = LIB) -> bool:
@@ -40,19 +54,26 @@ def up_to_date(out: str = LIB) -> bool:
     return all(os.path.getmtime(s) <= t for s in SOURCES + HEADERS)
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
+def build(force: bool = False, verbose: bool = False, out: str = LIB, extra=(),
+          file_flags=None) -> str:
+    if out == LIB and not force and up_to_date():
         return LIB
-    cmd = command()
-    tmp = LIB + ".tmp"
-    cmd[cmd.index(LIB)] = tmp
-    res = subprocess.run(cmd, capture_output=True, text=True)
-    if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
-    if verbose and res.stderr:
-        print(res.stderr, file=sys.stderr)
-    os.replace(tmp, LIB)
-    return LIB
+    tmp = out + ".tmp"
+    cmds = commands(tmp, extra, file_flags)
+    try:
+        for cmd in cmds:
+            res = subprocess.run(cmd, capture_output=True, text=True)
+            if res.returncode != 0:
+                raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + res.stdout + res.stderr)
+            if verbose and res.stderr:
+                print(res.stderr, file=sys.stderr)
+        os.replace(tmp, out)
+    finally:
+        for cmd in cmds[:-1]:
+            obj = cmd[cmd.index("-o") + 1]
+            if os.path.exists(obj):
+                os.remove(obj)
+    return out
 
 
 if __name__ == "__main__":

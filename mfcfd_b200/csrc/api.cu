@@ -65,6 +65,11 @@ struct mfcfd {
     int *d_sh_idx = nullptr, *d_sh_shape = nullptr;
     double *d_sh_geo = nullptr, *d_sh_my = nullptr;
     double *h_stage = nullptr;  // pinned staging [n][4]
+    // FP32-mixed state (precision == MFCFD_FP32_MIXED)
+    bool fp32 = false;
+    float4 *f_prim[2] = {nullptr, nullptr}, *f_q[2] = {nullptr, nullptr};
+    float *f_dq[2] = {nullptr, nullptr};
+    float *f_qm = nullptr, *f_eps2 = nullptr;
 
     int cur = 0;   // prim buffer holding the state
     int qcur = 0;  // q buffer holding q of the state
@@ -104,7 +109,8 @@ void free_all(mfcfd_t *h) {
                     h->d_my, h->d_prim[0], h->d_prim[1], h->d_q[0], h->d_q[1], h->d_dq[0],
                     h->d_dq[1], h->d_qm, h->d_delta, h->d_spd, h->d_res_part, h->d_flux_dbg,
                     h->d_hist, h->d_forces, h->d_ctl, h->d_sh_idx, h->d_sh_shape, h->d_sh_geo,
-                    h->d_sh_my};
+                    h->d_sh_my, h->f_prim[0], h->f_prim[1], h->f_q[0], h->f_q[1],
+                    h->f_dq[0], h->f_dq[1], h->f_qm, h->f_eps2};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (h->h_ctl) cudaFreeHost(h->h_ctl);
@@ -144,40 +150,79 @@ std::vector<int> rcm_order(int n, const std::vector<std::vector<int>> &adj) {
     return order;
 }
 
-int enqueue_iteration(mfcfd_t *h, cudaStream_t s) {
-    const int A = h->cur, B = h->cur ^ 1;
+// Launches the kernels of pseudo-time stage rk (prim buffers A -> B) and
+// calls `after` once after each launch.
+template <class F>
+void launch_stage(mfcfd_t *h, cudaStream_t s, int rk, int A, int B, F after) {
     const int m = h->p.inner_iterations;
-    for (int rk = 1; rk <= h->p.rks; ++rk) {
+    const bool last = rk == h->p.rks;
+    if (!h->fp32) {
         const R4 *q_in = h->d_q[h->qcur];
-        R4 *q_out = h->d_q[h->qcur ^ 1];
         launch_grad(h->geom, h->consts, q_in, h->d_spd, h->d_dq[0], h->d_qm, h->d_delta,
                     rk == 1, h->d_ctl, s);
-        for (int t = 1; t <= m; ++t)
+        after();
+        for (int t = 1; t <= m; ++t) {
             launch_inner(h->geom, h->consts, q_in, h->d_dq[(t - 1) & 1], h->d_dq[t & 1],
                          h->d_ctl, s);
+            after();
+        }
         StageBufs b;
         b.prim_in = rk == 1 ? h->d_prim[A] : h->d_prim[B];
         b.prim_out = h->d_prim[B];
         b.prim_old = h->d_prim[A];
         b.q_in = q_in;
-        b.q_out = q_out;
+        b.q_out = h->d_q[h->qcur ^ 1];
         b.dq = h->d_dq[m & 1];
         b.qm = h->d_qm;
         b.delta = h->d_delta;
         b.spd = h->d_spd;
         b.res_part = h->d_res_part;
         b.flux_dbg = h->keep_diag ? h->d_flux_dbg : nullptr;
-        launch_flux(h->geom, h->consts, b, rk, rk == h->p.rks, h->d_ctl, s);
-        h->qcur ^= 1;
-        h->launches += 2 + m;
+        launch_flux(h->geom, h->consts, b, rk, last, h->d_ctl, s);
+        after();
+    } else {
+        const float4 *q_in = h->f_q[h->qcur];
+        launch_grad32(h->geom, h->consts, q_in, h->d_spd, h->f_dq[0], h->f_qm, h->d_delta,
+                      rk == 1, h->d_ctl, s);
+        after();
+        for (int t = 1; t <= m; ++t) {
+            launch_inner32(h->geom, h->consts, q_in, h->f_dq[(t - 1) & 1], h->f_dq[t & 1],
+                           h->d_ctl, s);
+            after();
+        }
+        StageBufs32 b;
+        b.prim_in = rk == 1 ? h->f_prim[A] : h->f_prim[B];
+        b.prim_out = h->f_prim[B];
+        b.prim_old = h->f_prim[A];
+        b.q_in = q_in;
+        b.q_out = h->f_q[h->qcur ^ 1];
+        b.dq = h->f_dq[m & 1];
+        b.qm = h->f_qm;
+        b.eps2f = h->f_eps2;
+        b.delta = h->d_delta;
+        b.spd = h->d_spd;
+        b.res_part = h->d_res_part;
+        b.flux_dbg = h->keep_diag ? h->d_flux_dbg : nullptr;
+        launch_flux32(h->geom, h->consts, b, rk, last, h->d_ctl, s);
+        after();
     }
-    launch_residual(h->d_res_part, flux_blocks(h->n), h->d_ctl, h->d_hist, s);
+    h->qcur ^= 1;
+    h->launches += 2 + m;
+}
+
+// One iteration (fpi_solver): the stages, then the residual into hist.
+int enqueue_iteration_to(mfcfd_t *h, cudaStream_t s, double *hist) {
+    const int A = h->cur, B = h->cur ^ 1;
+    for (int rk = 1; rk <= h->p.rks; ++rk) launch_stage(h, s, rk, A, B, [] {});
+    launch_residual(h->d_res_part, flux_blocks(h->n), h->d_ctl, hist, s);
     h->launches += 1;
     h->cur = B;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
     return MFCFD_OK;
 }
+
+int enqueue_iteration(mfcfd_t *h, cudaStream_t s) { return enqueue_iteration_to(h, s, h->d_hist); }
 
 // Captures two consecutive iterations into one graph.  After two iterations
 // both the prim and the q buffer parity are back where they started.
@@ -215,7 +260,10 @@ int build_pair_graph(mfcfd_t *h) {
 }
 
 int upload_state_aux(mfcfd_t *h) {
-    launch_init_state(h->geom, h->d_prim[h->cur], h->d_q[h->qcur], h->d_spd, h->stream);
+    if (h->fp32)
+        launch_init_state32(h->geom, h->f_prim[h->cur], h->f_q[h->qcur], h->d_spd, h->stream);
+    else
+        launch_init_state(h->geom, h->d_prim[h->cur], h->d_q[h->qcur], h->d_spd, h->stream);
     h->launches += 1;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(h, e, "init_state launch");
@@ -269,8 +317,6 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
         return fail(nullptr, MFCFD_ERR_ARG, "params: cfl must be > 0 and all finite");
     if (P.precision != MFCFD_FP64 && P.precision != MFCFD_FP32_MIXED)
         return fail(nullptr, MFCFD_ERR_ARG, "params.precision unknown");
-    if (P.precision == MFCFD_FP32_MIXED)
-        return fail(nullptr, MFCFD_ERR_ARG, "params.precision FP32_MIXED is not built in this library");
     if (P.ordering != MFCFD_ORDER_KIND && P.ordering != MFCFD_ORDER_RCM)
         return fail(nullptr, MFCFD_ERR_ARG, "params.ordering unknown");
 
@@ -370,6 +416,7 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
         return fail(nullptr, MFCFD_ERR_NODEV, "no CUDA device");
     {
         cudaError_t e = init_kernels();
+        if (e == cudaSuccess) e = init_kernels32();
         if (e != cudaSuccess) return fail(nullptr, MFCFD_ERR_CUDA, cudaGetErrorString(e));
     }
     h = new (std::nothrow) mfcfd();
@@ -381,6 +428,7 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
     h->nint = n - nw - no;
     h->shapes = G.shapes;
     h->p = P;
+    h->fp32 = P.precision == MFCFD_FP32_MIXED;
     cudaGetDevice(&h->dev);
     h->pi = pi;
     h->theta = theta;
@@ -499,12 +547,23 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
     ALLOC(h->d_nbhs, n);
     ALLOC(h->d_mx, n);
     ALLOC(h->d_my, n);
-    for (int b = 0; b < 2; ++b) {
-        ALLOC(h->d_prim[b], n);
-        ALLOC(h->d_q[b], n);
-        ALLOC(h->d_dq[b], (size_t)8 * n);
+    if (!h->fp32) {
+        for (int b = 0; b < 2; ++b) {
+            ALLOC(h->d_prim[b], n);
+            ALLOC(h->d_q[b], n);
+            ALLOC(h->d_dq[b], (size_t)8 * n);
+        }
+        ALLOC(h->d_qm, (size_t)8 * n);
+    } else {
+        ALLOC(h->d_prim[0], n);  // FP64 copy of the state for forces/diagnostics
+        for (int b = 0; b < 2; ++b) {
+            ALLOC(h->f_prim[b], n);
+            ALLOC(h->f_q[b], n);
+            ALLOC(h->f_dq[b], (size_t)8 * n);
+        }
+        ALLOC(h->f_qm, (size_t)8 * n);
+        ALLOC(h->f_eps2, n);
     }
-    ALLOC(h->d_qm, (size_t)8 * n);
     ALLOC(h->d_delta, n);
     ALLOC(h->d_spd, n);
     ALLOC(h->d_res_part, flux_blocks(n));
@@ -527,6 +586,10 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
         (st = up(h->d_obc, hobc)) || (st = up(h->d_conn, hconn)) || (st = up(h->d_nbhs, hnb)) ||
         (st = up(h->d_mx, hmx)) || (st = up(h->d_my, hmy)))
         goto fail_create;
+    if (h->fp32) {
+        std::vector<float> feps(heps.begin(), heps.end());
+        if ((st = up(h->f_eps2, feps))) goto fail_create;
+    }
     if (h->nshape > 0) {
         if ((st = up(h->d_sh_idx, sidx)) || (st = up(h->d_sh_shape, sshape)) ||
             (st = up(h->d_sh_geo, sgeo)) || (st = up(h->d_sh_my, smy)))
@@ -557,11 +620,19 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
         }
     }
     // initial_conditions.F90:9-20: freestream everywhere
-    for (int p = 0; p < n; ++p)
-        for (int c = 0; c < 4; ++c) h->h_stage[4 * (size_t)p + c] = h->q_inf[c];
     {
-        cudaError_t e = cudaMemcpy(h->d_prim[0], h->h_stage, sizeof(double) * 4 * (size_t)n,
-                                   cudaMemcpyHostToDevice);
+        cudaError_t e;
+        if (!h->fp32) {
+            for (int p = 0; p < n; ++p)
+                for (int c = 0; c < 4; ++c) h->h_stage[4 * (size_t)p + c] = h->q_inf[c];
+            e = cudaMemcpy(h->d_prim[0], h->h_stage, sizeof(double) * 4 * (size_t)n,
+                           cudaMemcpyHostToDevice);
+        } else {
+            float *fs = reinterpret_cast<float *>(h->h_stage);
+            for (int p = 0; p < n; ++p)
+                for (int c = 0; c < 4; ++c) fs[4 * (size_t)p + c] = (float)h->q_inf[c];
+            e = cudaMemcpy(h->f_prim[0], fs, sizeof(float) * 4 * (size_t)n, cudaMemcpyHostToDevice);
+        }
         if (e != cudaSuccess) {
             st = cuda_fail(h, e, "cudaMemcpy prim");
             goto fail_create;
@@ -602,13 +673,25 @@ int mfcfd_set_stream(mfcfd_t *h, void *stream) {
 int mfcfd_set_state(mfcfd_t *h, const double *prim) {
     if (!h || !prim) return MFCFD_ERR_ARG;
     CK(cudaStreamSynchronize(h->stream));
-    for (int p = 0; p < h->n; ++p) {
-        const double *src = prim + 4 * (size_t)h->perm[p];
-        double *dst = h->h_stage + 4 * (size_t)p;
-        dst[0] = src[0]; dst[1] = src[1]; dst[2] = src[2]; dst[3] = src[3];
+    if (h->fp32) {
+        float *fs = reinterpret_cast<float *>(h->h_stage);
+        for (int p = 0; p < h->n; ++p) {
+            const double *src = prim + 4 * (size_t)h->perm[p];
+            float *dst = fs + 4 * (size_t)p;
+            dst[0] = (float)src[0]; dst[1] = (float)src[1]; dst[2] = (float)src[2];
+            dst[3] = (float)src[3];
+        }
+        CK(cudaMemcpyAsync(h->f_prim[h->cur], fs, sizeof(float) * 4 * (size_t)h->n,
+                           cudaMemcpyHostToDevice, h->stream));
+    } else {
+        for (int p = 0; p < h->n; ++p) {
+            const double *src = prim + 4 * (size_t)h->perm[p];
+            double *dst = h->h_stage + 4 * (size_t)p;
+            dst[0] = src[0]; dst[1] = src[1]; dst[2] = src[2]; dst[3] = src[3];
+        }
+        CK(cudaMemcpyAsync(h->d_prim[h->cur], h->h_stage, sizeof(double) * 4 * (size_t)h->n,
+                           cudaMemcpyHostToDevice, h->stream));
     }
-    CK(cudaMemcpyAsync(h->d_prim[h->cur], h->h_stage, sizeof(double) * 4 * (size_t)h->n,
-                       cudaMemcpyHostToDevice, h->stream));
     int st = upload_state_aux(h);
     if (st) return st;
     CK(cudaStreamSynchronize(h->stream));
@@ -617,6 +700,18 @@ int mfcfd_set_state(mfcfd_t *h, const double *prim) {
 
 int mfcfd_get_state(mfcfd_t *h, double *prim) {
     if (!h || !prim) return MFCFD_ERR_ARG;
+    if (h->fp32) {
+        float *fs = reinterpret_cast<float *>(h->h_stage);
+        CK(cudaMemcpyAsync(fs, h->f_prim[h->cur], sizeof(float) * 4 * (size_t)h->n,
+                           cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        for (int p = 0; p < h->n; ++p) {
+            const float *src = fs + 4 * (size_t)p;
+            double *dst = prim + 4 * (size_t)h->perm[p];
+            dst[0] = src[0]; dst[1] = src[1]; dst[2] = src[2]; dst[3] = src[3];
+        }
+        return MFCFD_OK;
+    }
     CK(cudaMemcpyAsync(h->h_stage, h->d_prim[h->cur], sizeof(double) * 4 * (size_t)h->n,
                        cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
@@ -678,8 +773,13 @@ int mfcfd_run(mfcfd_t *h, int it_first, int n_iters, double *residue, int *n_don
 
 int mfcfd_forces(mfcfd_t *h, double *cl, double *cd, double *cm, double *cp) {
     if (!h) return MFCFD_ERR_ARG;
-    launch_forces(h->shape, h->d_prim[h->cur], h->p.mach, h->cos_t, h->sin_t, h->d_forces,
-                  h->stream);
+    const R4 *prim = h->d_prim[h->cur];
+    if (h->fp32) {
+        launch_widen(h->f_prim[h->cur], h->d_prim[0], h->n, h->stream);
+        h->launches += 1;
+        prim = h->d_prim[0];
+    }
+    launch_forces(h->shape, prim, h->p.mach, h->cos_t, h->sin_t, h->d_forces, h->stream);
     h->launches += 1;
     CK(cudaGetLastError());
     std::vector<double> o(3 * h->shapes + h->nshape);
@@ -710,6 +810,24 @@ int mfcfd_get_array(mfcfd_t *h, const char *name, double *out) {
     const double *src = nullptr;
     int w = 0;
     std::string s(name);
+    const float *fsrc = nullptr;
+    if (h->fp32) {
+        if (s == "q") { fsrc = reinterpret_cast<const float *>(h->f_q[h->qcur ^ 1]); w = 4; }
+        else if (s == "dq") { fsrc = h->f_dq[h->p.inner_iterations & 1]; w = 8; }
+        else if (s == "qm") { fsrc = h->f_qm; w = 8; }
+    }
+    if (fsrc) {
+        std::vector<float> ft((size_t)w * h->n);
+        CK(cudaMemcpyAsync(ft.data(), fsrc, ft.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                           h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        for (int p = 0; p < h->n; ++p)
+            for (int c = 0; c < w; ++c) {
+                int cc = w == 8 ? (c % 4) * 2 + c / 4 : c;
+                out[(size_t)w * h->perm[p] + cc] = ft[(size_t)w * p + c];
+            }
+        return MFCFD_OK;
+    }
     if (s == "q") { src = reinterpret_cast<const double *>(h->d_q[h->qcur ^ 1]); w = 4; }
     else if (s == "dq") { src = h->d_dq[h->p.inner_iterations & 1]; w = 8; }
     else if (s == "qm") { src = h->d_qm; w = 8; }
@@ -770,35 +888,11 @@ int mfcfd_profile_iteration(mfcfd_t *h, int it, double *ms) {
     const int A = h->cur, B = h->cur ^ 1;
     int e = 0;
     CK(cudaEventRecord(ev[e++], h->stream));
-    for (int rk = 1; rk <= h->p.rks; ++rk) {
-        const R4 *q_in = h->d_q[h->qcur];
-        launch_grad(h->geom, h->consts, q_in, h->d_spd, h->d_dq[0], h->d_qm, h->d_delta,
-                    rk == 1, h->d_ctl, h->stream);
-        CK(cudaEventRecord(ev[e++], h->stream));
-        for (int t = 1; t <= m; ++t) {
-            launch_inner(h->geom, h->consts, q_in, h->d_dq[(t - 1) & 1], h->d_dq[t & 1],
-                         h->d_ctl, h->stream);
-            CK(cudaEventRecord(ev[e++], h->stream));
-        }
-        StageBufs b;
-        b.prim_in = rk == 1 ? h->d_prim[A] : h->d_prim[B];
-        b.prim_out = h->d_prim[B];
-        b.prim_old = h->d_prim[A];
-        b.q_in = q_in;
-        b.q_out = h->d_q[h->qcur ^ 1];
-        b.dq = h->d_dq[m & 1];
-        b.qm = h->d_qm;
-        b.delta = h->d_delta;
-        b.spd = h->d_spd;
-        b.res_part = h->d_res_part;
-        b.flux_dbg = h->keep_diag ? h->d_flux_dbg : nullptr;
-        launch_flux(h->geom, h->consts, b, rk, rk == h->p.rks, h->d_ctl, h->stream);
-        CK(cudaEventRecord(ev[e++], h->stream));
-        h->qcur ^= 1;
-    }
+    for (int rk = 1; rk <= h->p.rks; ++rk)
+        launch_stage(h, h->stream, rk, A, B, [&] { cudaEventRecord(ev[e++], h->stream); });
     launch_residual(h->d_res_part, flux_blocks(h->n), h->d_ctl, h->d_hist, h->stream);
     CK(cudaEventRecord(ev[e++], h->stream));
-    h->launches += nev - 1;
+    h->launches += 1;
     h->cur = B;
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->stream));
@@ -886,40 +980,9 @@ int noalloc_setup(mfcfd_t *h, double **out) {
     return MFCFD_OK;
 }
 
-// One iteration, as enqueue_iteration, with the history written to `hist`.
+// One iteration, as mfcfd_run enqueues it, with the history written to `hist`.
 int noalloc_iteration(mfcfd_t *h, cudaStream_t s, double *hist) {
-    const int A = h->cur, B = h->cur ^ 1;
-    const int m = h->p.inner_iterations;
-    for (int rk = 1; rk <= h->p.rks; ++rk) {
-        const R4 *q_in = h->d_q[h->qcur];
-        R4 *q_out = h->d_q[h->qcur ^ 1];
-        launch_grad(h->geom, h->consts, q_in, h->d_spd, h->d_dq[0], h->d_qm, h->d_delta,
-                    rk == 1, h->d_ctl, s);
-        for (int t = 1; t <= m; ++t)
-            launch_inner(h->geom, h->consts, q_in, h->d_dq[(t - 1) & 1], h->d_dq[t & 1],
-                         h->d_ctl, s);
-        StageBufs b;
-        b.prim_in = rk == 1 ? h->d_prim[A] : h->d_prim[B];
-        b.prim_out = h->d_prim[B];
-        b.prim_old = h->d_prim[A];
-        b.q_in = q_in;
-        b.q_out = q_out;
-        b.dq = h->d_dq[m & 1];
-        b.qm = h->d_qm;
-        b.delta = h->d_delta;
-        b.spd = h->d_spd;
-        b.res_part = h->d_res_part;
-        b.flux_dbg = h->keep_diag ? h->d_flux_dbg : nullptr;
-        launch_flux(h->geom, h->consts, b, rk, rk == h->p.rks, h->d_ctl, s);
-        h->qcur ^= 1;
-        h->launches += 2 + m;
-    }
-    launch_residual(h->d_res_part, flux_blocks(h->n), h->d_ctl, hist, s);
-    h->launches += 1;
-    h->cur = B;
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
-    return MFCFD_OK;
+    return enqueue_iteration_to(h, s, hist);
 }
 
 }  // namespace

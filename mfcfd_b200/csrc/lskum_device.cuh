@@ -65,32 +65,34 @@ __device__ __forceinline__ void q_from_prim(double rho, double u1, double u2, do
     q[3] = -two_times_beta;
 }
 
-// q_variables.F90:230-256 qtilde_to_primitive
-__device__ __forceinline__ void qtilde_to_primitive(const double qt[4], double gm1, double &u1,
-                                                    double &u2, double &rho, double &pr) {
-    double beta = -qt[3] * 0.5;
-    double temp = 0.5 / beta;
+// q_variables.F90:230-256 qtilde_to_primitive.  T is double on the FP64
+// path and float on the FP32-mixed path; the literals keep their values.
+template <class T>
+__device__ __forceinline__ void qtilde_to_primitive(const T qt[4], T gm1, T &u1, T &u2, T &rho,
+                                                    T &pr) {
+    T beta = -qt[3] * T(0.5);
+    T temp = T(0.5) / beta;
     u1 = qt[1] * temp;
     u2 = qt[2] * temp;
-    double temp1 = qt[0] + beta * (u1 * u1 + u2 * u2);
-    double temp2 = temp1 - (log(beta) / gm1);
+    T temp1 = qt[0] + beta * (u1 * u1 + u2 * u2);
+    T temp2 = temp1 - (log(beta) / gm1);
     rho = exp(temp2);
     pr = rho * temp;
 }
 
 // limiters.F90:64-110 venkat_limiter, one component.
-__device__ __forceinline__ double venkat_phi(double qtilde, double q, double qmax, double qmin,
-                                             double eps2) {
-    double del_neg = qtilde - q;
-    if (fabs(del_neg) <= MFCFD_VENKAT_THR) return 1.0;
-    double del_pos = del_neg > 0.0 ? qmax - q : qmin - q;
-    double num = (del_pos * del_pos) + eps2;
-    num = num * del_neg + 2.0 * del_neg * del_neg * del_pos;
-    double den = del_pos * del_pos + 2.0 * del_neg * del_neg;
+template <class T>
+__device__ __forceinline__ T venkat_phi(T qtilde, T q, T qmax, T qmin, T eps2) {
+    T del_neg = qtilde - q;
+    if (fabs(del_neg) <= T(MFCFD_VENKAT_THR)) return T(1.0);
+    T del_pos = del_neg > T(0.0) ? qmax - q : qmin - q;
+    T num = (del_pos * del_pos) + eps2;
+    num = num * del_neg + T(2.0) * del_neg * del_neg * del_pos;
+    T den = del_pos * del_pos + T(2.0) * del_neg * del_neg;
     den = den + del_neg * del_pos + eps2;
     den = den * del_neg;
-    double temp = num / den;
-    return temp < 1.0 ? temp : 1.0;
+    T temp = num / den;
+    return temp < T(1.0) ? temp : T(1.0);
 }
 
 // Limited reconstruction of one point towards one neighbour direction,
@@ -98,40 +100,41 @@ __device__ __forceinline__ double venkat_phi(double qtilde, double q, double qma
 // interior_fluxes.F90:158-172).  t = delx*dq(1,:) + dely*dq(2,:) is formed
 // once and used for both the unlimited and the limited qtilde, exactly as the
 // reference recomputes it.
-__device__ __forceinline__ void reconstruct(const double q[4], const double dqx[4],
-                                            const double dqy[4], const double qmax[4],
-                                            const double qmin[4], double eps2, double delx,
-                                            double dely, double gm1, double &u1, double &u2,
-                                            double &rho, double &pr) {
-    double qt[4];
+template <class T>
+__device__ __forceinline__ void reconstruct(const T q[4], const T dqx[4], const T dqy[4],
+                                            const T qmax[4], const T qmin[4], T eps2, T delx,
+                                            T dely, T gm1, T &u1, T &u2, T &rho, T &pr) {
+    T qt[4];
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        double t = delx * dqx[r] + dely * dqy[r];
-        double phi = venkat_phi(q[r] - 0.5 * t, q[r], qmax[r], qmin[r], eps2);
-        qt[r] = q[r] - 0.5 * phi * t;
+        T t = delx * dqx[r] + dely * dqy[r];
+        T phi = venkat_phi<T>(q[r] - T(0.5) * t, q[r], qmax[r], qmin[r], eps2);
+        qt[r] = q[r] - T(0.5) * phi * t;
     }
-    qtilde_to_primitive(qt, gm1, u1, u2, rho, pr);
+    qtilde_to_primitive<T>(qt, gm1, u1, u2, rho, pr);
 }
 
 // The per-state part shared by split_fluxes.F90 and quadrant_fluxes.F90: the
 // state in the point's (t, n) frame and the two Maxwellian half-moments.
-struct KState {
-    double rho, ut, un, pbr, usq, B1, B2, e1, e2;
+template <class T>
+struct KStateT {
+    T rho, ut, un, pbr, usq, B1, B2, e1, e2;
 };
+using KState = KStateT<double>;
 
-__device__ __forceinline__ KState kstate(double u1, double u2, double rho, double pr, double nx,
-                                         double ny, double pi) {
-    KState s;
-    double tx = ny, ty = -nx;
+template <class T>
+__device__ __forceinline__ KStateT<T> kstate(T u1, T u2, T rho, T pr, T nx, T ny, T pi) {
+    KStateT<T> s;
+    T tx = ny, ty = -nx;
     s.ut = u1 * tx + u2 * ty;
     s.un = u1 * nx + u2 * ny;
-    double beta = 0.5 * rho / pr;
-    double sb = sqrt(beta);
-    double S1 = s.ut * sb;
-    double S2 = s.un * sb;
-    double spb = sqrt(pi * beta);
-    s.B1 = 0.5 * exp(-S1 * S1) / spb;
-    s.B2 = 0.5 * exp(-S2 * S2) / spb;
+    T beta = T(0.5) * rho / pr;
+    T sb = sqrt(beta);
+    T S1 = s.ut * sb;
+    T S2 = s.un * sb;
+    T spb = sqrt(pi * beta);
+    s.B1 = T(0.5) * exp(-S1 * S1) / spb;
+    s.B2 = T(0.5) * exp(-S2 * S2) / spb;
     s.e1 = erf(S1);
     s.e2 = erf(S2);
     s.pbr = pr / rho;
@@ -141,53 +144,56 @@ __device__ __forceinline__ KState kstate(double u1, double u2, double rho, doubl
 }
 
 // split_fluxes.F90:8-96 flux_Gxp (s1 = +1) / flux_Gxn (s1 = -1)
-__device__ __forceinline__ void flux_gx(const KState &s, double s1, double G[4]) {
-    double A1 = 0.5 * (1.0 + s1 * s.e1);
+template <class T>
+__device__ __forceinline__ void flux_gx(const KStateT<T> &s, T s1, T G[4]) {
+    T A1 = T(0.5) * (T(1.0) + s1 * s.e1);
     G[0] = s.rho * (s.ut * A1 + s1 * s.B1);
-    double temp1 = s.pbr + s.ut * s.ut;
-    double temp2 = temp1 * A1 + s1 * (s.ut * s.B1);
+    T temp1 = s.pbr + s.ut * s.ut;
+    T temp2 = temp1 * A1 + s1 * (s.ut * s.B1);
     G[1] = s.rho * temp2;
     temp1 = s.ut * s.un * A1 + s1 * (s.un * s.B1);
     G[2] = s.rho * temp1;
-    temp1 = (7.0 * s.pbr) + s.usq;
-    temp2 = 0.5 * s.ut * temp1 * A1;
-    temp1 = (6.0 * s.pbr) + s.usq;
-    G[3] = s.rho * (temp2 + s1 * (0.5 * temp1 * s.B1));
+    temp1 = (T(7.0) * s.pbr) + s.usq;
+    temp2 = T(0.5) * s.ut * temp1 * A1;
+    temp1 = (T(6.0) * s.pbr) + s.usq;
+    G[3] = s.rho * (temp2 + s1 * (T(0.5) * temp1 * s.B1));
 }
 
 // split_fluxes.F90:99-190 flux_Gyp (s2 = +1) / flux_Gyn (s2 = -1)
-__device__ __forceinline__ void flux_gy(const KState &s, double s2, double G[4]) {
-    double A2 = 0.5 * (1.0 + s2 * s.e2);
+template <class T>
+__device__ __forceinline__ void flux_gy(const KStateT<T> &s, T s2, T G[4]) {
+    T A2 = T(0.5) * (T(1.0) + s2 * s.e2);
     G[0] = s.rho * (s.un * A2 + s2 * s.B2);
-    double temp1 = s.pbr + s.un * s.un;
-    double temp2 = temp1 * A2 + s2 * (s.un * s.B2);
+    T temp1 = s.pbr + s.un * s.un;
+    T temp2 = temp1 * A2 + s2 * (s.un * s.B2);
     G[2] = s.rho * temp2;
     temp1 = s.ut * s.un * A2 + s2 * (s.ut * s.B2);
     G[1] = s.rho * temp1;
-    temp1 = (7.0 * s.pbr) + s.usq;
-    temp2 = 0.5 * s.un * temp1 * A2;
-    temp1 = (6.0 * s.pbr) + s.usq;
-    G[3] = s.rho * (temp2 + s2 * (0.5 * temp1 * s.B2));
+    temp1 = (T(7.0) * s.pbr) + s.usq;
+    temp2 = T(0.5) * s.un * temp1 * A2;
+    temp1 = (T(6.0) * s.pbr) + s.usq;
+    G[3] = s.rho * (temp2 + s2 * (T(0.5) * temp1 * s.B2));
 }
 
 // quadrant_fluxes.F90:12-248: GxI (s1=-1,s2=-1), GxII (+1,-1), GxIII (+1,+1),
 // GxIV (-1,+1).
-__device__ __forceinline__ void flux_quad(const KState &s, double s1, double s2, double G[4]) {
-    double A1 = 0.5 * (1.0 + s1 * s.e1);
-    double A2 = 0.5 * (1.0 + s2 * s.e2);
-    double rA2 = s.rho * A2;
-    double a1b = s.ut * A1 + s1 * s.B1;
+template <class T>
+__device__ __forceinline__ void flux_quad(const KStateT<T> &s, T s1, T s2, T G[4]) {
+    T A1 = T(0.5) * (T(1.0) + s1 * s.e1);
+    T A2 = T(0.5) * (T(1.0) + s2 * s.e2);
+    T rA2 = s.rho * A2;
+    T a1b = s.ut * A1 + s1 * s.B1;
     G[0] = rA2 * a1b;
-    double temp1 = s.pbr + s.ut * s.ut;
-    double temp2 = temp1 * A1 + s1 * (s.ut * s.B1);
+    T temp1 = s.pbr + s.ut * s.ut;
+    T temp2 = temp1 * A1 + s1 * (s.ut * s.B1);
     G[1] = rA2 * temp2;
     temp2 = s.un * A2 + s2 * s.B2;
     G[2] = s.rho * a1b * temp2;
-    temp1 = (7.0 * s.pbr) + s.usq;
-    temp2 = 0.5 * s.ut * temp1 * A1;
-    temp1 = (6.0 * s.pbr) + s.usq;
-    double temp3 = 0.5 * s.B1 * temp1;
-    double temp4 = 0.5 * s.rho * s.un * s.B2 * a1b;
+    temp1 = (T(7.0) * s.pbr) + s.usq;
+    temp2 = T(0.5) * s.ut * temp1 * A1;
+    temp1 = (T(6.0) * s.pbr) + s.usq;
+    T temp3 = T(0.5) * s.B1 * temp1;
+    T temp4 = T(0.5) * s.rho * s.un * s.B2 * a1b;
     G[3] = rA2 * (temp2 + s1 * temp3) + s2 * temp4;
 }
 

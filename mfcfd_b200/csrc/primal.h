@@ -52,6 +52,33 @@ void launch_residual(const double *res_part, int nparts, Ctl *ctl, double *hist,
 // q and spd from prim (set_state)
 void launch_init_state(const Geom &g, const R4 *prim, R4 *q, double *spd, cudaStream_t s);
 
+// FP32-mixed stage buffers: FP32 prim/q/dq/qm, FP64 delta/spd/partials.
+struct StageBufs32 {
+    const float4 *prim_in;
+    float4 *prim_out;
+    const float4 *prim_old;
+    const float4 *q_in;
+    float4 *q_out;
+    const float *dq;     // [n][8]
+    const float *qm;     // [n][8]
+    const float *eps2f;  // eps2 rounded to FP32
+    const double *delta;
+    double *spd;
+    double *res_part;
+    double *flux_dbg;
+};
+cudaError_t init_kernels32();
+void launch_grad32(const Geom &g, const Consts &c, const float4 *q, const double *spd, float *dq,
+                   float *qm, double *delta, bool with_delta, const Ctl *ctl, cudaStream_t s);
+void launch_inner32(const Geom &g, const Consts &c, const float4 *q, const float *dq_in,
+                    float *dq_out, const Ctl *ctl, cudaStream_t s);
+void launch_flux32(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, bool last,
+                   const Ctl *ctl, cudaStream_t s);
+void launch_init_state32(const Geom &g, const float4 *prim, float4 *q, double *spd,
+                         cudaStream_t s);
+// float4 prim -> FP64 rows (for the force sums and diagnostics)
+void launch_widen(const float4 *in, R4 *out, int n, cudaStream_t s);
+
 // Shape-point force sums (compute_cl_cd_cm), serial in grid order.
 struct ShapeTab {
     int npts, shapes;

@@ -1,0 +1,416 @@
+// FP32-mixed kernels of the LSKUM pseudo-time loop on sm_100a.
+//
+// Stored per point in FP32: prim, q, dq, qm (half the FP64 gather traffic).
+// Computed in FP32: the per-neighbour work of the flux pass -- limiter,
+// qtilde -> primitive (log, exp), the Maxwellian moments (exp, erf, sqrt)
+// and the split fluxes -- with the flux contributions summed by compensated
+// (Kahan) FP32 addition in slot order.  Kept in FP64: coordinates and every
+// 2x2 least-squares normal equation (ill-conditioned on stretched near-wall
+// stencils), the sums of the q-derivative passes, the state update, the
+// residual norm and the force coefficients.
+#include <cuda_runtime.h>
+
+#include "primal.h"
+
+namespace lskum {
+
+namespace {
+
+constexpr int GRAD_BLOCK = 256;
+constexpr int LPP = 8;
+constexpr int FLUX_BLOCK = 128;
+constexpr int GROUPS = FLUX_BLOCK / LPP;
+constexpr int FREC = 11;  // dGxp..dGyn as 16 floats (8 doubles of storage), dels deln w
+#ifndef FLUX32_MIN_BLOCKS
+#define FLUX32_MIN_BLOCKS 5
+#endif
+constexpr double OBT = 1.0 / 3.0;
+constexpr double TBT = 2.0 / 3.0;
+
+__device__ __forceinline__ void ldf8(const float *p, float a[4], float b[4]) {
+    const float4 *v = reinterpret_cast<const float4 *>(p);
+    float4 x = __ldg(v), y = __ldg(v + 1);
+    a[0] = x.x; a[1] = x.y; a[2] = x.z; a[3] = x.w;
+    b[0] = y.x; b[1] = y.y; b[2] = y.z; b[3] = y.w;
+}
+
+__device__ __forceinline__ void stf8(float *p, const double a[4], const double b[4]) {
+    float4 *v = reinterpret_cast<float4 *>(p);
+    v[0] = make_float4((float)a[0], (float)a[1], (float)a[2], (float)a[3]);
+    v[1] = make_float4((float)b[0], (float)b[1], (float)b[2], (float)b[3]);
+}
+
+// eval_q_derivatives (q_variables.F90:41-112) with FP32 q and FP64 sums, and
+// func_delta (state_update.F90:190-236).
+__global__ void __launch_bounds__(GRAD_BLOCK)
+k_grad32(Geom g, Consts c, const float4 *__restrict__ q, const double *__restrict__ spd,
+         float *__restrict__ dq, float *__restrict__ qm, double *__restrict__ delta,
+         int with_delta, const Ctl *__restrict__ ctl) {
+    if (ctl->halted) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.n) return;
+    double2 pi_ = g.xy[i];
+    float4 qv = __ldg(q + i);
+    float qi[4] = {qv.x, qv.y, qv.z, qv.w};
+    float qmax[4] = {qi[0], qi[1], qi[2], qi[3]};
+    float qmin[4] = {qi[0], qi[1], qi[2], qi[3]};
+    double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
+    double sdxq[4] = {0.0, 0.0, 0.0, 0.0}, sdyq[4] = {0.0, 0.0, 0.0, 0.0};
+    double min_delt = 1.0;
+    int nb = g.nbhs[i];
+    for (int r = 0; r < nb; ++r) {
+        int k = g.conn[r * g.n + i];
+        float4 kv = __ldg(q + k);
+        float qk[4] = {kv.x, kv.y, kv.z, kv.w};
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            if (qk[m] > qmax[m]) qmax[m] = qk[m];
+            if (qk[m] < qmin[m]) qmin[m] = qk[m];
+        }
+        double2 pk = g.xy[k];
+        double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
+        double w = 1.0, dist = 0.0;
+        if (!c.power_zero || with_delta) dist = sqrt(delx * delx + dely * dely);
+        if (!c.power_zero) w = pow(dist, c.power);
+        sdx2 = sdx2 + delx * delx * w;
+        sdy2 = sdy2 + dely * dely * w;
+        sdxy = sdxy + delx * dely * w;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            double dqm = (double)qk[m] - (double)qi[m];
+            sdxq[m] = sdxq[m] + w * delx * dqm;
+            sdyq[m] = sdyq[m] + w * dely * dqm;
+        }
+        if (with_delta) {
+            double delta_t = dist / spd[k];
+            delta_t = c.cfl * delta_t;
+            if (min_delt > delta_t) min_delt = delta_t;
+        }
+    }
+    double det = sdx2 * sdy2 - sdxy * sdxy;
+    double one_by_det = 1.0 / det;
+    double dx[4], dy[4], mx[4], mn[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        dx[m] = (sdxq[m] * sdy2 - sdyq[m] * sdxy) * one_by_det;
+        dy[m] = (sdyq[m] * sdx2 - sdxq[m] * sdxy) * one_by_det;
+        mx[m] = qmax[m];
+        mn[m] = qmin[m];
+    }
+    stf8(dq + 8 * (size_t)i, dx, dy);
+    stf8(qm + 8 * (size_t)i, mx, mn);
+    if (with_delta) delta[i] = min_delt;
+}
+
+// eval_q_inner_loop + eval_update_innerloop (q_variables.F90:115-227).
+__global__ void __launch_bounds__(GRAD_BLOCK)
+k_inner32(Geom g, Consts c, const float4 *__restrict__ q, const float *__restrict__ dq_in,
+          float *__restrict__ dq_out, const Ctl *__restrict__ ctl) {
+    if (ctl->halted) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.n) return;
+    double2 pi_ = g.xy[i];
+    float4 qv = __ldg(q + i);
+    double qi[4] = {qv.x, qv.y, qv.z, qv.w};
+    float dxf[4], dyf[4];
+    ldf8(dq_in + 8 * (size_t)i, dxf, dyf);
+    double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
+    double sdxq[4] = {0.0, 0.0, 0.0, 0.0}, sdyq[4] = {0.0, 0.0, 0.0, 0.0};
+    int nb = g.nbhs[i];
+    for (int r = 0; r < nb; ++r) {
+        int k = g.conn[r * g.n + i];
+        float4 kv = __ldg(q + k);
+        float dxk[4], dyk[4];
+        ldf8(dq_in + 8 * (size_t)k, dxk, dyk);
+        double qk[4] = {kv.x, kv.y, kv.z, kv.w};
+        double2 pk = g.xy[k];
+        double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
+        double w = 1.0;
+        if (!c.power_zero) w = pow(sqrt(delx * delx + dely * dely), c.power);
+        sdx2 = sdx2 + delx * delx * w;
+        sdy2 = sdy2 + dely * dely * w;
+        sdxy = sdxy + delx * dely * w;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            double temp1 = qi[m] - 0.5 * (delx * dxf[m] + dely * dyf[m]);
+            double temp2 = qk[m] - 0.5 * (delx * dxk[m] + dely * dyk[m]);
+            sdxq[m] = sdxq[m] + (w * delx * (temp2 - temp1));
+            sdyq[m] = sdyq[m] + (w * dely * (temp2 - temp1));
+        }
+    }
+    double det = sdx2 * sdy2 - sdxy * sdxy;
+    double one_by_det = 1.0 / det;
+    double dx[4], dy[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        dx[m] = one_by_det * (sdxq[m] * sdy2 - sdyq[m] * sdxy);
+        dy[m] = one_by_det * (sdyq[m] * sdx2 - sdxq[m] * sdxy);
+    }
+    stf8(dq_out + 8 * (size_t)i, dx, dy);
+}
+
+// Compensated FP32 addition (Kahan): s += v with running correction cmp.
+__device__ __forceinline__ void kahan_add(float &s, float &cmp, float v) {
+    float y = __fsub_rn(v, cmp);
+    float t = __fadd_rn(s, y);
+    cmp = __fsub_rn(__fsub_rn(t, s), y);
+    s = t;
+}
+
+// cal_flux_residual + state_update + eval_q_variables of the new state, with
+// the per-neighbour work in FP32 (same lane layout as the FP64 kernel).
+__global__ void __launch_bounds__(FLUX_BLOCK, FLUX32_MIN_BLOCKS)
+k_flux32(Geom g, Consts c, StageBufs32 b, int rk, int last, const Ctl *__restrict__ ctl) {
+    extern __shared__ double sm[];
+    __shared__ double sres[GROUPS];
+    if (ctl->halted) return;
+    const int grp = threadIdx.x / LPP, lane = threadIdx.x % LPP;
+    const int i = blockIdx.x * GROUPS + grp;
+    const bool valid = i < g.n;
+    double *rec = sm + (size_t)grp * g.kp * FREC;
+
+    int nb = 0, kind = KIND_INTERIOR;
+    unsigned long long mx = 0, my = 0;
+    double nx = 0.0, ny = 1.0;
+    if (valid) {
+        nb = g.nbhs[i];
+        kind = i < g.nw ? KIND_WALL : (i < g.nw + g.no ? KIND_OUTER : KIND_INTERIOR);
+        mx = g.mx[i];
+        my = g.my[i];
+        const double2 nn = g.nrm[i];
+        nx = nn.x;
+        ny = nn.y;
+        const float nxf = (float)nx, nyf = (float)ny;
+        const float gm1 = (float)c.gm1, pif = (float)c.pi;
+        const float s2q = kind == KIND_WALL ? -1.0f : 1.0f;
+        for (int r = lane; r < nb; r += LPP) {
+            const int k = g.conn[r * g.n + i];
+            const double2 pi_ = g.xy[i];
+            const double2 pk = g.xy[k];
+            const double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
+            const float dxf = (float)delx, dyf = (float)dely;
+            KStateT<float> sk, si;
+            {
+                const float4 kv = __ldg(b.q_in + k);
+                const float qk[4] = {kv.x, kv.y, kv.z, kv.w};
+                float dxk[4], dyk[4], qmaxk[4], qmink[4];
+                ldf8(b.dq + 8 * (size_t)k, dxk, dyk);
+                ldf8(b.qm + 8 * (size_t)k, qmaxk, qmink);
+                float u1, u2, rho, pr;
+                reconstruct<float>(qk, dxk, dyk, qmaxk, qmink, b.eps2f[k], dxf, dyf, gm1, u1, u2,
+                                   rho, pr);
+                sk = kstate<float>(u1, u2, rho, pr, nxf, nyf, pif);
+            }
+            {
+                const float4 qv = __ldg(b.q_in + i);
+                const float qi[4] = {qv.x, qv.y, qv.z, qv.w};
+                float dxi[4], dyi[4], qmaxi[4], qmini[4];
+                ldf8(b.dq + 8 * (size_t)i, dxi, dyi);
+                ldf8(b.qm + 8 * (size_t)i, qmaxi, qmini);
+                float u1, u2, rho, pr;
+                reconstruct<float>(qi, dxi, dyi, qmaxi, qmini, b.eps2f[i], dxf, dyf, gm1, u1, u2,
+                                   rho, pr);
+                si = kstate<float>(u1, u2, rho, pr, nxf, nyf, pif);
+            }
+            const double tx = ny, ty = -nx;
+            const double dels = delx * tx + dely * ty;
+            const double deln = delx * nx + dely * ny;
+            double w = 1.0;
+            if (!c.power_zero) w = pow(sqrt(dels * dels + deln * deln), c.power);
+            double *e = rec + r * FREC;
+            float *ef = reinterpret_cast<float *>(e);
+            float Gi[4], Gk[4];
+#pragma unroll
+            for (int L = 0; L < 4; ++L) {
+                const unsigned long long bits = (L < 2) ? mx : my;
+                if (!((bits >> (r + ((L & 1) ? 32 : 0))) & 1ull)) continue;
+                const float sg = (L & 1) ? -1.0f : 1.0f;
+                if (L < 2) {
+                    if (kind == KIND_INTERIOR) {
+                        flux_gx<float>(si, sg, Gi);
+                        flux_gx<float>(sk, sg, Gk);
+                    } else {
+                        flux_quad<float>(si, sg, s2q, Gi);
+                        flux_quad<float>(sk, sg, s2q, Gk);
+                    }
+                } else {
+                    flux_gy<float>(si, sg, Gi);
+                    flux_gy<float>(sk, sg, Gk);
+                }
+#pragma unroll
+                for (int m = 0; m < 4; ++m) ef[4 * L + m] = Gk[m] - Gi[m];
+            }
+            e[8] = dels;
+            e[9] = deln;
+            e[10] = w;
+        }
+    }
+    __syncwarp();
+
+    double Gv0 = 0.0, Gv1 = 0.0;
+    if (valid) {
+        const int L = lane >> 1, c0 = (lane & 1) * 2;
+        const bool used = !((kind == KIND_WALL && L == 2) || (kind == KIND_OUTER && L == 3));
+        const unsigned long long bits = ((L < 2) ? mx : my) >> ((L & 1) ? 32 : 0);
+        if (used) {
+            double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
+            float fx0 = 0.f, fx1 = 0.f, fy0 = 0.f, fy1 = 0.f;
+            float cx0 = 0.f, cx1 = 0.f, cy0 = 0.f, cy1 = 0.f;
+            for (int r = 0; r < nb; ++r) {
+                if (!((bits >> r) & 1ull)) continue;
+                const double *e = rec + r * FREC;
+                const float *ef = reinterpret_cast<const float *>(e);
+                const double dels = e[8], deln = e[9], w = e[10];
+                const double dels_w = dels * w, deln_w = deln * w;
+                sdx2 = sdx2 + dels * dels_w;
+                sdy2 = sdy2 + deln * deln_w;
+                sdxy = sdxy + dels * deln_w;
+                const float d0 = ef[4 * L + c0], d1 = ef[4 * L + c0 + 1];
+                const float sw = (float)dels_w, nw = (float)deln_w;
+                kahan_add(fx0, cx0, d0 * sw);
+                kahan_add(fy0, cy0, d0 * nw);
+                kahan_add(fx1, cx1, d1 * sw);
+                kahan_add(fy1, cy1, d1 * nw);
+            }
+            const double det = sdx2 * sdy2 - sdxy * sdxy;
+            const double one_by_det = 1.0 / det;
+            const double X0 = (double)fx0 - cx0, X1 = (double)fx1 - cx1;
+            const double Y0 = (double)fy0 - cy0, Y1 = (double)fy1 - cy1;
+            if (L < 2) {
+                Gv0 = (X0 * sdy2 - Y0 * sdxy) * one_by_det;
+                Gv1 = (X1 * sdy2 - Y1 * sdxy) * one_by_det;
+            } else {
+                Gv0 = (Y0 * sdx2 - X0 * sdxy) * one_by_det;
+                Gv1 = (Y1 * sdx2 - X1 * sdxy) * one_by_det;
+            }
+        }
+    }
+    double G[4][4];
+#pragma unroll
+    for (int L = 0; L < 4; ++L) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            G[L][2 * h] = __shfl_sync(0xffffffffu, Gv0, 2 * L + h, LPP);
+            G[L][2 * h + 1] = __shfl_sync(0xffffffffu, Gv1, 2 * L + h, LPP);
+        }
+    }
+
+    double res_sqr = 0.0;
+    if (valid && lane == 0) {
+        const double delta = b.delta[i];
+        double fr[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            if (kind == KIND_WALL) fr[m] = 2.0 * delta * (G[0][m] + G[1][m] + G[3][m]);
+            else if (kind == KIND_OUTER) fr[m] = delta * (G[0][m] + G[1][m] + G[2][m]);
+            else fr[m] = delta * (G[0][m] + G[1][m] + G[2][m] + G[3][m]);
+        }
+        if (b.flux_dbg) st4(reinterpret_cast<R4 *>(b.flux_dbg) + i, fr[0], fr[1], fr[2], fr[3]);
+        const float4 P = b.prim_in[i];
+        double U[4], Uo[4] = {0.0, 0.0, 0.0, 0.0};
+        if (kind == KIND_OUTER) {
+            const double *inf = g.obc + 8 * (size_t)(i - g.nw);
+            conserved_ubar(P.x, P.y, P.z, P.w, nx, ny, inf, c.pi, c.gm1, U);
+            if (rk == 3) {
+                const float4 O = b.prim_old[i];
+                conserved_ubar(O.x, O.y, O.z, O.w, nx, ny, inf, c.pi, c.gm1, Uo);
+            }
+        } else {
+            prim_to_conserved(P.x, P.y, P.z, P.w, nx, ny, U);
+            if (rk == 3) {
+                const float4 O = b.prim_old[i];
+                prim_to_conserved(O.x, O.y, O.z, O.w, nx, ny, Uo);
+            }
+        }
+        double temp = U[0];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            if (rk != 3) U[m] = U[m] - (0.5 * c.euler * fr[m]);
+            else U[m] = TBT * Uo[m] + OBT * (U[m] - 0.5 * fr[m]);
+        }
+        if (kind == KIND_WALL) U[2] = 0.0;
+        double U2_rot = U[1], U3_rot = U[2];
+        U[1] = U2_rot * ny + U3_rot * nx;
+        U[2] = U3_rot * ny - U2_rot * nx;
+        if (kind != KIND_OUTER) res_sqr = (U[0] - temp) * (U[0] - temp);
+        double rho = U[0];
+        temp = 1.0 / U[0];
+        double u1 = U[1] * temp;
+        double u2 = U[2] * temp;
+        double pr = 0.4 * (U[3] - (0.5 * temp) * (U[1] * U[1] + U[2] * U[2]));
+        b.prim_out[i] = make_float4((float)rho, (float)u1, (float)u2, (float)pr);
+        double qn[4];
+        q_from_prim((double)(float)rho, (double)(float)u1, (double)(float)u2, (double)(float)pr,
+                    qn);
+        b.q_out[i] = make_float4((float)qn[0], (float)qn[1], (float)qn[2], (float)qn[3]);
+        if (last) {
+            double fu1 = (float)u1, fu2 = (float)u2, frho = (float)rho, fpr = (float)pr;
+            b.spd[i] = sqrt(fu1 * fu1 + fu2 * fu2) + 3.0 * sqrt(fpr / frho);
+        }
+    }
+    if (last) {
+        if (lane == 0) sres[grp] = res_sqr;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s = 0.0;
+            for (int q = 0; q < GROUPS; ++q) s = s + sres[q];
+            b.res_part[blockIdx.x] = s;
+        }
+    }
+}
+
+__global__ void k_init_state32(Geom g, const float4 *__restrict__ prim, float4 *__restrict__ q,
+                               double *__restrict__ spd) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.n) return;
+    float4 P = prim[i];
+    double qn[4];
+    q_from_prim((double)P.x, (double)P.y, (double)P.z, (double)P.w, qn);
+    q[i] = make_float4((float)qn[0], (float)qn[1], (float)qn[2], (float)qn[3]);
+    double u1 = P.y, u2 = P.z, rho = P.x, pr = P.w;
+    spd[i] = sqrt(u1 * u1 + u2 * u2) + 3.0 * sqrt(pr / rho);
+}
+
+__global__ void k_widen(const float4 *__restrict__ in, R4 *__restrict__ out, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 v = in[i];
+    st4(out + i, v.x, v.y, v.z, v.w);
+}
+
+inline int nblk(int n, int b) { return (n + b - 1) / b; }
+
+}  // namespace
+
+cudaError_t init_kernels32() {
+    return cudaFuncSetAttribute(k_flux32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                GROUPS * 20 * FREC * (int)sizeof(double));
+}
+
+void launch_grad32(const Geom &g, const Consts &c, const float4 *q, const double *spd, float *dq,
+                   float *qm, double *delta, bool with_delta, const Ctl *ctl, cudaStream_t s) {
+    k_grad32<<<nblk(g.n, GRAD_BLOCK), GRAD_BLOCK, 0, s>>>(g, c, q, spd, dq, qm, delta,
+                                                         with_delta ? 1 : 0, ctl);
+}
+
+void launch_inner32(const Geom &g, const Consts &c, const float4 *q, const float *dq_in,
+                    float *dq_out, const Ctl *ctl, cudaStream_t s) {
+    k_inner32<<<nblk(g.n, GRAD_BLOCK), GRAD_BLOCK, 0, s>>>(g, c, q, dq_in, dq_out, ctl);
+}
+
+void launch_flux32(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, bool last,
+                   const Ctl *ctl, cudaStream_t s) {
+    size_t smem = (size_t)GROUPS * g.kp * FREC * sizeof(double);
+    k_flux32<<<flux_blocks(g.n), FLUX_BLOCK, smem, s>>>(g, c, b, rk, last ? 1 : 0, ctl);
+}
+
+void launch_init_state32(const Geom &g, const float4 *prim, float4 *q, double *spd,
+                         cudaStream_t s) {
+    k_init_state32<<<nblk(g.n, GRAD_BLOCK), GRAD_BLOCK, 0, s>>>(g, prim, q, spd);
+}
+
+void launch_widen(const float4 *in, R4 *out, int n, cudaStream_t s) {
+    k_widen<<<nblk(n, GRAD_BLOCK), GRAD_BLOCK, 0, s>>>(in, out, n);
+}
+
+}  // namespace lskum
