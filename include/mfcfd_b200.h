@@ -93,6 +93,20 @@ typedef struct mfcfd_params {
 
 typedef struct mfcfd mfcfd_t;
 
+/* Reverse-mode derivative of the loop (the reference's checkpointed adjoint
+ * q_lskum_chkpts_b + FPI_SOLVER_B, src_mpi_adjoint/sensitivity_files/
+ * q_lskum_chkpts_b.F90:23-300).  From the handle's current state (held
+ * fixed) it runs n_iters iterations, J = sum over shapes of Cl (objective 0)
+ * or Cd (objective 1) of the final state, and writes dJ/dx, dJ/dy per point
+ * (caller order) -- the content of sensitivity/sensitivity.dat.  min_dist is
+ * data (not a function of x, y), as in the reference.  prim snapshots are
+ * kept in HBM within ckpt_bytes (32 bytes a point each, binomial placement);
+ * *J (may be NULL) gets the objective, *n_forward (may be NULL) the number of
+ * forward iterations run, recomputation included.  The handle is left at the
+ * final state.  FP64 handles with power == 0 only (else MFCFD_ERR_ARG). */
+int mfcfd_adjoint(mfcfd_t *h, int objective, int n_iters, size_t ckpt_bytes, double *J,
+                  double *dJdx, double *dJdy, int *n_forward);
+
 /* Sets the default parameters of the reference's readcase (cfl 0,
  * power 0, vl_const 150, ssprk43, no inner iterations, legacy format) with
  * Mach 0.63 and aoa 2 (parameter.F90:5-6). */

@@ -29,7 +29,7 @@ EXPORTS = ("mfcfd_default_params", "mfcfd_create", "mfcfd_destroy", "mfcfd_set_s
            "mfcfd_get_state", "mfcfd_run", "mfcfd_forces", "mfcfd_set_stream",
            "mfcfd_get_array", "mfcfd_keep_diagnostics", "mfcfd_info", "mfcfd_strerror",
            "mfcfd_last_error", "mfcfd_launch_count", "mfcfd_profile_iteration",
-           "mfcfd_run_noalloc")
+           "mfcfd_run_noalloc", "mfcfd_adjoint")
 MFCFD_NOALLOC_MAX_ITERS = 65536
 
 
@@ -90,6 +90,7 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     lib.mfcfd_launch_count.restype = C.c_longlong
     lib.mfcfd_profile_iteration.argtypes = [P, C.c_int, D]
     lib.mfcfd_run_noalloc.argtypes = [P, C.c_int, C.c_int, D, I]
+    lib.mfcfd_adjoint.argtypes = [P, C.c_int, C.c_int, C.c_size_t, D, D, D, I]
     for name in EXPORTS:
         if name not in ("mfcfd_strerror", "mfcfd_last_error", "mfcfd_launch_count"):
             getattr(lib, name).restype = C.c_int

@@ -1,0 +1,50 @@
+// Internal interface of the reverse (adjoint) kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "primal.h"
+
+namespace lskum {
+
+constexpr int ADJ_CW = 22;  // contribution record per (point, slot)
+enum { ADJ_GATHER_FLUX = 0, ADJ_GATHER_INNER = 1, ADJ_GATHER_GRAD = 2 };
+
+struct AdjConsts {
+    double q_inf[4];
+};
+
+// Shape points in grid order with their renumbered ring neighbours.
+struct AdjShape {
+    int npts;
+    const int *idx, *left, *right;
+    const double *nx, *ny;
+};
+
+cudaError_t init_adjoint_kernels();
+void launch_update_b(const Geom &g, const Consts &c, const AdjConsts &a, const R4 *prim_in,
+                     const R4 *prim_old, const R4 *fr, const double *pb_out, double *pb_in,
+                     double *pb_old, double *frb, double *nxb, double *nyb, int rk,
+                     cudaStream_t s);
+void launch_flux_b(const Geom &g, const Consts &c, const R4 *q_in, const double *dq,
+                   const double *qm, const double *delta, const double *frb, double *qb,
+                   double *dqb, double *qmb, double *xb, double *yb, double *nxb, double *nyb,
+                   double *deltab, double *contrib, cudaStream_t s);
+void launch_inner_b(const Geom &g, const R4 *q, const double *dq_in, const double *dqb_out,
+                    double *dqb_in, double *qb, double *xb, double *yb, double *contrib,
+                    cudaStream_t s);
+void launch_grad_b(const Geom &g, const Consts &c, const R4 *q, const R4 *primA,
+                   const double *dqb, const double *qmb, const double *deltab, bool with_delta,
+                   double *qb, double *xb, double *yb, double *contrib, cudaStream_t s);
+void launch_gather(int n, int kp, const int *tptr, const int *tlist, const double *contrib,
+                   int mode, double *a4, double *a8, double *b8, double *xb, double *yb,
+                   cudaStream_t s);
+void launch_qvar_b(int n, const R4 *prim, const double *qb, double *pb, cudaStream_t s);
+void launch_forces_b(const AdjShape &t, const R4 *prim, const double2 *xy, double mach,
+                     double cos_t, double sin_t, int objective, double *pb, double *xb,
+                     double *yb, double *nxb, double *nyb, cudaStream_t s);
+void launch_normals_b(int nbnd, const int *left, const int *right, const double2 *xy,
+                      const double *nxb, const double *nyb, double *xb, double *yb,
+                      cudaStream_t s);
+
+}  // namespace lskum

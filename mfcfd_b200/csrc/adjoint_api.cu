@@ -1,0 +1,405 @@
+// mfcfd_adjoint: reverse-mode derivative of the pseudo-time loop.
+//
+// Replaces the reference's q_lskum_chkpts_b + REVOLV driver
+// (src_mpi_adjoint/sensitivity_files/q_lskum_chkpts_b.F90:23-300,
+// src_mpi_adjoint/revolve.f:347-591) and FPI_SOLVER_B
+// (fpi_solver_b.F90:28-156).  From the handle's current state prim_0 (held
+// fixed) it runs n iterations, takes J = sum over shapes of Cl or Cd of the
+// final state (the reference seeds vector_cost_funcb = 1 for J = Cd,
+// objective_function_b.F90:22-33) and returns dJ/dx, dJ/dy per point.
+//
+// Checkpointing: prim snapshots (32 bytes a point) in HBM, placed by a
+// binomial schedule (Griewank's reversal with s snapshots and t sweeps
+// reverses C(s+t, t) iterations) within the caller's byte budget.  Each
+// iteration is re-run forward from its snapshot with every stage input taped
+// in HBM, then reversed stage by stage.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "adjoint.h"
+#include "handle.h"
+
+using namespace lskum;
+using lskum_host::cuda_fail;
+using lskum_host::dmalloc;
+using lskum_host::fail;
+
+struct AdjointState {
+    int n = 0, kp = 0, m = 0, rks = 0;
+    int *d_tptr = nullptr, *d_tlist = nullptr;
+    int nshape = 0;
+    int *d_sidx = nullptr, *d_sleft = nullptr, *d_sright = nullptr;
+    double *d_snx = nullptr, *d_sny = nullptr;
+    int nbnd = 0;
+    int *d_bleft = nullptr, *d_bright = nullptr;
+    R4 *tprim[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    R4 *tq[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    R4 *tfr[4] = {nullptr, nullptr, nullptr, nullptr};
+    double *tdq = nullptr, *tqm = nullptr, *tdelta = nullptr, *tspd = nullptr;
+    double *pb[2] = {nullptr, nullptr}, *pbA = nullptr;
+    double *qb = nullptr, *dqb[2] = {nullptr, nullptr}, *qmb = nullptr, *deltab = nullptr;
+    double *frb = nullptr, *xb = nullptr, *yb = nullptr, *nxb = nullptr, *nyb = nullptr;
+    double *contrib = nullptr;
+    double *hist = nullptr;
+    int hist_cap = 0;
+    std::vector<R4 *> snaps;  // snapshot pool (device buffers of n rows)
+    R4 *snap0 = nullptr;      // the initial state
+    R4 *fin = nullptr;        // the final state
+    // run bookkeeping
+    int n_iters = 0, objective = 1;
+    double J = 0.0;
+    long long forward_iters = 0;
+};
+
+namespace {
+
+double *dq_at(AdjointState *a, int rk, int t) {
+    return a->tdq + ((size_t)(rk - 1) * (a->m + 1) + t) * 8 * (size_t)a->n;
+}
+double *qm_at(AdjointState *a, int rk) { return a->tqm + (size_t)(rk - 1) * 8 * (size_t)a->n; }
+
+int adj_setup(mfcfd_t *h) {
+    if (h->adj) return MFCFD_OK;
+    AdjointState *a = new AdjointState();
+    h->adj = a;
+    const int n = h->n, kp = h->kp, m = h->p.inner_iterations, rks = h->p.rks;
+    a->n = n;
+    a->kp = kp;
+    a->m = m;
+    a->rks = rks;
+    // transposed stencil: for each point k the (i, r) with conn[r][i] = k,
+    // in increasing (i, r) order
+    std::vector<int> hconn((size_t)kp * n), hnb(n);
+    CK(cudaMemcpy(hconn.data(), h->d_conn, hconn.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(hnb.data(), h->d_nbhs, hnb.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<int> tptr(n + 1, 0), tlist;
+    for (int i = 0; i < n; ++i)
+        for (int r = 0; r < hnb[i]; ++r) tptr[hconn[(size_t)r * n + i] + 1]++;
+    for (int k = 0; k < n; ++k) tptr[k + 1] += tptr[k];
+    tlist.resize(tptr[n]);
+    std::vector<int> fill(tptr.begin(), tptr.end() - 1);
+    for (int i = 0; i < n; ++i)
+        for (int r = 0; r < hnb[i]; ++r) tlist[fill[hconn[(size_t)r * n + i]]++] = i * kp + r;
+    CK(dmalloc(&a->d_tptr, n + 1));
+    CK(dmalloc(&a->d_tlist, tlist.size()));
+    CK(cudaMemcpy(a->d_tptr, tptr.data(), tptr.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(a->d_tlist, tlist.data(), tlist.size() * sizeof(int), cudaMemcpyHostToDevice));
+    // renumbered ring neighbours and shape table
+    std::vector<int> inv(n);
+    for (int p = 0; p < n; ++p) inv[h->perm[p]] = p;
+    a->nbnd = h->nw + h->no;
+    std::vector<int> bl(std::max(a->nbnd, 1)), br(std::max(a->nbnd, 1));
+    for (int p = 0; p < a->nbnd; ++p) {
+        bl[p] = inv[h->left0[h->perm[p]] - 1];
+        br[p] = inv[h->right0[h->perm[p]] - 1];
+    }
+    std::vector<double2> hnrm(n);
+    CK(cudaMemcpy(hnrm.data(), h->d_nrm, n * sizeof(double2), cudaMemcpyDeviceToHost));
+    std::vector<int> si, sl, sr;
+    std::vector<double> snx, sny;
+    for (int i = 0; i < n; ++i) {
+        if (h->flag2_0[i] <= 0) continue;
+        const int p = inv[i];
+        si.push_back(p);
+        sl.push_back(inv[h->left0[i] - 1]);
+        sr.push_back(inv[h->right0[i] - 1]);
+        snx.push_back(hnrm[p].x);
+        sny.push_back(hnrm[p].y);
+    }
+    a->nshape = (int)si.size();
+    const size_t ns = std::max(a->nshape, 1);
+    CK(dmalloc(&a->d_bleft, bl.size()));
+    CK(dmalloc(&a->d_bright, br.size()));
+    CK(dmalloc(&a->d_sidx, ns));
+    CK(dmalloc(&a->d_sleft, ns));
+    CK(dmalloc(&a->d_sright, ns));
+    CK(dmalloc(&a->d_snx, ns));
+    CK(dmalloc(&a->d_sny, ns));
+    CK(cudaMemcpy(a->d_bleft, bl.data(), bl.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(a->d_bright, br.data(), br.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (a->nshape) {
+        CK(cudaMemcpy(a->d_sidx, si.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(a->d_sleft, sl.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(a->d_sright, sr.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(a->d_snx, snx.data(), ns * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(a->d_sny, sny.data(), ns * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    // tape of one iteration and the adjoint arrays
+    for (int s = 0; s <= rks; ++s) {
+        CK(dmalloc(&a->tprim[s], n));
+        CK(dmalloc(&a->tq[s], n));
+    }
+    for (int s = 0; s < rks; ++s) CK(dmalloc(&a->tfr[s], n));
+    CK(dmalloc(&a->tdq, (size_t)rks * (m + 1) * 8 * n));
+    CK(dmalloc(&a->tqm, (size_t)rks * 8 * n));
+    CK(dmalloc(&a->tdelta, n));
+    CK(dmalloc(&a->tspd, n));
+    for (int b = 0; b < 2; ++b) {
+        CK(dmalloc(&a->pb[b], (size_t)4 * n));
+        CK(dmalloc(&a->dqb[b], (size_t)8 * n));
+    }
+    CK(dmalloc(&a->pbA, (size_t)4 * n));
+    CK(dmalloc(&a->qb, (size_t)4 * n));
+    CK(dmalloc(&a->qmb, (size_t)8 * n));
+    CK(dmalloc(&a->deltab, n));
+    CK(dmalloc(&a->frb, (size_t)4 * n));
+    CK(dmalloc(&a->xb, n));
+    CK(dmalloc(&a->yb, n));
+    CK(dmalloc(&a->nxb, n));
+    CK(dmalloc(&a->nyb, n));
+    CK(dmalloc(&a->contrib, (size_t)n * kp * ADJ_CW));
+    CK(dmalloc(&a->snap0, n));
+    CK(dmalloc(&a->fin, n));
+    cudaError_t e = init_adjoint_kernels();
+    if (e != cudaSuccess) return cuda_fail(h, e, "init_adjoint_kernels");
+    return MFCFD_OK;
+}
+
+int reset_ctl(mfcfd_t *h) {
+    h->h_ctl->it = 1;
+    h->h_ctl->it_first = 1;
+    h->h_ctl->halted = 0;
+    h->h_ctl->done = 0;
+    CK(cudaMemcpyAsync(h->d_ctl, h->h_ctl, 4 * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    return MFCFD_OK;
+}
+
+// Runs k plain iterations from state `from` and stores the result in `to`.
+int advance(mfcfd_t *h, AdjointState *a, const R4 *from, int k, R4 *to) {
+    const size_t bytes = sizeof(R4) * (size_t)a->n;
+    CK(cudaMemcpyAsync(h->d_prim[h->cur], from, bytes, cudaMemcpyDeviceToDevice, h->stream));
+    int st = lskum_host::upload_state_aux(h);
+    if (st) return st;
+    if ((st = reset_ctl(h))) return st;
+    for (int j = 0; j < k; ++j) {
+        if ((st = lskum_host::enqueue_iteration_to(h, h->stream, a->hist))) return st;
+    }
+    a->forward_iters += k;
+    CK(cudaMemcpyAsync(to, h->d_prim[h->cur], bytes, cudaMemcpyDeviceToDevice, h->stream));
+    return MFCFD_OK;
+}
+
+// One forward iteration from `from` with every stage input taped.
+int record(mfcfd_t *h, AdjointState *a, const R4 *from) {
+    const size_t bytes = sizeof(R4) * (size_t)a->n;
+    const int m = a->m, rks = a->rks;
+    int st = reset_ctl(h);
+    if (st) return st;
+    CK(cudaMemcpyAsync(a->tprim[0], from, bytes, cudaMemcpyDeviceToDevice, h->stream));
+    launch_init_state(h->geom, a->tprim[0], a->tq[0], a->tspd, h->stream);
+    for (int rk = 1; rk <= rks; ++rk) {
+        launch_grad(h->geom, h->consts, a->tq[rk - 1], a->tspd, dq_at(a, rk, 0), qm_at(a, rk),
+                    a->tdelta, rk == 1, h->d_ctl, h->stream);
+        for (int t = 1; t <= m; ++t)
+            launch_inner(h->geom, h->consts, a->tq[rk - 1], dq_at(a, rk, t - 1), dq_at(a, rk, t),
+                         h->d_ctl, h->stream);
+        StageBufs b;
+        b.prim_in = a->tprim[rk - 1];
+        b.prim_out = a->tprim[rk];
+        b.prim_old = a->tprim[0];
+        b.q_in = a->tq[rk - 1];
+        b.q_out = a->tq[rk];
+        b.dq = dq_at(a, rk, m);
+        b.qm = qm_at(a, rk);
+        b.delta = a->tdelta;
+        b.spd = a->tspd;
+        b.res_part = h->d_res_part;
+        b.flux_dbg = reinterpret_cast<double *>(a->tfr[rk - 1]);
+        launch_flux(h->geom, h->consts, b, rk, rk == rks, h->d_ctl, h->stream);
+    }
+    h->launches += 1 + (long long)rks * (2 + m);
+    a->forward_iters += 1;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(h, e, "adjoint record launch");
+    return MFCFD_OK;
+}
+
+// Reverse of one taped iteration: pb[0] holds the adjoint of its output on
+// entry and of its input on exit.
+int reverse_taped(mfcfd_t *h, AdjointState *a) {
+    const int n = a->n, m = a->m, rks = a->rks;
+    cudaStream_t s = h->stream;
+    AdjConsts ac{{h->q_inf[0], h->q_inf[1], h->q_inf[2], h->q_inf[3]}};
+    CK(cudaMemsetAsync(a->pbA, 0, sizeof(double) * 4 * n, s));
+    CK(cudaMemsetAsync(a->deltab, 0, sizeof(double) * n, s));
+    int out = 0;  // pb[out] = adjoint of the current stage's output
+    for (int rk = rks; rk >= 1; --rk) {
+        double *pb_out = a->pb[out];
+        double *pb_in = rk == 1 ? a->pbA : a->pb[out ^ 1];
+        if (rk != 1) CK(cudaMemsetAsync(pb_in, 0, sizeof(double) * 4 * n, s));
+        launch_update_b(h->geom, h->consts, ac, a->tprim[rk - 1], a->tprim[0], a->tfr[rk - 1],
+                        pb_out, pb_in, a->pbA, a->frb, a->nxb, a->nyb, rk, s);
+        CK(cudaMemsetAsync(a->qb, 0, sizeof(double) * 4 * n, s));
+        CK(cudaMemsetAsync(a->qmb, 0, sizeof(double) * 8 * n, s));
+        CK(cudaMemsetAsync(a->dqb[m & 1], 0, sizeof(double) * 8 * n, s));
+        launch_flux_b(h->geom, h->consts, a->tq[rk - 1], dq_at(a, rk, m), qm_at(a, rk), a->tdelta,
+                      a->frb, a->qb, a->dqb[m & 1], a->qmb, a->xb, a->yb, a->nxb, a->nyb,
+                      a->deltab, a->contrib, s);
+        launch_gather(n, a->kp, a->d_tptr, a->d_tlist, a->contrib, ADJ_GATHER_FLUX, a->qb,
+                      a->dqb[m & 1], a->qmb, a->xb, a->yb, s);
+        for (int t = m; t >= 1; --t) {
+            launch_inner_b(h->geom, a->tq[rk - 1], dq_at(a, rk, t - 1), a->dqb[t & 1],
+                           a->dqb[(t - 1) & 1], a->qb, a->xb, a->yb, a->contrib, s);
+            launch_gather(n, a->kp, a->d_tptr, a->d_tlist, a->contrib, ADJ_GATHER_INNER, a->qb,
+                          a->dqb[(t - 1) & 1], nullptr, a->xb, a->yb, s);
+        }
+        launch_grad_b(h->geom, h->consts, a->tq[rk - 1], a->tprim[0], a->dqb[0], a->qmb,
+                      a->deltab, rk == 1, a->qb, a->xb, a->yb, a->contrib, s);
+        launch_gather(n, a->kp, a->d_tptr, a->d_tlist, a->contrib, ADJ_GATHER_GRAD, a->qb,
+                      nullptr, a->pbA, a->xb, a->yb, s);
+        launch_qvar_b(n, a->tprim[rk - 1], a->qb, pb_in, s);
+        h->launches += 6 + 2LL * m;
+        out ^= 1;
+    }
+    CK(cudaMemcpyAsync(a->pb[0], a->pbA, sizeof(double) * 4 * n, cudaMemcpyDeviceToDevice, s));
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(h, e, "adjoint reverse launch");
+    return MFCFD_OK;
+}
+
+// Reverse of iteration k from its input state: tapes it; the last iteration
+// also seeds the adjoint from the objective of its output.
+int reverse_iteration(mfcfd_t *h, AdjointState *a, int k, const R4 *state) {
+    int st = record(h, a, state);
+    if (st) return st;
+    if (k == a->n_iters - 1) {
+        const int n = a->n;
+        cudaStream_t s = h->stream;
+        CK(cudaMemsetAsync(a->pb[0], 0, sizeof(double) * 4 * n, s));
+        AdjShape t{a->nshape, a->d_sidx, a->d_sleft, a->d_sright, a->d_snx, a->d_sny};
+        launch_forces_b(t, a->tprim[a->rks], h->d_xy, h->p.mach, h->cos_t, h->sin_t,
+                        a->objective, a->pb[0], a->xb, a->yb, a->nxb, a->nyb, s);
+        // keep the final state: the handle holds it at the end, as after mfcfd_run
+        CK(cudaMemcpyAsync(a->fin, a->tprim[a->rks], sizeof(R4) * (size_t)n,
+                           cudaMemcpyDeviceToDevice, s));
+        h->launches += 1;
+    }
+    return reverse_taped(h, a);
+}
+
+long long binom(int s, int t) {
+    long long r = 1;
+    for (int j = 1; j <= t; ++j) {
+        r = r * (s + j) / j;
+        if (r > (1LL << 40)) return 1LL << 40;
+    }
+    return r;
+}
+
+// Reverses iterations [lo, hi) whose input state lo is held in `state`.
+int reverse_range(mfcfd_t *h, AdjointState *a, int lo, int hi, R4 *state,
+                  std::vector<R4 *> &free_slots, R4 *scratch) {
+    const int n = hi - lo;
+    if (n <= 0) return MFCFD_OK;
+    if (n == 1) return reverse_iteration(h, a, lo, state);
+    const int s = (int)free_slots.size();
+    if (s == 0) {
+        for (int k = hi - 1; k >= lo; --k) {
+            int st = advance(h, a, state, k - lo, scratch);
+            if (st) return st;
+            if ((st = reverse_iteration(h, a, k, scratch))) return st;
+        }
+        return MFCFD_OK;
+    }
+    int t = 1;
+    while (binom(s, t) < n) ++t;
+    const long long right = binom(s - 1, t);
+    const int d = (int)std::max<long long>(1, n - std::min<long long>(right, n - 1));
+    R4 *slot = free_slots.back();
+    free_slots.pop_back();
+    int st = advance(h, a, state, d, slot);
+    if (!st) st = reverse_range(h, a, lo + d, hi, slot, free_slots, scratch);
+    free_slots.push_back(slot);
+    if (st) return st;
+    return reverse_range(h, a, lo, lo + d, state, free_slots, scratch);
+}
+
+}  // namespace
+
+void lskum_host::free_adjoint(mfcfd_t *h) {
+    AdjointState *a = h->adj;
+    if (!a) return;
+    void *bufs[] = {a->d_tptr, a->d_tlist, a->d_sidx, a->d_sleft, a->d_sright, a->d_snx,
+                    a->d_sny, a->d_bleft, a->d_bright, a->tdq, a->tqm, a->tdelta, a->tspd,
+                    a->pb[0], a->pb[1], a->pbA, a->qb, a->dqb[0], a->dqb[1], a->qmb,
+                    a->deltab, a->frb, a->xb, a->yb, a->nxb, a->nyb, a->contrib, a->hist,
+                    a->snap0, a->fin};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    for (int s = 0; s < 5; ++s) {
+        if (a->tprim[s]) cudaFree(a->tprim[s]);
+        if (a->tq[s]) cudaFree(a->tq[s]);
+    }
+    for (int s = 0; s < 4; ++s)
+        if (a->tfr[s]) cudaFree(a->tfr[s]);
+    for (R4 *p : a->snaps) cudaFree(p);
+    delete a;
+    h->adj = nullptr;
+}
+
+extern "C" int mfcfd_adjoint(mfcfd_t *h, int objective, int n_iters, size_t ckpt_bytes,
+                             double *J, double *dJdx, double *dJdy, int *n_forward) {
+    if (!h || n_iters < 1 || (objective != 0 && objective != 1) || !dJdx || !dJdy)
+        return MFCFD_ERR_ARG;
+    if (h->fp32) return fail(h, MFCFD_ERR_ARG, "mfcfd_adjoint: FP64 handles only");
+    if (h->p.power != 0.0)
+        return fail(h, MFCFD_ERR_ARG, "mfcfd_adjoint: LSQ weights with power != 0 are not differentiated");
+    int st = adj_setup(h);
+    if (st) return st;
+    AdjointState *a = h->adj;
+    const int n = h->n;
+    const size_t row = sizeof(R4) * (size_t)n;
+    a->n_iters = n_iters;
+    a->objective = objective;
+    a->forward_iters = 0;
+    if (a->hist_cap < n_iters) {
+        if (a->hist) cudaFree(a->hist);
+        a->hist = nullptr;
+        CK(dmalloc(&a->hist, (size_t)n_iters));
+        a->hist_cap = n_iters;
+    }
+    // snapshot pool within the byte budget (the initial state counts)
+    const long long want = ckpt_bytes > row ? (long long)(ckpt_bytes / row) - 1 : 0;
+    const int nsnap = (int)std::min<long long>(want, n_iters - 1);
+    while ((int)a->snaps.size() < nsnap + 1) {  // + one scratch row
+        R4 *p = nullptr;
+        CK(dmalloc(&p, (size_t)n));
+        a->snaps.push_back(p);
+    }
+    std::vector<R4 *> free_slots(a->snaps.begin(), a->snaps.begin() + nsnap);
+    R4 *scratch = a->snaps[nsnap];
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpyAsync(a->snap0, h->d_prim[h->cur], row, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemsetAsync(a->xb, 0, sizeof(double) * n, h->stream));
+    CK(cudaMemsetAsync(a->yb, 0, sizeof(double) * n, h->stream));
+    CK(cudaMemsetAsync(a->nxb, 0, sizeof(double) * n, h->stream));
+    CK(cudaMemsetAsync(a->nyb, 0, sizeof(double) * n, h->stream));
+    st = reverse_range(h, a, 0, n_iters, a->snap0, free_slots, scratch);
+    if (st) return st;
+    launch_normals_b(a->nbnd, a->d_bleft, a->d_bright, h->d_xy, a->nxb, a->nyb, a->xb, a->yb,
+                     h->stream);
+    h->launches += 1;
+    CK(cudaGetLastError());
+    // leave the final state current, as mfcfd_run would
+    CK(cudaMemcpyAsync(h->d_prim[h->cur], a->fin, row, cudaMemcpyDeviceToDevice, h->stream));
+    if ((st = lskum_host::upload_state_aux(h))) return st;
+    std::vector<double> xb(n), yb(n);
+    CK(cudaMemcpyAsync(xb.data(), a->xb, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(yb.data(), a->yb, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int p = 0; p < n; ++p) {
+        dJdx[h->perm[p]] = xb[p];
+        dJdy[h->perm[p]] = yb[p];
+    }
+    if (J) {
+        std::vector<double> cl(h->shapes), cd(h->shapes), cm(h->shapes);
+        if ((st = mfcfd_forces(h, cl.data(), cd.data(), cm.data(), nullptr))) return st;
+        double s = 0.0;
+        for (int k = 0; k < h->shapes; ++k) s += objective == 1 ? cd[k] : cl[k];
+        *J = s;
+    }
+    if (n_forward) *n_forward = (int)a->forward_iters;
+    return MFCFD_OK;
+}

@@ -22,6 +22,7 @@
 #include <string>
 #include <vector>
 
+#include "handle.h"
 #include "mfcfd_b200.h"
 #include "primal.h"
 
@@ -32,57 +33,11 @@ namespace {
 constexpr int MAXNB = 20;
 thread_local std::string g_create_error;
 
-template <class T>
-cudaError_t dmalloc(T **p, size_t count) {
-    return cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T) + (count == 0 ? 16 : 0));
-}
-
 }  // namespace
 
-struct mfcfd {
-    int dev = 0;
-    int n = 0, kp = 1, nw = 0, no = 0, nint = 0, shapes = 1, nshape = 0;
-    mfcfd_params p{};
-    std::vector<int> perm;  // new index -> caller index
-    double pi = 0, theta = 0, cos_t = 0, sin_t = 0, q_inf[4] = {0, 0, 0, 0};
+using lskum_host::dmalloc;
 
-    Geom geom{};
-    Consts consts{};
-    ShapeTab shape{};
-
-    // device buffers
-    double2 *d_xy = nullptr, *d_nrm = nullptr;
-    double *d_eps2 = nullptr, *d_obc = nullptr;
-    int *d_conn = nullptr, *d_nbhs = nullptr;
-    unsigned long long *d_mx = nullptr, *d_my = nullptr;
-    R4 *d_prim[2] = {nullptr, nullptr}, *d_q[2] = {nullptr, nullptr};
-    double *d_dq[2] = {nullptr, nullptr};
-    double *d_qm = nullptr, *d_delta = nullptr, *d_spd = nullptr, *d_res_part = nullptr;
-    double *d_flux_dbg = nullptr, *d_hist = nullptr, *d_forces = nullptr;
-    int hist_cap = 0;
-    Ctl *d_ctl = nullptr;
-    Ctl *h_ctl = nullptr;  // pinned
-    int *d_sh_idx = nullptr, *d_sh_shape = nullptr;
-    double *d_sh_geo = nullptr, *d_sh_my = nullptr;
-    double *h_stage = nullptr;  // pinned staging [n][4]
-    // FP32-mixed state (precision == MFCFD_FP32_MIXED)
-    bool fp32 = false;
-    float4 *f_prim[2] = {nullptr, nullptr}, *f_q[2] = {nullptr, nullptr};
-    float *f_dq[2] = {nullptr, nullptr};
-    float *f_qm = nullptr, *f_eps2 = nullptr;
-
-    int cur = 0;   // prim buffer holding the state
-    int qcur = 0;  // q buffer holding q of the state
-    int iters_done_total = 0;
-    cudaStream_t own = nullptr, stream = nullptr;
-    cudaGraphExec_t pair_exec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [cur][qcur]
-    bool keep_diag = false;
-    long long launches = 0;
-    std::string err;
-    std::vector<double> shape_cp;
-};
-
-namespace {
+namespace lskum_host {
 
 int fail(mfcfd_t *h, int code, const std::string &msg) {
     if (h) h->err = msg;
@@ -95,13 +50,15 @@ int cuda_fail(mfcfd_t *h, cudaError_t e, const char *where) {
     return fail(h, e == cudaErrorMemoryAllocation ? MFCFD_ERR_OOM : MFCFD_ERR_CUDA, m);
 }
 
-#define CK(call)                                                    \
-    do {                                                            \
-        cudaError_t e_ = (call);                                    \
-        if (e_ != cudaSuccess) return cuda_fail(h, e_, #call);      \
-    } while (0)
+}  // namespace lskum_host
+
+using lskum_host::cuda_fail;
+using lskum_host::fail;
+
+namespace {
 
 void free_all(mfcfd_t *h) {
+    lskum_host::free_adjoint(h);
     for (auto &row : h->pair_exec)
         for (auto &g : row)
             if (g) cudaGraphExecDestroy(g);
@@ -210,8 +167,10 @@ void launch_stage(mfcfd_t *h, cudaStream_t s, int rk, int A, int B, F after) {
     h->launches += 2 + m;
 }
 
+}  // namespace
+
 // One iteration (fpi_solver): the stages, then the residual into hist.
-int enqueue_iteration_to(mfcfd_t *h, cudaStream_t s, double *hist) {
+int lskum_host::enqueue_iteration_to(mfcfd_t *h, cudaStream_t s, double *hist) {
     const int A = h->cur, B = h->cur ^ 1;
     for (int rk = 1; rk <= h->p.rks; ++rk) launch_stage(h, s, rk, A, B, [] {});
     launch_residual(h->d_res_part, flux_blocks(h->n), h->d_ctl, hist, s);
@@ -221,6 +180,9 @@ int enqueue_iteration_to(mfcfd_t *h, cudaStream_t s, double *hist) {
     if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
     return MFCFD_OK;
 }
+
+namespace {
+using lskum_host::enqueue_iteration_to;
 
 int enqueue_iteration(mfcfd_t *h, cudaStream_t s) { return enqueue_iteration_to(h, s, h->d_hist); }
 
@@ -259,7 +221,9 @@ int build_pair_graph(mfcfd_t *h) {
     return MFCFD_OK;
 }
 
-int upload_state_aux(mfcfd_t *h) {
+}  // namespace
+
+int lskum_host::upload_state_aux(mfcfd_t *h) {
     if (h->fp32)
         launch_init_state32(h->geom, h->f_prim[h->cur], h->f_q[h->qcur], h->d_spd, h->stream);
     else
@@ -270,7 +234,7 @@ int upload_state_aux(mfcfd_t *h) {
     return MFCFD_OK;
 }
 
-}  // namespace
+using lskum_host::upload_state_aux;
 
 extern "C" {
 
@@ -429,6 +393,9 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
     h->shapes = G.shapes;
     h->p = P;
     h->fp32 = P.precision == MFCFD_FP32_MIXED;
+    h->left0.assign(G.left, G.left + n);
+    h->right0.assign(G.right, G.right + n);
+    h->flag2_0.assign(G.flag_2, G.flag_2 + n);
     cudaGetDevice(&h->dev);
     h->pi = pi;
     h->theta = theta;

@@ -1,0 +1,79 @@
+// Internal: the handle behind mfcfd_t, shared by the C ABI files.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "mfcfd_b200.h"
+#include "primal.h"
+
+using namespace lskum;
+
+struct AdjointState;  // adjoint buffers (adjoint_api.cu), created on first use
+
+struct mfcfd {
+    int dev = 0;
+    int n = 0, kp = 1, nw = 0, no = 0, nint = 0, shapes = 1, nshape = 0;
+    mfcfd_params p{};
+    std::vector<int> perm;  // new index -> caller index
+    double pi = 0, theta = 0, cos_t = 0, sin_t = 0, q_inf[4] = {0, 0, 0, 0};
+
+    Geom geom{};
+    Consts consts{};
+    ShapeTab shape{};
+
+    // device buffers
+    double2 *d_xy = nullptr, *d_nrm = nullptr;
+    double *d_eps2 = nullptr, *d_obc = nullptr;
+    int *d_conn = nullptr, *d_nbhs = nullptr;
+    unsigned long long *d_mx = nullptr, *d_my = nullptr;
+    R4 *d_prim[2] = {nullptr, nullptr}, *d_q[2] = {nullptr, nullptr};
+    double *d_dq[2] = {nullptr, nullptr};
+    double *d_qm = nullptr, *d_delta = nullptr, *d_spd = nullptr, *d_res_part = nullptr;
+    double *d_flux_dbg = nullptr, *d_hist = nullptr, *d_forces = nullptr;
+    int hist_cap = 0;
+    Ctl *d_ctl = nullptr;
+    Ctl *h_ctl = nullptr;  // pinned
+    int *d_sh_idx = nullptr, *d_sh_shape = nullptr;
+    double *d_sh_geo = nullptr, *d_sh_my = nullptr;
+    double *h_stage = nullptr;  // pinned staging [n][4]
+    // FP32-mixed state (precision == MFCFD_FP32_MIXED)
+    bool fp32 = false;
+    float4 *f_prim[2] = {nullptr, nullptr}, *f_q[2] = {nullptr, nullptr};
+    float *f_dq[2] = {nullptr, nullptr};
+    float *f_qm = nullptr, *f_eps2 = nullptr;
+
+    int cur = 0;   // prim buffer holding the state
+    int qcur = 0;  // q buffer holding q of the state
+    int iters_done_total = 0;
+    cudaStream_t own = nullptr, stream = nullptr;
+    cudaGraphExec_t pair_exec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [cur][qcur]
+    bool keep_diag = false;
+    long long launches = 0;
+    std::string err;
+    std::vector<double> shape_cp;
+    AdjointState *adj = nullptr;
+    // caller-order ring neighbours of every point (for the adjoint set-up)
+    std::vector<int> left0, right0, flag2_0;
+};
+
+
+namespace lskum_host {
+int fail(mfcfd_t *h, int code, const std::string &msg);
+int cuda_fail(mfcfd_t *h, cudaError_t e, const char *where);
+int enqueue_iteration_to(mfcfd_t *h, cudaStream_t s, double *hist);
+int upload_state_aux(mfcfd_t *h);
+void free_adjoint(mfcfd_t *h);
+template <class T>
+inline cudaError_t dmalloc(T **p, size_t count) {
+    return cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T) + (count == 0 ? 16 : 0));
+}
+}  // namespace lskum_host
+
+#define CK(call)                                                                   \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) return lskum_host::cuda_fail(h, e_, #call);         \
+    } while (0)

@@ -123,6 +123,20 @@ class Solver:
                    self.h, "mfcfd_forces")
         return cl, cd, cm, cp
 
+    def adjoint(self, n_iters: int, objective: str = "cd", ckpt_bytes: int = 2 << 30):
+        """dJ/dx, dJ/dy per point for J = Cl or Cd after ``n_iters`` iterations
+        from the current state (reverse mode, binomial checkpointing).
+        Returns (J, dJdx, dJdy, forward iterations run)."""
+        dx, dy = np.zeros(self.n), np.zeros(self.n)
+        J = C.c_double(0.0)
+        nf = C.c_int(0)
+        obj = {"cl": 0, "cd": 1}[objective.lower()]
+        _lib.check(self.lib.mfcfd_adjoint(self.h, obj, int(n_iters), int(ckpt_bytes),
+                                          C.byref(J), _dptr(dx), _dptr(dy), C.byref(nf)),
+                   self.h, "mfcfd_adjoint")
+        self.it = (self.it or 0) + n_iters
+        return J.value, dx, dy, nf.value
+
     # diagnostics -----------------------------------------------------------
     def keep_diagnostics(self, on: bool = True) -> None:
         _lib.check(self.lib.mfcfd_keep_diagnostics(self.h, 1 if on else 0), self.h,
