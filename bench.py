@@ -200,6 +200,46 @@ def run_reference(args, grid, flow, cfg):
     print(json.dumps(line), flush=True)
 
 
+def adjoint_cost(args, stream, world, dist):
+    """Adjoint/primal cost on the adjoint configuration: the primal run of n
+    iterations and the reverse-mode gradient over the same n iterations
+    (binomial checkpoints within 2 GB), device-timed on the same stream."""
+    import torch
+    from mfcfd_b200.grid import config_flow, config_grid
+    from mfcfd_b200.solver import Solver
+    grid = config_grid(args.adjoint_config)
+    flow = config_flow(args.adjoint_config)
+    n = args.adjoint_iters
+    with Solver(grid, **flow) as s:
+        s.set_stream(stream.cuda_stream)
+        s.run(args.warmup)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.run(n)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        primal_ms = e0.elapsed_time(e1)
+    with Solver(grid, **flow) as s:
+        s.set_stream(stream.cuda_stream)
+        s.run(args.warmup)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        J, dx, dy, nf = s.adjoint(n, "cd", ckpt_bytes=2 << 30)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        adj_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([primal_ms, adj_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        primal_ms, adj_ms = (float(v) for v in t.tolist())
+    return {"config": f"{args.adjoint_config}: {grid.n:,} points, J = Cd, {n} iterations reversed",
+            "primal_ms": primal_ms, "adjoint_ms": adj_ms, "cost_ratio": adj_ms / primal_ms,
+            "forward_iterations": nf, "checkpoint_budget_bytes": 2 << 30,
+            "J": J, "grad_max": float(max(np.abs(dx).max(), np.abs(dy).max()))}
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -211,6 +251,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--adjoint-iters", type=int, default=50,
+                    help="iterations of the adjoint-cost leg (0 = skip)")
+    ap.add_argument("--adjoint-config", default="C3")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "mfcfd":
         args.warmup = 3
@@ -353,6 +396,10 @@ def main():
                "timed": ("set_state from host, one mfcfd_run per step (residue to host each "
                          "step), get_state + forces at the end")}
 
+    adjoint = None
+    if args.adjoint_iters > 0:
+        adjoint = adjoint_cost(args, stream, world, dist)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(grid, flow, args.cpu_seconds)
@@ -367,6 +414,7 @@ def main():
             "kernel_ms": kt, "iteration_roofline": iteration_roof,
             "final_residue": float(res[-1]) if len(res) else None,
             "fp32_mixed": fp32,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     solver.close()
