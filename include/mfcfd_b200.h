@@ -191,6 +191,83 @@ int mfcfd_run_noalloc(mfcfd_t *h, int it_first, int n_iters, double *residue, in
  * would advance it (no CUDA graph). */
 int mfcfd_profile_iteration(mfcfd_t *h, int it, double *ms);
 
+/* ------------------------------------------------------------------------
+ * Batched runs: many independent grids (instances) advanced together on one
+ * GPU.  No counterpart in the reference, which runs one grid per process
+ * (meshfree_solver.F90:83 -> q_lskum); every instance follows exactly the
+ * loop of mfcfd_run, and its states and residues are bit-identical to those
+ * of a handle created from the same grid and parameters.  The points of all
+ * instances share one set of device arrays; every pass is one grid-stride
+ * launch over the tiles (16 points) of the instances still running, so
+ * small grids do not pay a launch each.  Instances retire independently.
+ * ------------------------------------------------------------------------ */
+typedef struct mfcfd_batch mfcfd_batch_t;
+
+#define MFCFD_BATCH_MAX 256  /* instances per batch */
+
+/* Why an instance stopped in the last mfcfd_batch_run. */
+#define MFCFD_BATCH_RUNNING    0  /* not run                                  */
+#define MFCFD_BATCH_CONVERGED  1  /* residue <= tol                           */
+#define MFCFD_BATCH_MAX_ITERS  2  /* ran max_iters iterations                 */
+#define MFCFD_BATCH_NONFINITE  3  /* residue NaN (the loop's exit, as mfcfd_run) */
+
+/* Builds a batch of n_inst (1..MFCFD_BATCH_MAX) instances: grids[i] with
+ * params[i], each checked and set up as mfcfd_create does, starting from the
+ * freestream state at iteration 1.  cfl, power, rks, euler,
+ * inner_iterations and precision must be equal in all params (else
+ * MFCFD_ERR_ARG); mach, aoa, vl_const and the rest may differ.  Errors are
+ * reported by mfcfd_last_error(NULL). */
+int mfcfd_batch_create(int n_inst, const mfcfd_grid *const *grids, const mfcfd_params *params,
+                       mfcfd_batch_t **out);
+
+/* Frees the batch.  NULL is a no-op. */
+int mfcfd_batch_destroy(mfcfd_batch_t *b);
+
+/* Uses the given cudaStream_t (NULL = the batch's own stream). */
+int mfcfd_batch_set_stream(mfcfd_batch_t *b, void *stream);
+
+/* prim(4,N_inst) of one instance in and out, as mfcfd_set_state/get_state. */
+int mfcfd_batch_set_state(mfcfd_batch_t *b, int inst, const double *prim);
+int mfcfd_batch_get_state(mfcfd_batch_t *b, int inst, double *prim);
+
+/* Advances every instance from its own iteration counter until its residue
+ * is <= tol, or it has run max_iters iterations in this call, or its residue
+ * is NaN (residue as mfcfd_run defines it; 0 for the first two iterations
+ * of a fresh run).  Per instance (arrays of n_inst, any may be NULL):
+ * iters_done, the MFCFD_BATCH_* reason it stopped, and residue history rows
+ * residue[inst * max_iters + k], k < iters_done[inst].  The host is not
+ * involved between iterations (retirement happens on the device); it polls
+ * a counter every 16 iterations to stop once no instance runs.  Returns
+ * MFCFD_ERR_NONFINITE if an instance stopped on a NaN residue (the others
+ * still ran), else MFCFD_OK. */
+int mfcfd_batch_run(mfcfd_batch_t *b, double tol, int max_iters, int *iters_done, int *state,
+                    double *residue);
+
+/* Cl, Cd, Cm and cp of one instance, as mfcfd_forces. */
+int mfcfd_batch_forces(mfcfd_batch_t *b, int inst, double *cl, double *cd, double *cm,
+                       double *cp);
+
+/* Autotuner: times iters iterations (>= 2) of each candidate launch shape
+ * (block size of the point passes; blocks of every grid-stride pass as 1, 2
+ * or 4 waves of resident blocks, or one block per tile) on a copy of the
+ * current state, keeps the fastest and restores the state.  Results do not
+ * depend on the launch shape.  *ms_per_iter (may be NULL) gets the best time
+ * per iteration. */
+int mfcfd_batch_tune(mfcfd_batch_t *b, int iters, double *ms_per_iter);
+
+/* Sets the launch shape by hand: block size of the D and I passes (128 or
+ * 256) and the blocks of the D/I and F passes (0 = one wave of resident
+ * blocks). */
+int mfcfd_batch_set_launch(mfcfd_batch_t *b, int point_block, int point_grid, int flux_grid);
+
+/* Instances, total points (sum of N_inst), the current launch shape. */
+int mfcfd_batch_info(mfcfd_batch_t *b, int *n_inst, long long *n_points, int *point_block,
+                     int *point_grid, int *flux_grid);
+
+/* Last error of the batch (NULL: of mfcfd_batch_create) and kernel count. */
+const char *mfcfd_batch_last_error(mfcfd_batch_t *b);
+long long mfcfd_batch_launch_count(mfcfd_batch_t *b);
+
 #ifdef __cplusplus
 }
 #endif

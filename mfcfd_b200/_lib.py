@@ -29,7 +29,12 @@ EXPORTS = ("mfcfd_default_params", "mfcfd_create", "mfcfd_destroy", "mfcfd_set_s
            "mfcfd_get_state", "mfcfd_run", "mfcfd_forces", "mfcfd_set_stream",
            "mfcfd_get_array", "mfcfd_keep_diagnostics", "mfcfd_info", "mfcfd_strerror",
            "mfcfd_last_error", "mfcfd_launch_count", "mfcfd_profile_iteration",
-           "mfcfd_run_noalloc", "mfcfd_adjoint")
+           "mfcfd_run_noalloc", "mfcfd_adjoint", "mfcfd_batch_create", "mfcfd_batch_destroy",
+           "mfcfd_batch_set_stream", "mfcfd_batch_set_state", "mfcfd_batch_get_state",
+           "mfcfd_batch_run", "mfcfd_batch_forces", "mfcfd_batch_tune", "mfcfd_batch_set_launch",
+           "mfcfd_batch_info", "mfcfd_batch_last_error", "mfcfd_batch_launch_count")
+MFCFD_BATCH_MAX = 256
+BATCH_STATES = {0: "running", 1: "converged", 2: "max_iters", 3: "nonfinite"}
 MFCFD_NOALLOC_MAX_ITERS = 65536
 
 
@@ -91,8 +96,24 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     lib.mfcfd_profile_iteration.argtypes = [P, C.c_int, D]
     lib.mfcfd_run_noalloc.argtypes = [P, C.c_int, C.c_int, D, I]
     lib.mfcfd_adjoint.argtypes = [P, C.c_int, C.c_int, C.c_size_t, D, D, D, I]
+    lib.mfcfd_batch_create.argtypes = [C.c_int, C.POINTER(C.POINTER(Grid)), C.POINTER(Params),
+                                       C.POINTER(P)]
+    lib.mfcfd_batch_destroy.argtypes = [P]
+    lib.mfcfd_batch_set_stream.argtypes = [P, P]
+    lib.mfcfd_batch_set_state.argtypes = [P, C.c_int, D]
+    lib.mfcfd_batch_get_state.argtypes = [P, C.c_int, D]
+    lib.mfcfd_batch_run.argtypes = [P, C.c_double, C.c_int, I, I, D]
+    lib.mfcfd_batch_forces.argtypes = [P, C.c_int, D, D, D, D]
+    lib.mfcfd_batch_tune.argtypes = [P, C.c_int, D]
+    lib.mfcfd_batch_set_launch.argtypes = [P, C.c_int, C.c_int, C.c_int]
+    lib.mfcfd_batch_info.argtypes = [P, I, C.POINTER(C.c_longlong), I, I, I]
+    lib.mfcfd_batch_last_error.argtypes = [P]
+    lib.mfcfd_batch_last_error.restype = C.c_char_p
+    lib.mfcfd_batch_launch_count.argtypes = [P]
+    lib.mfcfd_batch_launch_count.restype = C.c_longlong
     for name in EXPORTS:
-        if name not in ("mfcfd_strerror", "mfcfd_last_error", "mfcfd_launch_count"):
+        if name not in ("mfcfd_strerror", "mfcfd_last_error", "mfcfd_launch_count",
+                        "mfcfd_batch_last_error", "mfcfd_batch_launch_count"):
             getattr(lib, name).restype = C.c_int
     _LIB = lib
     return lib

@@ -157,14 +157,7 @@ int adj_setup(mfcfd_t *h) {
     return MFCFD_OK;
 }
 
-int reset_ctl(mfcfd_t *h) {
-    h->h_ctl->it = 1;
-    h->h_ctl->it_first = 1;
-    h->h_ctl->halted = 0;
-    h->h_ctl->done = 0;
-    CK(cudaMemcpyAsync(h->d_ctl, h->h_ctl, 4 * sizeof(int), cudaMemcpyHostToDevice, h->stream));
-    return MFCFD_OK;
-}
+int reset_ctl(mfcfd_t *h) { return lskum_host::reset_run(h, 1); }
 
 // Runs k plain iterations from state `from` and stores the result in `to`.
 int advance(mfcfd_t *h, AdjointState *a, const R4 *from, int k, R4 *to) {
@@ -190,11 +183,11 @@ int record(mfcfd_t *h, AdjointState *a, const R4 *from) {
     CK(cudaMemcpyAsync(a->tprim[0], from, bytes, cudaMemcpyDeviceToDevice, h->stream));
     launch_init_state(h->geom, a->tprim[0], a->tq[0], a->tspd, h->stream);
     for (int rk = 1; rk <= rks; ++rk) {
-        launch_grad(h->geom, h->consts, a->tq[rk - 1], a->tspd, dq_at(a, rk, 0), qm_at(a, rk),
-                    a->tdelta, rk == 1, h->d_ctl, h->stream);
+        launch_grad(h->geom, h->consts, h->sched, a->tq[rk - 1], a->tspd, dq_at(a, rk, 0),
+                    qm_at(a, rk), a->tdelta, rk == 1, h->point_block, h->point_grid, h->stream);
         for (int t = 1; t <= m; ++t)
-            launch_inner(h->geom, h->consts, a->tq[rk - 1], dq_at(a, rk, t - 1), dq_at(a, rk, t),
-                         h->d_ctl, h->stream);
+            launch_inner(h->geom, h->consts, h->sched, a->tq[rk - 1], dq_at(a, rk, t - 1),
+                         dq_at(a, rk, t), h->point_block, h->point_grid, h->stream);
         StageBufs b;
         b.prim_in = a->tprim[rk - 1];
         b.prim_out = a->tprim[rk];
@@ -207,7 +200,7 @@ int record(mfcfd_t *h, AdjointState *a, const R4 *from) {
         b.spd = a->tspd;
         b.res_part = h->d_res_part;
         b.flux_dbg = reinterpret_cast<double *>(a->tfr[rk - 1]);
-        launch_flux(h->geom, h->consts, b, rk, rk == rks, h->d_ctl, h->stream);
+        launch_flux(h->geom, h->consts, h->sched, b, rk, rk == rks, h->flux_grid, h->stream);
     }
     h->launches += 1 + (long long)rks * (2 + m);
     a->forward_iters += 1;

@@ -67,11 +67,13 @@ void free_all(mfcfd_t *h) {
                     h->d_dq[1], h->d_qm, h->d_delta, h->d_spd, h->d_res_part, h->d_flux_dbg,
                     h->d_hist, h->d_forces, h->d_ctl, h->d_sh_idx, h->d_sh_shape, h->d_sh_geo,
                     h->d_sh_my, h->f_prim[0], h->f_prim[1], h->f_q[0], h->f_q[1],
-                    h->f_dq[0], h->f_dq[1], h->f_qm, h->f_eps2};
+                    h->f_dq[0], h->f_dq[1], h->f_qm, h->f_eps2, h->d_inst, h->d_sched,
+                    h->d_run};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (h->h_ctl) cudaFreeHost(h->h_ctl);
     if (h->h_stage) cudaFreeHost(h->h_stage);
+    if (h->h_sched) cudaFreeHost(h->h_sched);
     if (h->own) cudaStreamDestroy(h->own);
 }
 
@@ -115,12 +117,12 @@ void launch_stage(mfcfd_t *h, cudaStream_t s, int rk, int A, int B, F after) {
     const bool last = rk == h->p.rks;
     if (!h->fp32) {
         const R4 *q_in = h->d_q[h->qcur];
-        launch_grad(h->geom, h->consts, q_in, h->d_spd, h->d_dq[0], h->d_qm, h->d_delta,
-                    rk == 1, h->d_ctl, s);
+        launch_grad(h->geom, h->consts, h->sched, q_in, h->d_spd, h->d_dq[0], h->d_qm,
+                    h->d_delta, rk == 1, h->point_block, h->point_grid, s);
         after();
         for (int t = 1; t <= m; ++t) {
-            launch_inner(h->geom, h->consts, q_in, h->d_dq[(t - 1) & 1], h->d_dq[t & 1],
-                         h->d_ctl, s);
+            launch_inner(h->geom, h->consts, h->sched, q_in, h->d_dq[(t - 1) & 1],
+                         h->d_dq[t & 1], h->point_block, h->point_grid, s);
             after();
         }
         StageBufs b;
@@ -135,16 +137,16 @@ void launch_stage(mfcfd_t *h, cudaStream_t s, int rk, int A, int B, F after) {
         b.spd = h->d_spd;
         b.res_part = h->d_res_part;
         b.flux_dbg = h->keep_diag ? h->d_flux_dbg : nullptr;
-        launch_flux(h->geom, h->consts, b, rk, last, h->d_ctl, s);
+        launch_flux(h->geom, h->consts, h->sched, b, rk, last, h->flux_grid, s);
         after();
     } else {
         const float4 *q_in = h->f_q[h->qcur];
-        launch_grad32(h->geom, h->consts, q_in, h->d_spd, h->f_dq[0], h->f_qm, h->d_delta,
-                      rk == 1, h->d_ctl, s);
+        launch_grad32(h->geom, h->consts, h->sched, q_in, h->d_spd, h->f_dq[0], h->f_qm,
+                      h->d_delta, rk == 1, h->point_block, h->point_grid, s);
         after();
         for (int t = 1; t <= m; ++t) {
-            launch_inner32(h->geom, h->consts, q_in, h->f_dq[(t - 1) & 1], h->f_dq[t & 1],
-                           h->d_ctl, s);
+            launch_inner32(h->geom, h->consts, h->sched, q_in, h->f_dq[(t - 1) & 1],
+                           h->f_dq[t & 1], h->point_block, h->point_grid, s);
             after();
         }
         StageBufs32 b;
@@ -160,7 +162,7 @@ void launch_stage(mfcfd_t *h, cudaStream_t s, int rk, int A, int B, F after) {
         b.spd = h->d_spd;
         b.res_part = h->d_res_part;
         b.flux_dbg = h->keep_diag ? h->d_flux_dbg : nullptr;
-        launch_flux32(h->geom, h->consts, b, rk, last, h->d_ctl, s);
+        launch_flux32(h->geom, h->consts, h->sched, b, rk, last, h->flux_grid, s);
         after();
     }
     h->qcur ^= 1;
@@ -173,7 +175,7 @@ void launch_stage(mfcfd_t *h, cudaStream_t s, int rk, int A, int B, F after) {
 int lskum_host::enqueue_iteration_to(mfcfd_t *h, cudaStream_t s, double *hist) {
     const int A = h->cur, B = h->cur ^ 1;
     for (int rk = 1; rk <= h->p.rks; ++rk) launch_stage(h, s, rk, A, B, [] {});
-    launch_residual(h->d_res_part, flux_blocks(h->n), h->d_ctl, hist, s);
+    launch_residual(h->d_inst, 1, h->d_res_part, h->d_ctl, hist, 0, h->d_run, h->d_sched, s);
     h->launches += 1;
     h->cur = B;
     cudaError_t e = cudaGetLastError();
@@ -236,6 +238,21 @@ int lskum_host::upload_state_aux(mfcfd_t *h) {
 
 using lskum_host::upload_state_aux;
 
+int lskum_host::reset_run(mfcfd_t *h, int it_first) {
+    h->h_ctl->it = it_first;
+    h->h_ctl->it_first = it_first;
+    h->h_ctl->halted = 0;
+    h->h_ctl->done = 0;
+    h->h_ctl->active = 1;
+    h->h_ctl->state = BATCH_RUNNING;
+    const int one = 1;
+    sched_fill(h->h_sched, &h->inst_h, &one, 1);
+    CK(cudaMemcpyAsync(h->d_ctl, h->h_ctl, CTL_RESET_BYTES, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_sched, h->h_sched, sizeof(int) * SCHED_INTS, cudaMemcpyHostToDevice,
+                       h->stream));
+    return MFCFD_OK;
+}
+
 extern "C" {
 
 int mfcfd_default_params(mfcfd_params *p) {
@@ -258,12 +275,12 @@ int mfcfd_default_params(mfcfd_params *p) {
     return MFCFD_OK;
 }
 
-int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **out) {
-    mfcfd_t *h = nullptr;
-    if (!out) return fail(nullptr, MFCFD_ERR_ARG, "out is NULL");
-    *out = nullptr;
-    if (!grid || !params) return fail(nullptr, MFCFD_ERR_ARG, "grid or params is NULL");
-    const mfcfd_grid &G = *grid;
+}  // extern "C"
+
+// Host half of mfcfd_create: checks of the grid and parameters, normals,
+// split membership, renumbering and the renumbered arrays, all in caller
+// arithmetic; no device call.  Errors are reported as by mfcfd_create.
+int lskum_host::prepare_grid(const mfcfd_grid &G, const mfcfd_params &P, HostGrid &hg) {
     const int n = G.n;
     if (n <= 0) return fail(nullptr, MFCFD_ERR_ARG, "grid.n must be positive");
     if (!G.x || !G.y || !G.nx || !G.ny || !G.min_dist || !G.flag_1 || !G.flag_2 || !G.left ||
@@ -271,7 +288,6 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
         return fail(nullptr, MFCFD_ERR_ARG, "a grid array is NULL");
     if (G.ld_conn < n) return fail(nullptr, MFCFD_ERR_ARG, "grid.ld_conn < grid.n");
     if (G.shapes < 1) return fail(nullptr, MFCFD_ERR_ARG, "grid.shapes must be >= 1");
-    const mfcfd_params &P = *params;
     if (!(P.rks == 1 || P.rks == 4))
         return fail(nullptr, MFCFD_ERR_ARG, "params.rks must be 4 (ssprk43) or 1 (first)");
     if (P.inner_iterations < 0 || P.inner_iterations > 64)
@@ -374,35 +390,16 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
         if (G.flag_2[i] > 0 && (G.left[i] < 1 || G.left[i] > n || G.right[i] < 1 || G.right[i] > n))
             return fail(nullptr, MFCFD_ERR_GRID, "shape point without valid left/right");
 
-    // host checks done: now the device
-    int dev_count = 0;
-    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
-        return fail(nullptr, MFCFD_ERR_NODEV, "no CUDA device");
-    {
-        cudaError_t e = init_kernels();
-        if (e == cudaSuccess) e = init_kernels32();
-        if (e != cudaSuccess) return fail(nullptr, MFCFD_ERR_CUDA, cudaGetErrorString(e));
-    }
-    h = new (std::nothrow) mfcfd();
-    if (!h) return fail(nullptr, MFCFD_ERR_OOM, "host allocation failed");
-    h->n = n;
-    h->kp = kp;
-    h->nw = nw;
-    h->no = no;
-    h->nint = n - nw - no;
-    h->shapes = G.shapes;
-    h->p = P;
-    h->fp32 = P.precision == MFCFD_FP32_MIXED;
-    h->left0.assign(G.left, G.left + n);
-    h->right0.assign(G.right, G.right + n);
-    h->flag2_0.assign(G.flag_2, G.flag_2 + n);
-    cudaGetDevice(&h->dev);
-    h->pi = pi;
-    h->theta = theta;
-    h->cos_t = cos(theta);
-    h->sin_t = sin(theta);
-    for (int c = 0; c < 4; ++c) h->q_inf[c] = q_inf[c];
-
+    hg.n = n;
+    hg.kp = kp;
+    hg.nw = nw;
+    hg.no = no;
+    hg.shapes = G.shapes;
+    hg.pi = pi;
+    hg.theta = theta;
+    hg.cos_t = cos(theta);
+    hg.sin_t = sin(theta);
+    for (int c = 0; c < 4; ++c) hg.q_inf[c] = q_inf[c];
     // renumbering: new -> caller index
     std::vector<int> base(n);
     if (P.ordering == MFCFD_ORDER_RCM) {
@@ -422,20 +419,22 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
     } else {
         for (int i = 0; i < n; ++i) base[i] = i;
     }
-    h->perm.reserve(n);
+    hg.perm.reserve(n);
     for (int want : {0, 2, 1})
         for (int i : base)
-            if (G.flag_1[i] == want) h->perm.push_back(i);
+            if (G.flag_1[i] == want) hg.perm.push_back(i);
     std::vector<int> inv(n);
-    for (int p = 0; p < n; ++p) inv[h->perm[p]] = p;
+    for (int p = 0; p < n; ++p) inv[hg.perm[p]] = p;
 
     // renumbered host arrays
-    std::vector<double2> hxy(n), hnrm(n);
-    std::vector<double> heps(n), hobc((size_t)8 * std::max(no, 1), 0.0);
-    std::vector<int> hconn((size_t)kp * n), hnb(n);
-    std::vector<unsigned long long> hmx(n), hmy(n);
+    auto &hxy = hg.xy, &hnrm = hg.nrm;
+    auto &heps = hg.eps2, &hobc = hg.obc;
+    auto &hconn = hg.conn, &hnb = hg.nbhs;
+    auto &hmx = hg.mx, &hmy = hg.my;
+    hxy.resize(n); hnrm.resize(n); heps.resize(n); hobc.assign((size_t)8 * std::max(no, 1), 0.0);
+    hconn.resize((size_t)kp * n); hnb.resize(n); hmx.resize(n); hmy.resize(n);
     for (int p = 0; p < n; ++p) {
-        int i = h->perm[p];
+        int i = hg.perm[p];
         hxy[p] = make_double2(G.x[i], G.y[i]);
         hnrm[p] = make_double2(nx[i], ny[i]);
         double epsi = P.vl_const * G.min_dist[i];
@@ -451,7 +450,7 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
         if (p >= nw && p < nw + no) {
             // state_update.F90:248-263: the freestream half of Ubar
             const double pr_inf = 1.0 / 1.4, rho_inf = 1.0, gamma = 1.4;
-            double u1_inf = h->q_inf[1], u2_inf = h->q_inf[2];
+            double u1_inf = hg.q_inf[1], u2_inf = hg.q_inf[2];
             double tx = ny[i], ty = -nx[i];
             double u1r = u1_inf * tx + u2_inf * ty;
             double u2r = u1_inf * nx[i] + u2_inf * ny[i];
@@ -459,15 +458,15 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
             double e_inf = pr_inf / (rho_inf * (gamma - 1.0)) + 0.5 * (temp1);
             double beta = (0.5 * rho_inf) / pr_inf;
             double S2 = u2r * sqrt(beta);
-            double B2_inf = exp(-S2 * S2) / (2.0 * sqrt(h->pi * beta));
+            double B2_inf = exp(-S2 * S2) / (2.0 * sqrt(hg.pi * beta));
             double A2n_inf = 0.5 * (1.0 - erf(S2));
             double *o = &hobc[(size_t)8 * (p - nw)];
             o[0] = u1r; o[1] = u2r; o[2] = e_inf; o[3] = A2n_inf; o[4] = B2_inf;
         }
     }
     // shape points in grid order (compute_force_coeffs.F90:40-78)
-    std::vector<int> sidx, sshape;
-    std::vector<double> sgeo, smy;
+    auto &sidx = hg.sidx, &sshape = hg.sshape;
+    auto &sgeo = hg.sgeo, &smy = hg.smy;
     for (int i = 0; i < n; ++i) {
         if (G.flag_2[i] <= 0) continue;
         int l = G.left[i] - 1, r = G.right[i] - 1;
@@ -482,7 +481,62 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
         sgeo.insert(sgeo.end(), {nx[i], ny[i], ds, mxx});
         smy.push_back(myy);
     }
-    h->nshape = (int)sidx.size();
+    hg.nshape = (int)sidx.size();
+
+    return MFCFD_OK;
+}
+
+extern "C" {
+
+int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **out) {
+    mfcfd_t *h = nullptr;
+    if (!out) return fail(nullptr, MFCFD_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!grid || !params) return fail(nullptr, MFCFD_ERR_ARG, "grid or params is NULL");
+    const mfcfd_grid &G = *grid;
+    const mfcfd_params &P = *params;
+    HostGrid hg;
+    {
+        int st0 = lskum_host::prepare_grid(G, P, hg);
+        if (st0) return st0;
+    }
+    const int n = hg.n, kp = hg.kp, nw = hg.nw, no = hg.no;
+    const auto &hxy = hg.xy, &hnrm = hg.nrm;
+    const auto &heps = hg.eps2, &hobc = hg.obc;
+    const auto &hconn = hg.conn, &hnb = hg.nbhs;
+    const auto &hmx = hg.mx, &hmy = hg.my;
+    const auto &sidx = hg.sidx, &sshape = hg.sshape;
+    const auto &sgeo = hg.sgeo, &smy = hg.smy;
+    // host checks done: now the device
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+        return fail(nullptr, MFCFD_ERR_NODEV, "no CUDA device");
+    {
+        cudaError_t e = init_kernels();
+        if (e == cudaSuccess) e = init_kernels32();
+        if (e != cudaSuccess) return fail(nullptr, MFCFD_ERR_CUDA, cudaGetErrorString(e));
+    }
+    h = new (std::nothrow) mfcfd();
+    if (!h) return fail(nullptr, MFCFD_ERR_OOM, "host allocation failed");
+    h->n = n;
+    h->kp = kp;
+    h->nw = nw;
+    h->no = no;
+    h->nint = n - nw - no;
+    h->shapes = hg.shapes;
+    h->nshape = hg.nshape;
+    h->perm = std::move(hg.perm);
+    h->p = P;
+    h->fp32 = P.precision == MFCFD_FP32_MIXED;
+    h->left0.assign(G.left, G.left + n);
+    h->right0.assign(G.right, G.right + n);
+    h->flag2_0.assign(G.flag_2, G.flag_2 + n);
+    cudaGetDevice(&h->dev);
+    h->pi = hg.pi;
+    h->theta = hg.theta;
+    h->cos_t = hg.cos_t;
+    h->sin_t = hg.sin_t;
+    for (int c = 0; c < 4; ++c) h->q_inf[c] = hg.q_inf[c];
 
     // device arrays
     int st = MFCFD_OK;
@@ -536,12 +590,17 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
     ALLOC(h->d_res_part, flux_blocks(n));
     ALLOC(h->d_forces, 3 * h->shapes + std::max(h->nshape, 1));
     ALLOC(h->d_ctl, 1);
+    ALLOC(h->d_inst, 1);
+    ALLOC(h->d_sched, SCHED_INTS);
+    ALLOC(h->d_run, 1);
     ALLOC(h->d_sh_idx, std::max(h->nshape, 1));
     ALLOC(h->d_sh_shape, std::max(h->nshape, 1));
     ALLOC(h->d_sh_geo, 4 * std::max(h->nshape, 1));
     ALLOC(h->d_sh_my, std::max(h->nshape, 1));
     {
         cudaError_t e = cudaMallocHost(reinterpret_cast<void **>(&h->h_ctl), sizeof(Ctl));
+        if (e == cudaSuccess)
+            e = cudaMallocHost(reinterpret_cast<void **>(&h->h_sched), sizeof(int) * SCHED_INTS);
         if (e == cudaSuccess)
             e = cudaMallocHost(reinterpret_cast<void **>(&h->h_stage), sizeof(double) * 4 * (size_t)n);
         if (e != cudaSuccess) {
@@ -572,6 +631,26 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
     h->consts.power_zero = P.power == 0.0 ? 1 : 0;
     h->consts.rks = P.rks;
     h->shape = ShapeTab{h->nshape, h->shapes, h->d_sh_idx, h->d_sh_shape, h->d_sh_geo, h->d_sh_my};
+    // the grid as a schedule of one instance; launch shape: a thread per
+    // point and a block per tile
+    h->inst_h = InstInfo{0, n, nw, no, 0, 0, flux_blocks(n), 0};
+    h->sched = sched_view(h->d_inst, h->d_sched);
+    h->point_block = 256;
+    h->point_grid = (n + 255) / 256;
+    h->flux_grid = flux_blocks(n);
+    {
+        const BatchRun run{-INFINITY, 0x7fffffff, 0};
+        const int one = 1;
+        sched_fill(h->h_sched, &h->inst_h, &one, 1);
+        cudaError_t e = cudaMemcpy(h->d_inst, &h->inst_h, sizeof(InstInfo), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(h->d_run, &run, sizeof(BatchRun), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(h->d_sched, h->h_sched, sizeof(int) * SCHED_INTS, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            st = cuda_fail(h, e, "cudaMemcpy schedule");
+            goto fail_create;
+        }
+    }
     {
         Ctl c{};
         c.it = 1;
@@ -703,12 +782,8 @@ int mfcfd_run(mfcfd_t *h, int it_first, int n_iters, double *residue, int *n_don
         drop_graphs(h);  // the graphs hold the old history pointer
     }
     CK(cudaStreamSynchronize(h->stream));
-    // reset it / it_first / halted / done; res_old stays on the device
-    h->h_ctl->it = it_first;
-    h->h_ctl->it_first = it_first;
-    h->h_ctl->halted = 0;
-    h->h_ctl->done = 0;
-    CK(cudaMemcpyAsync(h->d_ctl, h->h_ctl, 4 * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    // reset it .. state and the schedule; res_old stays on the device
+    if (int st = lskum_host::reset_run(h, it_first)) return st;
     int rem = n_iters;
     if (rem & 1) {
         int st = enqueue_iteration(h, h->stream);
@@ -843,21 +918,18 @@ int mfcfd_profile_iteration(mfcfd_t *h, int it, double *ms) {
     std::vector<cudaEvent_t> ev(nev);
     for (auto &e : ev) CK(cudaEventCreate(&e));
     CK(cudaStreamSynchronize(h->stream));
-    h->h_ctl->it = it;
-    h->h_ctl->it_first = it;
-    h->h_ctl->halted = 0;
-    h->h_ctl->done = 0;
     if (h->hist_cap < 1) {
         CK(dmalloc(&h->d_hist, 1));
         h->hist_cap = 1;
     }
-    CK(cudaMemcpyAsync(h->d_ctl, h->h_ctl, 4 * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    if (int st = lskum_host::reset_run(h, it)) return st;
     const int A = h->cur, B = h->cur ^ 1;
     int e = 0;
     CK(cudaEventRecord(ev[e++], h->stream));
     for (int rk = 1; rk <= h->p.rks; ++rk)
         launch_stage(h, h->stream, rk, A, B, [&] { cudaEventRecord(ev[e++], h->stream); });
-    launch_residual(h->d_res_part, flux_blocks(h->n), h->d_ctl, h->d_hist, h->stream);
+    launch_residual(h->d_inst, 1, h->d_res_part, h->d_ctl, h->d_hist, 0, h->d_run, h->d_sched,
+                    h->stream);
     CK(cudaEventRecord(ev[e++], h->stream));
     h->launches += 1;
     h->cur = B;
@@ -967,11 +1039,7 @@ extern "C" int mfcfd_run_noalloc(mfcfd_t *h, int it_first, int n_iters, double *
     int st = noalloc_setup(h, &hist);
     if (st) return st;
     CK(cudaStreamSynchronize(h->stream));
-    h->h_ctl->it = it_first;
-    h->h_ctl->it_first = it_first;
-    h->h_ctl->halted = 0;
-    h->h_ctl->done = 0;
-    CK(cudaMemcpyAsync(h->d_ctl, h->h_ctl, 4 * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    if ((st = lskum_host::reset_run(h, it_first))) return st;
     for (int k = 0; k < n_iters; ++k) {
         st = noalloc_iteration(h, h->stream, hist);
         if (st) return st;

@@ -45,6 +45,16 @@ struct mfcfd {
     float *f_dq[2] = {nullptr, nullptr};
     float *f_qm = nullptr, *f_eps2 = nullptr;
 
+    // the handle's grid as a schedule of one instance (kernels are shared
+    // with batched runs)
+    InstInfo inst_h{};
+    InstInfo *d_inst = nullptr;
+    int *d_sched = nullptr;    // SCHED_INTS
+    int *h_sched = nullptr;    // pinned SCHED_INTS
+    BatchRun *d_run = nullptr; // no retirement but on a NaN residue
+    Sched sched{};
+    int point_block = 256, point_grid = 1, flux_grid = 1;  // launch shape
+
     int cur = 0;   // prim buffer holding the state
     int qcur = 0;  // q buffer holding q of the state
     int iters_done_total = 0;
@@ -60,11 +70,28 @@ struct mfcfd {
 };
 
 
+// Renumbered host arrays of one grid (the host half of mfcfd_create).
+struct HostGrid {
+    int n = 0, kp = 1, nw = 0, no = 0, shapes = 1, nshape = 0;
+    double pi = 0, theta = 0, cos_t = 0, sin_t = 0, q_inf[4] = {0, 0, 0, 0};
+    std::vector<int> perm;  // new index -> caller index
+    std::vector<double2> xy, nrm;
+    std::vector<double> eps2, obc;  // obc: 8 per outer point (at least 8)
+    std::vector<int> conn, nbhs;    // conn[r * n + p], renumbered, padded with p
+    std::vector<unsigned long long> mx, my;
+    std::vector<int> sidx, sshape;  // shape points in caller order
+    std::vector<double> sgeo, smy;
+};
+
 namespace lskum_host {
+int prepare_grid(const mfcfd_grid &G, const mfcfd_params &P, HostGrid &hg);
 int fail(mfcfd_t *h, int code, const std::string &msg);
 int cuda_fail(mfcfd_t *h, cudaError_t e, const char *where);
 int enqueue_iteration_to(mfcfd_t *h, cudaStream_t s, double *hist);
 int upload_state_aux(mfcfd_t *h);
+// Control block and schedule for a run starting at iteration it_first
+// (enqueued on the handle's stream).
+int reset_run(mfcfd_t *h, int it_first);
 void free_adjoint(mfcfd_t *h);
 template <class T>
 inline cudaError_t dmalloc(T **p, size_t count) {

@@ -10,12 +10,73 @@ namespace lskum {
 // Control block in device memory (one per handle).
 struct Ctl {
     int it;           // iteration number the next residual belongs to
-    int it_first;     // first iteration of the current mfcfd_run call
-    int halted;       // 1 once a residue was NaN: later kernels return at once
+    int it_first;     // first iteration of the current run call
+    int halted;       // 1 once a residue was NaN
     int done;         // iterations completed in the current call
+    int active;       // 1 while the instance is scheduled (0 after it retires)
+    int state;        // BatchState the instance retired with
     int restart;      // reference `restart` flag
     int plen;         // points in the residual norm
     double res_old;   // residual norm the residue is measured against
+};
+// Ctl fields a run call resets from the host (it .. state); the rest stays
+// on the device between calls.
+constexpr size_t CTL_RESET_BYTES = 6 * sizeof(int);
+
+// Batched runs ------------------------------------------------------------
+constexpr int TILE = 16;        // points per schedule tile (= points per flux block)
+constexpr int MAX_BATCH = 256;  // instances per batch
+enum BatchState { BATCH_RUNNING = 0, BATCH_CONVERGED = 1, BATCH_MAX_ITERS = 2,
+                  BATCH_NONFINITE = 3 };
+
+// One instance inside the concatenated point set (all counts in points
+// except tile0/ntiles).
+struct InstInfo {
+    int base;     // first global point (a multiple of TILE)
+    int n, nw, no;
+    int obc_off;  // first row of the instance's outer points in Geom::obc
+    int tile0;    // base / TILE
+    int ntiles;   // ceil(n / TILE)
+    int pad;
+};
+
+// Schedule of the running instances, one int block in device memory:
+// [nact, ticket counter, pre[MAX_BATCH + 1], act[MAX_BATCH]] -- pre[a] = tiles
+// before running slot a (pre[nact] = total), act[a] = its instance.  Written
+// by the host at the start of a run and by the residual kernel after every
+// iteration.
+constexpr int SCHED_NACT = 0, SCHED_COUNTER = 1, SCHED_PRE = 2, SCHED_ACT = 3 + MAX_BATCH;
+constexpr int SCHED_INTS = 3 + 2 * MAX_BATCH;
+struct Sched {
+    const InstInfo *inst;  // [n_inst]
+    const int *pre;
+    const int *act;
+    const int *nact;
+};
+inline Sched sched_view(const InstInfo *inst, const int *blk) {
+    return Sched{inst, blk + SCHED_PRE, blk + SCHED_ACT, blk + SCHED_NACT};
+}
+// Host: the schedule of the instances with active[i] != 0, in instance order.
+inline void sched_fill(int *blk, const InstInfo *inst, const int *active, int n_inst) {
+    int na = 0, pre = 0;
+    for (int i = 0; i < n_inst; ++i)
+        if (active[i]) {
+            blk[SCHED_PRE + na] = pre;
+            blk[SCHED_ACT + na] = i;
+            pre += inst[i].ntiles;
+            ++na;
+        }
+    blk[SCHED_PRE + na] = pre;
+    blk[SCHED_NACT] = na;
+    blk[SCHED_COUNTER] = 0;
+}
+
+// Retirement rule of the current batched run (device memory, read by
+// kb_residual, so the captured graphs need no update).
+struct BatchRun {
+    double tol;     // retire once residue <= tol
+    int max_iters;  // retire after this many iterations of the run
+    int pad;
 };
 
 // Buffers one pseudo-time stage reads and writes.
@@ -33,22 +94,36 @@ struct StageBufs {
     double *flux_dbg;    // [n][4] flux_res, or nullptr
 };
 
+// The passes of one stage.  Each is a grid-stride kernel over the tiles of
+// the scheduled instances; `block` threads per block for the point passes
+// and `grid` blocks (0 = one wave of resident blocks).
 // D pass: qm and dq (eval_q_derivatives); with_delta also computes the
 // local time step (func_delta) from spd of the neighbours.
-void launch_grad(const Geom &g, const Consts &c, const R4 *q, const double *spd, double *dq,
-                 double *qm, double *delta, bool with_delta, const Ctl *ctl, cudaStream_t s);
+void launch_grad(const Geom &g, const Consts &c, const Sched &s, const R4 *q, const double *spd,
+                 double *dq, double *qm, double *delta, bool with_delta, int block, int grid,
+                 cudaStream_t st);
 // I pass: one inner iteration (eval_q_inner_loop + eval_update_innerloop).
-void launch_inner(const Geom &g, const Consts &c, const R4 *q, const double *dq_in,
-                  double *dq_out, const Ctl *ctl, cudaStream_t s);
+void launch_inner(const Geom &g, const Consts &c, const Sched &s, const R4 *q,
+                  const double *dq_in, double *dq_out, int block, int grid, cudaStream_t st);
+// F pass: flux residual + state update of stage rk (1-based).
+void launch_flux(const Geom &g, const Consts &c, const Sched &s, const StageBufs &b, int rk,
+                 bool last, int grid, cudaStream_t st);
+// Residual norm and residue of one iteration per instance (hist row i, entry
+// it - it_first), retirement, and the schedule of the next iteration.
+void launch_residual(const InstInfo *inst, int n_inst, const double *res_part, Ctl *ctl,
+                     double *hist, int hist_ld, const BatchRun *run, int *sched,
+                     cudaStream_t st);
 // One-time kernel attributes (before any stream capture).
 cudaError_t init_kernels();
-// F pass: flux residual + state update of stage rk (1-based).
+// tiles (flux blocks) of n points
 int flux_blocks(int n);
-void launch_flux(const Geom &g, const Consts &c, const StageBufs &b, int rk, bool last,
-                 const Ctl *ctl, cudaStream_t s);
-// residual norm / residue of one iteration; writes hist[it - it_first].
-void launch_residual(const double *res_part, int nparts, Ctl *ctl, double *hist,
-                     cudaStream_t s);
+// resident blocks per SM (kind: 0 D pass, 1 I pass, 2 F pass; fp32 selects
+// the FP32-mixed kernels)
+int batch_occupancy(int kind, bool fp32, int block, size_t smem);
+int batch_occupancy32(int kind, int block, size_t smem);
+// dynamic shared memory of the flux passes for stencils of kp slots
+size_t flux_smem_bytes(int kp);
+size_t flux32_smem_bytes(int kp);
 // q and spd from prim (set_state)
 void launch_init_state(const Geom &g, const R4 *prim, R4 *q, double *spd, cudaStream_t s);
 
@@ -68,14 +143,16 @@ struct StageBufs32 {
     double *flux_dbg;
 };
 cudaError_t init_kernels32();
-void launch_grad32(const Geom &g, const Consts &c, const float4 *q, const double *spd, float *dq,
-                   float *qm, double *delta, bool with_delta, const Ctl *ctl, cudaStream_t s);
-void launch_inner32(const Geom &g, const Consts &c, const float4 *q, const float *dq_in,
-                    float *dq_out, const Ctl *ctl, cudaStream_t s);
-void launch_flux32(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, bool last,
-                   const Ctl *ctl, cudaStream_t s);
+void launch_grad32(const Geom &g, const Consts &c, const Sched &s, const float4 *q,
+                   const double *spd, float *dq, float *qm, double *delta, bool with_delta,
+                   int block, int grid, cudaStream_t st);
+void launch_inner32(const Geom &g, const Consts &c, const Sched &s, const float4 *q,
+                    const float *dq_in, float *dq_out, int block, int grid, cudaStream_t st);
+void launch_flux32(const Geom &g, const Consts &c, const Sched &s, const StageBufs32 &b, int rk,
+                   bool last, int grid, cudaStream_t st);
 void launch_init_state32(const Geom &g, const float4 *prim, float4 *q, double *spd,
                          cudaStream_t s);
+
 // float4 prim -> FP64 rows (for the force sums and diagnostics)
 void launch_widen(const float4 *in, R4 *out, int n, cudaStream_t s);
 

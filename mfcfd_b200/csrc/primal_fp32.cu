@@ -10,6 +10,7 @@
 // residual norm and the force coefficients.
 #include <cuda_runtime.h>
 
+#include "batch.cuh"
 #include "primal.h"
 
 namespace lskum {
@@ -42,13 +43,10 @@ __device__ __forceinline__ void stf8(float *p, const double a[4], const double b
 
 // eval_q_derivatives (q_variables.F90:41-112) with FP32 q and FP64 sums, and
 // func_delta (state_update.F90:190-236).
-__global__ void __launch_bounds__(GRAD_BLOCK)
-k_grad32(Geom g, Consts c, const float4 *__restrict__ q, const double *__restrict__ spd,
-         float *__restrict__ dq, float *__restrict__ qm, double *__restrict__ delta,
-         int with_delta, const Ctl *__restrict__ ctl) {
-    if (ctl->halted) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.n) return;
+__device__ __forceinline__ void
+grad32_point(const Geom &g, const Consts &c, const float4 *__restrict__ q,
+             const double *__restrict__ spd, float *__restrict__ dq, float *__restrict__ qm,
+             double *__restrict__ delta, int with_delta, int i) {
     double2 pi_ = g.xy[i];
     float4 qv = __ldg(q + i);
     float qi[4] = {qv.x, qv.y, qv.z, qv.w};
@@ -102,13 +100,24 @@ k_grad32(Geom g, Consts c, const float4 *__restrict__ q, const double *__restric
     if (with_delta) delta[i] = min_delt;
 }
 
-// eval_q_inner_loop + eval_update_innerloop (q_variables.F90:115-227).
 __global__ void __launch_bounds__(GRAD_BLOCK)
-k_inner32(Geom g, Consts c, const float4 *__restrict__ q, const float *__restrict__ dq_in,
-          float *__restrict__ dq_out, const Ctl *__restrict__ ctl) {
-    if (ctl->halted) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.n) return;
+kb_grad32(Geom g, Consts c, Sched s, const float4 *__restrict__ q,
+          const double *__restrict__ spd, float *__restrict__ dq, float *__restrict__ qm,
+          double *__restrict__ delta, int with_delta) {
+    __shared__ SchedSmem ss;
+    load_sched(s, ss);
+    const int total = ss.pre[ss.nact] * TILE;
+    for (int vp = blockIdx.x * blockDim.x + threadIdx.x; vp < total;
+         vp += gridDim.x * blockDim.x) {
+        const int i = sched_point(s, ss, vp);
+        if (i >= 0) grad32_point(g, c, q, spd, dq, qm, delta, with_delta, i);
+    }
+}
+
+// eval_q_inner_loop + eval_update_innerloop (q_variables.F90:115-227).
+__device__ __forceinline__ void
+inner32_point(const Geom &g, const Consts &c, const float4 *__restrict__ q,
+              const float *__restrict__ dq_in, float *__restrict__ dq_out, int i) {
     double2 pi_ = g.xy[i];
     float4 qv = __ldg(q + i);
     double qi[4] = {qv.x, qv.y, qv.z, qv.w};
@@ -149,6 +158,19 @@ k_inner32(Geom g, Consts c, const float4 *__restrict__ q, const float *__restric
     stf8(dq_out + 8 * (size_t)i, dx, dy);
 }
 
+__global__ void __launch_bounds__(GRAD_BLOCK)
+kb_inner32(Geom g, Consts c, Sched s, const float4 *__restrict__ q,
+           const float *__restrict__ dq_in, float *__restrict__ dq_out) {
+    __shared__ SchedSmem ss;
+    load_sched(s, ss);
+    const int total = ss.pre[ss.nact] * TILE;
+    for (int vp = blockIdx.x * blockDim.x + threadIdx.x; vp < total;
+         vp += gridDim.x * blockDim.x) {
+        const int i = sched_point(s, ss, vp);
+        if (i >= 0) inner32_point(g, c, q, dq_in, dq_out, i);
+    }
+}
+
 // Compensated FP32 addition (Kahan): s += v with running correction cmp.
 __device__ __forceinline__ void kahan_add(float &s, float &cmp, float v) {
     float y = __fsub_rn(v, cmp);
@@ -159,14 +181,11 @@ __device__ __forceinline__ void kahan_add(float &s, float &cmp, float v) {
 
 // cal_flux_residual + state_update + eval_q_variables of the new state, with
 // the per-neighbour work in FP32 (same lane layout as the FP64 kernel).
-__global__ void __launch_bounds__(FLUX_BLOCK, FLUX32_MIN_BLOCKS)
-k_flux32(Geom g, Consts c, StageBufs32 b, int rk, int last, const Ctl *__restrict__ ctl) {
-    extern __shared__ double sm[];
-    __shared__ double sres[GROUPS];
-    if (ctl->halted) return;
+// One call handles one tile of GROUPS points (arguments as in the FP64 pass).
+__device__ __forceinline__ void
+flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, int last, int i,
+            bool valid, int kind0, int orow, int part, double *sm, double *sres) {
     const int grp = threadIdx.x / LPP, lane = threadIdx.x % LPP;
-    const int i = blockIdx.x * GROUPS + grp;
-    const bool valid = i < g.n;
     double *rec = sm + (size_t)grp * g.kp * FREC;
 
     int nb = 0, kind = KIND_INTERIOR;
@@ -174,7 +193,7 @@ k_flux32(Geom g, Consts c, StageBufs32 b, int rk, int last, const Ctl *__restric
     double nx = 0.0, ny = 1.0;
     if (valid) {
         nb = g.nbhs[i];
-        kind = i < g.nw ? KIND_WALL : (i < g.nw + g.no ? KIND_OUTER : KIND_INTERIOR);
+        kind = kind0;
         mx = g.mx[i];
         my = g.my[i];
         const double2 nn = g.nrm[i];
@@ -309,7 +328,7 @@ k_flux32(Geom g, Consts c, StageBufs32 b, int rk, int last, const Ctl *__restric
         const float4 P = b.prim_in[i];
         double U[4], Uo[4] = {0.0, 0.0, 0.0, 0.0};
         if (kind == KIND_OUTER) {
-            const double *inf = g.obc + 8 * (size_t)(i - g.nw);
+            const double *inf = g.obc + 8 * (size_t)orow;
             conserved_ubar(P.x, P.y, P.z, P.w, nx, ny, inf, c.pi, c.gm1, U);
             if (rk == 3) {
                 const float4 O = b.prim_old[i];
@@ -354,8 +373,25 @@ k_flux32(Geom g, Consts c, StageBufs32 b, int rk, int last, const Ctl *__restric
         if (threadIdx.x == 0) {
             double s = 0.0;
             for (int q = 0; q < GROUPS; ++q) s = s + sres[q];
-            b.res_part[blockIdx.x] = s;
+            b.res_part[part] = s;
         }
+    }
+}
+
+__global__ void __launch_bounds__(FLUX_BLOCK, FLUX32_MIN_BLOCKS)
+kb_flux32(Geom g, Consts c, Sched s, StageBufs32 b, int rk, int last) {
+    extern __shared__ double sm[];
+    __shared__ double sres[GROUPS];
+    __shared__ SchedSmem ss;
+    load_sched(s, ss);
+    const int total = ss.pre[ss.nact];
+    for (int v = blockIdx.x; v < total; v += gridDim.x) {
+        const TileRef t = sched_tile(s, ss, v);
+        const int j = t.j0 + threadIdx.x / LPP;
+        const int kind = j < t.nw ? KIND_WALL : (j < t.nw + t.no ? KIND_OUTER : KIND_INTERIOR);
+        flux32_tile(g, c, b, rk, last, t.base + j, j < t.n, kind, t.obc_off + j - t.nw, t.tile,
+                    sm, sres);
+        __syncthreads();  // the next tile reuses sm and sres
     }
 }
 
@@ -383,25 +419,50 @@ inline int nblk(int n, int b) { return (n + b - 1) / b; }
 }  // namespace
 
 cudaError_t init_kernels32() {
-    return cudaFuncSetAttribute(k_flux32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(kb_flux32, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 GROUPS * 20 * FREC * (int)sizeof(double));
 }
 
-void launch_grad32(const Geom &g, const Consts &c, const float4 *q, const double *spd, float *dq,
-                   float *qm, double *delta, bool with_delta, const Ctl *ctl, cudaStream_t s) {
-    k_grad32<<<nblk(g.n, GRAD_BLOCK), GRAD_BLOCK, 0, s>>>(g, c, q, spd, dq, qm, delta,
-                                                         with_delta ? 1 : 0, ctl);
+size_t flux32_smem_bytes(int kp) { return (size_t)GROUPS * kp * FREC * sizeof(double); }
+
+int batch_occupancy32(int kind, int block, size_t smem) {
+    int nb = 0;
+    cudaError_t e = cudaErrorInvalidValue;
+    if (kind == 0) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_grad32, block, smem);
+    else if (kind == 1)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_inner32, block, smem);
+    else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_flux32, block, smem);
+    return e == cudaSuccess ? nb : 1;
 }
 
-void launch_inner32(const Geom &g, const Consts &c, const float4 *q, const float *dq_in,
-                    float *dq_out, const Ctl *ctl, cudaStream_t s) {
-    k_inner32<<<nblk(g.n, GRAD_BLOCK), GRAD_BLOCK, 0, s>>>(g, c, q, dq_in, dq_out, ctl);
+namespace {
+int wave32(int kind, int block, size_t smem, int grid) {
+    if (grid > 0) return grid;
+    int dev = 0, sms = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int nb = batch_occupancy32(kind, block, smem);
+    return (sms > 0 ? sms : 1) * (nb > 0 ? nb : 1);
+}
+}  // namespace
+
+void launch_grad32(const Geom &g, const Consts &c, const Sched &s, const float4 *q,
+                         const double *spd, float *dq, float *qm, double *delta, bool with_delta,
+                         int block, int grid, cudaStream_t st) {
+    kb_grad32<<<wave32(0, block, 0, grid), block, 0, st>>>(g, c, s, q, spd, dq, qm,
+                                                                     delta, with_delta ? 1 : 0);
 }
 
-void launch_flux32(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, bool last,
-                   const Ctl *ctl, cudaStream_t s) {
+void launch_inner32(const Geom &g, const Consts &c, const Sched &s, const float4 *q,
+                          const float *dq_in, float *dq_out, int block, int grid, cudaStream_t st) {
+    kb_inner32<<<wave32(1, block, 0, grid), block, 0, st>>>(g, c, s, q, dq_in, dq_out);
+}
+
+void launch_flux32(const Geom &g, const Consts &c, const Sched &s, const StageBufs32 &b,
+                         int rk, bool last, int grid, cudaStream_t st) {
     size_t smem = (size_t)GROUPS * g.kp * FREC * sizeof(double);
-    k_flux32<<<flux_blocks(g.n), FLUX_BLOCK, smem, s>>>(g, c, b, rk, last ? 1 : 0, ctl);
+    kb_flux32<<<wave32(2, FLUX_BLOCK, smem, grid), FLUX_BLOCK, smem, st>>>(g, c, s, b, rk,
+                                                                           last ? 1 : 0);
 }
 
 void launch_init_state32(const Geom &g, const float4 *prim, float4 *q, double *spd,

@@ -1,11 +1,16 @@
 // FP64 kernels of the LSKUM pseudo-time loop on sm_100a.
 //
 // Per pseudo-time stage (fpi_solver.F90:27-53):
-//   k_grad   D pass  -- eval_q_derivatives (+ func_delta on the first stage)
-//   k_inner  I pass  -- eval_q_inner_loop + eval_update_innerloop (ping-pong)
-//   k_flux   F pass  -- cal_flux_residual + state_update + eval_q_variables of
-//                       the new state (+ res_sqr partials on the last stage)
-// and per iteration k_residual (fpi_solver.F90:57-70).
+//   kb_grad   D pass  -- eval_q_derivatives (+ func_delta on the first stage)
+//   kb_inner  I pass  -- eval_q_inner_loop + eval_update_innerloop (ping-pong)
+//   kb_flux   F pass  -- cal_flux_residual + state_update + eval_q_variables of
+//                        the new state (+ res_sqr partials on the last stage)
+// and per iteration kb_residual (fpi_solver.F90:57-70).
+//
+// Every pass walks a schedule of instances (batch.cuh): a single grid is a
+// schedule of one instance, a batch of independent grids one of many, and
+// both run the same compiled kernels, so an instance's results do not depend
+// on what it is batched with.
 //
 // Layout in HBM (renumbered points: wall | outer | interior): one 32-byte
 // row per point for prim and q, 64-byte rows for dq and qm, 16-byte rows for
@@ -13,6 +18,9 @@
 // thread-per-point passes read them coalesced.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
+#include "batch.cuh"
 #include "primal.h"
 
 namespace lskum {
@@ -47,13 +55,10 @@ __device__ __forceinline__ void ld8(const double *p, double a[4], double b[4]) {
 
 // q_variables.F90:41-112 eval_q_derivatives, and state_update.F90:190-236
 // func_delta (spd[k] = |u_k| + 3 sqrt(p_k/rho_k) of the neighbour's state).
-__global__ void __launch_bounds__(GRAD_BLOCK)
-k_grad(Geom g, Consts c, const R4 *__restrict__ q, const double *__restrict__ spd,
-       double *__restrict__ dq, double *__restrict__ qm, double *__restrict__ delta,
-       int with_delta, const Ctl *__restrict__ ctl) {
-    if (ctl->halted) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.n) return;
+__device__ __forceinline__ void
+grad_point(const Geom &g, const Consts &c, const R4 *__restrict__ q, const double *__restrict__ spd,
+           double *__restrict__ dq, double *__restrict__ qm, double *__restrict__ delta,
+           int with_delta, int i) {
     double2 pi_ = g.xy[i];
     R4 qv = ld4(q + i);
     double qi[4] = {qv.a, qv.b, qv.c, qv.d};
@@ -103,14 +108,27 @@ k_grad(Geom g, Consts c, const R4 *__restrict__ q, const double *__restrict__ sp
     if (with_delta) delta[i] = min_delt;
 }
 
+// D pass: grid-stride over the points of the scheduled instances (a single
+// grid is the one-instance case).
+__global__ void __launch_bounds__(GRAD_BLOCK)
+kb_grad(Geom g, Consts c, Sched s, const R4 *__restrict__ q, const double *__restrict__ spd,
+        double *__restrict__ dq, double *__restrict__ qm, double *__restrict__ delta,
+        int with_delta) {
+    __shared__ SchedSmem ss;
+    load_sched(s, ss);
+    const int total = ss.pre[ss.nact] * TILE;
+    for (int vp = blockIdx.x * blockDim.x + threadIdx.x; vp < total;
+         vp += gridDim.x * blockDim.x) {
+        const int i = sched_point(s, ss, vp);
+        if (i >= 0) grad_point(g, c, q, spd, dq, qm, delta, with_delta, i);
+    }
+}
+
 // q_variables.F90:115-227 eval_q_inner_loop + eval_update_innerloop: reads
 // dq_in, writes dq_out (the buffers swap instead of copying temp into dq).
-__global__ void __launch_bounds__(GRAD_BLOCK)
-k_inner(Geom g, Consts c, const R4 *__restrict__ q, const double *__restrict__ dq_in,
-        double *__restrict__ dq_out, const Ctl *__restrict__ ctl) {
-    if (ctl->halted) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.n) return;
+__device__ __forceinline__ void
+inner_point(const Geom &g, const Consts &c, const R4 *__restrict__ q,
+            const double *__restrict__ dq_in, double *__restrict__ dq_out, int i) {
     double2 pi_ = g.xy[i];
     R4 qv = ld4(q + i);
     double qi[4] = {qv.a, qv.b, qv.c, qv.d};
@@ -151,6 +169,19 @@ k_inner(Geom g, Consts c, const R4 *__restrict__ q, const double *__restrict__ d
     st8(dq_out + 8 * (size_t)i, dx, dy);
 }
 
+__global__ void __launch_bounds__(GRAD_BLOCK)
+kb_inner(Geom g, Consts c, Sched s, const R4 *__restrict__ q, const double *__restrict__ dq_in,
+         double *__restrict__ dq_out) {
+    __shared__ SchedSmem ss;
+    load_sched(s, ss);
+    const int total = ss.pre[ss.nact] * TILE;
+    for (int vp = blockIdx.x * blockDim.x + threadIdx.x; vp < total;
+         vp += gridDim.x * blockDim.x) {
+        const int i = sched_point(s, ss, vp);
+        if (i >= 0) inner_point(g, c, q, dq_in, dq_out, i);
+    }
+}
+
 // flux_residual.F90:14-73 cal_flux_residual + state_update.F90:10-141 +
 // q_variables.F90:8-37 on the new state.
 //
@@ -162,14 +193,14 @@ k_inner(Geom g, Consts c, const R4 *__restrict__ q, const double *__restrict__ d
 // memory.  Then lane pair (2L, 2L+1) sums list L in slot order -- the
 // reference's loop order -- for components (0,1) and (2,3), and lane 0
 // gathers the four list derivatives and updates the state.
-__global__ void __launch_bounds__(FLUX_BLOCK, FLUX_MIN_BLOCKS)
-k_flux(Geom g, Consts c, StageBufs b, int rk, int last, const Ctl *__restrict__ ctl) {
-    extern __shared__ double sm[];
-    __shared__ double sres[GROUPS];
-    if (ctl->halted) return;
+//
+// One call handles one tile of GROUPS points; point i of this thread's group
+// is valid or padding, kind0 is its kind, orow its row in g.obc (outer
+// points) and part the slot of the tile's res_sqr partial.
+__device__ __forceinline__ void
+flux_tile(const Geom &g, const Consts &c, const StageBufs &b, int rk, int last, int i,
+          bool valid, int kind0, int orow, int part, double *sm, double *sres) {
     const int grp = threadIdx.x / LPP, lane = threadIdx.x % LPP;
-    const int i = blockIdx.x * GROUPS + grp;
-    const bool valid = i < g.n;
     double *rec = sm + (size_t)grp * g.kp * REC;
 
     int nb = 0, kind = KIND_INTERIOR;
@@ -177,7 +208,7 @@ k_flux(Geom g, Consts c, StageBufs b, int rk, int last, const Ctl *__restrict__ 
     double nx = 0.0, ny = 1.0;
     if (valid) {
         nb = g.nbhs[i];
-        kind = i < g.nw ? KIND_WALL : (i < g.nw + g.no ? KIND_OUTER : KIND_INTERIOR);
+        kind = kind0;
         mx = g.mx[i];
         my = g.my[i];
         const double2 nn = g.nrm[i];
@@ -309,7 +340,7 @@ k_flux(Geom g, Consts c, StageBufs b, int rk, int last, const Ctl *__restrict__ 
         R4 P = ld4(b.prim_in + i);
         double U[4], Uo[4] = {0.0, 0.0, 0.0, 0.0};
         if (kind == KIND_OUTER) {
-            const double *inf = g.obc + 8 * (size_t)(i - g.nw);
+            const double *inf = g.obc + 8 * (size_t)orow;
             conserved_ubar(P.a, P.b, P.c, P.d, nx, ny, inf, c.pi, c.gm1, U);
             if (rk == 3) {
                 R4 O = ld4(b.prim_old + i);
@@ -350,17 +381,37 @@ k_flux(Geom g, Consts c, StageBufs b, int rk, int last, const Ctl *__restrict__ 
         if (threadIdx.x == 0) {
             double s = 0.0;
             for (int q = 0; q < GROUPS; ++q) s = s + sres[q];
-            b.res_part[blockIdx.x] = s;
+            b.res_part[part] = s;
         }
+    }
+}
+
+// F pass: each block walks the scheduled tiles with a stride of the grid.  A
+// tile never straddles two instances and its partial lands in slot
+// (instance's first tile + tile number), so an instance's residual sums do
+// not depend on the other instances or on the launch shape.
+__global__ void __launch_bounds__(FLUX_BLOCK, FLUX_MIN_BLOCKS)
+kb_flux(Geom g, Consts c, Sched s, StageBufs b, int rk, int last) {
+    extern __shared__ double sm[];
+    __shared__ double sres[GROUPS];
+    __shared__ SchedSmem ss;
+    load_sched(s, ss);
+    const int total = ss.pre[ss.nact];
+    for (int v = blockIdx.x; v < total; v += gridDim.x) {
+        const TileRef t = sched_tile(s, ss, v);
+        const int j = t.j0 + threadIdx.x / LPP;
+        const int kind = j < t.nw ? KIND_WALL : (j < t.nw + t.no ? KIND_OUTER : KIND_INTERIOR);
+        flux_tile(g, c, b, rk, last, t.base + j, j < t.n, kind, t.obc_off + j - t.nw, t.tile,
+                  sm, sres);
+        __syncthreads();  // the next tile reuses sm and sres
     }
 }
 
 // fpi_solver.F90:57-70: res_new = sqrt(sum res_sqr)/plen and the residue.
 // Partials are summed in a fixed order (deterministic).
-__global__ void __launch_bounds__(1024)
-k_residual(const double *__restrict__ part, int nparts, Ctl *ctl, double *hist) {
-    __shared__ double s[1024];
-    if (ctl->halted) return;
+// Whole block of 1024 threads; the residue is returned on thread 0.
+__device__ __forceinline__ double residual_block(const double *__restrict__ part, int nparts,
+                                                 Ctl *ctl, double *hist, double *s) {
     double acc = 0.0;
     for (int t = threadIdx.x; t < nparts; t += blockDim.x) acc = acc + part[t];
     s[threadIdx.x] = acc;
@@ -383,6 +434,84 @@ k_residual(const double *__restrict__ part, int nparts, Ctl *ctl, double *hist) 
         ctl->it = it + 1;
         ctl->done = ctl->done + 1;
         if (isnan(residue)) ctl->halted = 1;
+        return residue;
+    }
+    return 0.0;
+}
+
+// Per-instance residual (block b = instance b): the instance's tile partials
+// are reduced in the order of residual_block, then the retirement rule of the
+// run is applied (NaN residue, residue <= tol, max_iters iterations).  The
+// last block to finish (threadfence + ticket, no waiting) rebuilds the
+// schedule from Ctl::active for the next iteration's passes: a stable
+// compaction of the running instances and the prefix sums of their tile
+// counts (Hillis-Steele scans over MAX_BATCH slots).
+__global__ void __launch_bounds__(1024)
+kb_residual(const InstInfo *__restrict__ inst, int n_inst, const double *__restrict__ part,
+            Ctl *ctl, double *hist, int hist_ld, const BatchRun *__restrict__ run,
+            int *sched) {
+    __shared__ double s[1024];
+    __shared__ int s_active, s_last;
+    __shared__ int cnt[MAX_BATCH], til[MAX_BATCH];
+    Ctl *c = ctl + blockIdx.x;
+    if (threadIdx.x == 0) s_active = c->active;
+    __syncthreads();
+    if (s_active) {
+        const InstInfo in = inst[blockIdx.x];
+        const double residue =
+            residual_block(part + in.tile0, in.ntiles, c, hist + (size_t)blockIdx.x * hist_ld, s);
+        if (threadIdx.x == 0) {
+            if (isnan(residue)) {
+                c->active = 0;
+                c->state = BATCH_NONFINITE;
+            } else if (residue <= run->tol) {
+                c->active = 0;
+                c->state = BATCH_CONVERGED;
+            } else if (c->done >= run->max_iters) {
+                c->active = 0;
+                c->state = BATCH_MAX_ITERS;
+            }
+        }
+    }
+    int *counter = sched + SCHED_COUNTER;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const int t = threadIdx.x;
+    int a = 0, nt = 0;
+    if (t < MAX_BATCH) {
+        a = (t < n_inst && reinterpret_cast<volatile const int *>(&ctl[t].active)[0]) ? 1 : 0;
+        nt = a ? inst[t].ntiles : 0;
+        cnt[t] = a;
+        til[t] = nt;
+    }
+    __syncthreads();
+    for (int off = 1; off < MAX_BATCH; off <<= 1) {
+        int x = 0, y = 0;
+        if (t < MAX_BATCH && t >= off) {
+            x = cnt[t - off];
+            y = til[t - off];
+        }
+        __syncthreads();
+        if (t < MAX_BATCH) {
+            cnt[t] += x;
+            til[t] += y;
+        }
+        __syncthreads();
+    }
+    int *pre = sched + SCHED_PRE, *act = sched + SCHED_ACT;
+    if (a) {
+        act[cnt[t] - 1] = t;
+        pre[cnt[t] - 1] = til[t] - nt;
+    }
+    if (t == MAX_BATCH - 1) {
+        sched[SCHED_NACT] = cnt[t];
+        pre[cnt[t]] = til[t];
+        *counter = 0;
     }
 }
 
@@ -431,30 +560,56 @@ inline int nblk(int n, int b) { return (n + b - 1) / b; }
 int flux_blocks(int n) { return nblk(n, GROUPS); }
 
 cudaError_t init_kernels() {
-    return cudaFuncSetAttribute(k_flux, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(kb_flux, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 GROUPS * 20 * REC * (int)sizeof(double));
 }
 
-void launch_grad(const Geom &g, const Consts &c, const R4 *q, const double *spd, double *dq,
-                 double *qm, double *delta, bool with_delta, const Ctl *ctl, cudaStream_t s) {
-    k_grad<<<nblk(g.n, GRAD_BLOCK), GRAD_BLOCK, 0, s>>>(g, c, q, spd, dq, qm, delta,
-                                                       with_delta ? 1 : 0, ctl);
+namespace {
+// blocks of one wave of resident blocks of a batched kernel (grid == 0)
+int wave(int kind, int block, size_t smem, int grid) {
+    if (grid > 0) return grid;
+    int dev = 0, sms = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return std::max(sms, 1) * std::max(1, batch_occupancy(kind, false, block, smem));
+}
+}  // namespace
+
+size_t flux_smem_bytes(int kp) { return (size_t)GROUPS * kp * REC * sizeof(double); }
+
+int batch_occupancy(int kind, bool fp32, int block, size_t smem) {
+    if (fp32) return batch_occupancy32(kind, block, smem);
+    int nb = 0;
+    cudaError_t e = cudaErrorInvalidValue;
+    if (kind == 0) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_grad, block, smem);
+    else if (kind == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_inner, block, smem);
+    else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_flux, block, smem);
+    return e == cudaSuccess ? nb : 1;
 }
 
-void launch_inner(const Geom &g, const Consts &c, const R4 *q, const double *dq_in,
-                  double *dq_out, const Ctl *ctl, cudaStream_t s) {
-    k_inner<<<nblk(g.n, GRAD_BLOCK), GRAD_BLOCK, 0, s>>>(g, c, q, dq_in, dq_out, ctl);
+void launch_grad(const Geom &g, const Consts &c, const Sched &s, const R4 *q, const double *spd,
+                 double *dq, double *qm, double *delta, bool with_delta, int block, int grid,
+                 cudaStream_t st) {
+    kb_grad<<<wave(0, block, 0, grid), block, 0, st>>>(g, c, s, q, spd, dq, qm, delta,
+                                                       with_delta ? 1 : 0);
 }
 
-void launch_flux(const Geom &g, const Consts &c, const StageBufs &b, int rk, bool last,
-                 const Ctl *ctl, cudaStream_t s) {
-    size_t smem = (size_t)GROUPS * g.kp * REC * sizeof(double);
-    k_flux<<<flux_blocks(g.n), FLUX_BLOCK, smem, s>>>(g, c, b, rk, last ? 1 : 0, ctl);
+void launch_inner(const Geom &g, const Consts &c, const Sched &s, const R4 *q,
+                  const double *dq_in, double *dq_out, int block, int grid, cudaStream_t st) {
+    kb_inner<<<wave(1, block, 0, grid), block, 0, st>>>(g, c, s, q, dq_in, dq_out);
 }
 
-void launch_residual(const double *res_part, int nparts, Ctl *ctl, double *hist,
-                     cudaStream_t s) {
-    k_residual<<<1, 1024, 0, s>>>(res_part, nparts, ctl, hist);
+void launch_flux(const Geom &g, const Consts &c, const Sched &s, const StageBufs &b, int rk,
+                 bool last, int grid, cudaStream_t st) {
+    size_t smem = flux_smem_bytes(g.kp);
+    kb_flux<<<wave(2, FLUX_BLOCK, smem, grid), FLUX_BLOCK, smem, st>>>(g, c, s, b, rk,
+                                                                      last ? 1 : 0);
+}
+
+void launch_residual(const InstInfo *inst, int n_inst, const double *res_part, Ctl *ctl,
+                     double *hist, int hist_ld, const BatchRun *run, int *sched,
+                     cudaStream_t st) {
+    kb_residual<<<n_inst, 1024, 0, st>>>(inst, n_inst, res_part, ctl, hist, hist_ld, run, sched);
 }
 
 void launch_init_state(const Geom &g, const R4 *prim, R4 *q, double *spd, cudaStream_t s) {

@@ -390,6 +390,37 @@ def config_grid(name: str, **overrides) -> Grid:
                       name=f"{name}_{c['ni']}x{c['nj']}")
 
 
+def batch_instances(n_inst: int = 64, config: int = 4, n_min: int = 4000, n_max: int = 256000,
+                    aspect: float = 1.6, mach=(0.5, 0.8), aoa=(-2.0, 4.0),
+                    thickness=(0.08, 0.16), first_spacing: float = 5e-3, inner_iterations=0,
+                    build: bool = True):
+    """Instances of a batched workload: instance k draws from PCG64 seeded
+    1000*config + k a point count log-uniform in [n_min, n_max] (ni x nj with
+    ni ~ aspect*nj, ni even), a Mach number, an angle of attack and a
+    thickness, each uniform in its range.  Returns (grids, flows, specs); with
+    build=False the grids are None (only the draws).  The 5e-3 first spacing
+    is C1's: the coarse instances need it to stay free of the growing wall
+    mode (see CONFIGS)."""
+    grids, flows, specs = [], [], []
+    for k in range(n_inst):
+        rng = np.random.default_rng(1000 * config + k)
+        n = float(np.exp(rng.uniform(np.log(n_min), np.log(n_max))))
+        m = float(rng.uniform(*mach))
+        a = float(rng.uniform(*aoa))
+        t = float(rng.uniform(*thickness))
+        nj = max(8, int(round(np.sqrt(n / aspect))))
+        ni = max(16, 2 * int(round(aspect * nj / 2)))
+        spec = dict(ni=ni, nj=nj, mach=m, aoa=a, thickness=t, seed=1000 * config + k)
+        specs.append(spec)
+        flow = dict(FLOW_DEFAULTS)
+        flow.update(mach=m, aoa=a, inner_iterations=inner_iterations)
+        flows.append(flow)
+        grids.append(naca_ogrid(ni, nj, thickness=t, seed=spec["seed"],
+                                first_spacing=first_spacing, name=f"B{config}_{k}_{ni}x{nj}")
+                     if build else None)
+    return grids, flows, specs
+
+
 def config_flow(name: str) -> dict:
     """Solver parameters of a configuration (case.in keys)."""
     c = CONFIGS[name]
