@@ -145,12 +145,10 @@ void free_batch(mfcfd_batch_t *b) {
 }
 
 // blocks in one wave of resident blocks of a batched pass
-int wave_blocks(const mfcfd_batch_t *b, int kind, int block) {
-    int sms = 1;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->dev);
+int batch_wave(const mfcfd_batch_t *b, int kind, int block) {
     size_t smem = 0;
     if (kind == 2) smem = b->fp32 ? flux32_smem_bytes(b->kp) : flux_smem_bytes(b->kp);
-    return std::max(sms, 1) * std::max(1, batch_occupancy(kind, b->fp32, block, smem));
+    return wave_blocks(b->dev, kind, block, smem, b->fp32);
 }
 
 // Launch shape from (block, waves): waves 0 = one block per tile (flux) and
@@ -158,8 +156,8 @@ int wave_blocks(const mfcfd_batch_t *b, int kind, int block) {
 void set_shape(mfcfd_batch_t *b, int block, int waves) {
     b->point_block = block;
     if (waves > 0) {
-        b->point_grid = waves * wave_blocks(b, 0, block);
-        b->flux_grid = waves * wave_blocks(b, 2, 128);
+        b->point_grid = waves * batch_wave(b, 0, block);
+        b->flux_grid = waves * batch_wave(b, 2, 128);
     } else {
         b->point_grid = (b->ntot + block - 1) / block;
         b->flux_grid = b->ntiles;

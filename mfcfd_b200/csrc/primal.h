@@ -124,6 +124,8 @@ int batch_occupancy32(int kind, int block, size_t smem);
 // dynamic shared memory of the flux passes for stencils of kp slots
 size_t flux_smem_bytes(int kp);
 size_t flux32_smem_bytes(int kp);
+// blocks of one wave of resident blocks of a pass on device dev
+int wave_blocks(int dev, int kind, int block, size_t smem, bool fp32);
 // q and spd from prim (set_state)
 void launch_init_state(const Geom &g, const R4 *prim, R4 *q, double *spd, cudaStream_t s);
 

@@ -438,11 +438,9 @@ int batch_occupancy32(int kind, int block, size_t smem) {
 namespace {
 int wave32(int kind, int block, size_t smem, int grid) {
     if (grid > 0) return grid;
-    int dev = 0, sms = 1;
+    int dev = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int nb = batch_occupancy32(kind, block, smem);
-    return (sms > 0 ? sms : 1) * (nb > 0 ? nb : 1);
+    return wave_blocks(dev, kind, block, smem, true);
 }
 }  // namespace
 

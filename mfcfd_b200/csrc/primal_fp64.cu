@@ -564,14 +564,19 @@ cudaError_t init_kernels() {
                                 GROUPS * 20 * REC * (int)sizeof(double));
 }
 
+int wave_blocks(int dev, int kind, int block, size_t smem, bool fp32) {
+    int sms = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return std::max(sms, 1) * std::max(1, batch_occupancy(kind, fp32, block, smem));
+}
+
 namespace {
-// blocks of one wave of resident blocks of a batched kernel (grid == 0)
+// grid of a launch: `grid` blocks, or one wave of resident blocks (grid == 0)
 int wave(int kind, int block, size_t smem, int grid) {
     if (grid > 0) return grid;
-    int dev = 0, sms = 1;
+    int dev = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return std::max(sms, 1) * std::max(1, batch_occupancy(kind, false, block, smem));
+    return wave_blocks(dev, kind, block, smem, false);
 }
 }  // namespace
 

@@ -88,11 +88,13 @@ def naca_thickness(x: np.ndarray, t: float) -> np.ndarray:
                       + 0.2843 * x**3 - 0.1036 * x**4)
 
 
-def _stretch_ratio(length: np.ndarray, d1: float, nseg: int) -> np.ndarray:
+def _stretch_ratio(length: np.ndarray, d1, nseg: int) -> np.ndarray:
     """Solve d1 * (r**nseg - 1)/(r - 1) = length for r > 1, per ray (bisection)."""
     lo = np.full_like(length, 1.0 + 1e-12)
     hi = np.full_like(length, 2.0)
-    f = lambda r: d1 * np.expm1(nseg * np.log(r)) / (r - 1.0) - length
+    def f(r):
+        with np.errstate(over="ignore"):
+            return d1 * np.expm1(nseg * np.log(r)) / (r - 1.0) - length
     while np.any(f(hi) < 0):
         hi = np.where(f(hi) < 0, hi * 2.0, hi)
     for _ in range(200):
@@ -217,12 +219,15 @@ def naca_ogrid(ni: int, nj: int, thickness: float = 0.12, radius: float = 20.0,
     """NACA 00tt O-grid point cloud of ni (around) x nj (radial) points.
 
     Ring j=0 is the airfoil (flag_1=0, flag_2=1) with ``spacing`` "cosine"
-    (clustered at both ends) or "halfcos" (clustered at the leading edge);
+    (clustered at both ends), "halfcos" (clustered at the leading edge) or
+    "arc" (uniform in arc length on each surface);
     ring j=nj-1 a circle of ``radius`` chords about (0.5, 0) (flag_1=2).
     Points on both rings run clockwise in i (i=0 is the trailing edge), so
     ``right`` is the next point clockwise and the reference's normal formula
     points out of the body and out of the domain.  Radial spacing grows
-    geometrically from ``first_spacing`` (ratio solved per ray).  ``rays``
+    geometrically from ``first_spacing`` (ratio solved per ray); "match"
+    makes it, per ray, the wall spacing at the ray's foot, so that the cells
+    next to the wall are near-square.  ``rays``
     "straight" joins wall point i to outer point i; "blend" leaves the wall
     along the wall normal on the rounded front and turns to the straight line
     towards the trailing edge and the outer circle.  Interior points are
@@ -243,6 +248,17 @@ def naca_ogrid(ni: int, nj: int, thickness: float = 0.12, radius: float = 20.0,
         xw = 0.5 * (1.0 + np.cos(phi))
     elif spacing == "halfcos":
         xw = 1.0 - np.cos(0.5 * math.pi * np.abs(1.0 - phi / math.pi))
+    elif spacing == "arc":
+        if ni % 2:
+            raise ValueError("spacing 'arc' needs an even ni")
+        h = ni // 2
+        xs = 0.5 * (1.0 + np.cos(np.linspace(0.0, math.pi, 20001)))  # TE -> LE
+        cum = np.concatenate(([0.0], np.cumsum(np.hypot(np.diff(xs),
+                                                       np.diff(naca_thickness(xs, thickness))))))
+        xh = np.interp(np.linspace(0.0, cum[-1], h + 1), cum, xs)
+        xw = np.empty(ni)
+        xw[:h + 1] = xh
+        xw[h + 1:] = xh[1:h][::-1]
     else:
         raise ValueError(f"unknown spacing {spacing!r}")
     yt = naca_thickness(xw, thickness)
@@ -258,15 +274,40 @@ def naca_ogrid(ni: int, nj: int, thickness: float = 0.12, radius: float = 20.0,
     yw[on_axis] = 0.0
     dxr, dyr = xo - xw, yo - yw
     length = np.hypot(dxr, dyr)
-    r = _stretch_ratio(length, first_spacing, nj - 1)
+    if isinstance(first_spacing, str):
+        if first_spacing != "match":
+            raise ValueError(f"unknown first_spacing {first_spacing!r}")
+        # per ray: the mean of the two wall segments at the ray's foot
+        seg = np.hypot(np.roll(xw, -1) - xw, np.roll(yw, -1) - yw)
+        d1 = 0.5 * (seg + np.roll(seg, 1))
+    else:
+        d1 = np.full(ni, float(first_spacing))
+    r = _stretch_ratio(length, d1, nj - 1)
     j = np.arange(nj)[:, None]
-    s = first_spacing * np.expm1(j * np.log(r)[None, :]) / (r[None, :] - 1.0)
+    s = d1[None, :] * np.expm1(j * np.log(r)[None, :]) / (r[None, :] - 1.0)
     s[-1, :] = length
     frac = s / length[None, :]
     ex, ey = dxr / length, dyr / length
     if rays == "straight":
         X = xw[None, :] + s * ex[None, :]
         Y = yw[None, :] + s * ey[None, :]
+    elif rays == "smooth":
+        # Ray direction b: the outward wall normal averaged over a window of
+        # ni/32 rays each side, so the rays fan out gradually around the
+        # sharp trailing edge instead of leaving it almost tangent to the
+        # surface; the ray bends from b to the straight line as in "blend".
+        tdx, tdy = np.roll(xw, -1) - np.roll(xw, 1), np.roll(yw, -1) - np.roll(yw, 1)
+        tn = np.hypot(tdx, tdy)
+        nwx, nwy = -tdy / tn, tdx / tn
+        wdw = max(2, ni // 32)
+        bx = sum(np.roll(nwx, m) for m in range(-wdw, wdw + 1))
+        by = sum(np.roll(nwy, m) for m in range(-wdw, wdw + 1))
+        bn = np.hypot(bx, by)
+        bx, by = bx / bn, by / bn
+        lam = 0.5
+        off = lam * (-np.expm1(-s / lam)) * (1.0 - frac)
+        X = xw[None, :] + s * ex[None, :] + off * (bx - ex)[None, :]
+        Y = yw[None, :] + s * ey[None, :] + off * (by - ey)[None, :]
     elif rays == "blend":
         # Ray direction b: the wall normal over the rounded front, turning to
         # the straight line towards the sharp trailing edge.  Along a ray the
@@ -366,14 +407,20 @@ def naca_ogrid(ni: int, nj: int, thickness: float = 0.12, radius: float = 20.0,
 # Configurations the benchmarks and parity tests use (ni x nj, flow).  C1 uses
 # a 5e-3 first spacing: at 160 points around, 1e-3 gives near-wall cells of
 # aspect ratio ~20 on which the scheme has a growing wall mode (the oracle
-# diverges near iteration 560 at CFL 0.2 and near 1100 at CFL 0.1).
+# diverges near iteration 560 at CFL 0.2 and near 1100 at CFL 0.1).  The
+# same mode grows at the sharp trailing edge of the fine cosine-spaced grids,
+# where straight rays leave the surface at ~7 degrees: C2 and C5 end on a NaN
+# residue near iteration 370 (their benchmarks time the first iterations).
+# C3 and the batched instances use wall points uniform in arc length with
+# square first cells ("arc", "match"), stable over 3000 iterations at
+# M 0.63-0.85 up to 640x400.
 CONFIGS = {
     "C1": dict(ni=160, nj=100, mach=0.63, aoa=2.0, inner_iterations=0, iters=1000,
                seed=1000, first_spacing=5e-3),
     "C2": dict(ni=1280, nj=800, mach=0.85, aoa=1.0, inner_iterations=3, iters=5000,
                seed=2000, first_spacing=1e-3),
     "C3": dict(ni=640, nj=400, mach=0.63, aoa=2.0, inner_iterations=0, iters=2000,
-               seed=3000, first_spacing=1e-3),
+               seed=3000, first_spacing="match", spacing="arc"),
     "C5": dict(ni=2560, nj=1600, mach=0.8, aoa=1.25, inner_iterations=0, iters=5000,
                seed=5000, first_spacing=1e-3),
     # profiling case: the C2 flow on half the points (working set still > L2)
@@ -387,20 +434,20 @@ def config_grid(name: str, **overrides) -> Grid:
     c = dict(CONFIGS[name])
     c.update(overrides)
     return naca_ogrid(c["ni"], c["nj"], seed=c["seed"], first_spacing=c["first_spacing"],
-                      name=f"{name}_{c['ni']}x{c['nj']}")
+                      spacing=c.get("spacing", "cosine"), name=f"{name}_{c['ni']}x{c['nj']}")
 
 
 def batch_instances(n_inst: int = 64, config: int = 4, n_min: int = 4000, n_max: int = 256000,
                     aspect: float = 1.6, mach=(0.5, 0.8), aoa=(-2.0, 4.0),
-                    thickness=(0.08, 0.16), first_spacing: float = 5e-3, inner_iterations=0,
-                    build: bool = True):
+                    thickness=(0.08, 0.16), first_spacing="match", spacing="arc",
+                    inner_iterations=0, build: bool = True):
     """Instances of a batched workload: instance k draws from PCG64 seeded
     1000*config + k a point count log-uniform in [n_min, n_max] (ni x nj with
     ni ~ aspect*nj, ni even), a Mach number, an angle of attack and a
     thickness, each uniform in its range.  Returns (grids, flows, specs); with
-    build=False the grids are None (only the draws).  The 5e-3 first spacing
-    is C1's: the coarse instances need it to stay free of the growing wall
-    mode (see CONFIGS)."""
+    build=False the grids are None (only the draws).  The grids are C3's kind
+    (arc-length wall spacing, square first cells), free of the growing
+    trailing-edge mode (see CONFIGS)."""
     grids, flows, specs = [], [], []
     for k in range(n_inst):
         rng = np.random.default_rng(1000 * config + k)
@@ -415,7 +462,7 @@ def batch_instances(n_inst: int = 64, config: int = 4, n_min: int = 4000, n_max:
         flow = dict(FLOW_DEFAULTS)
         flow.update(mach=m, aoa=a, inner_iterations=inner_iterations)
         flows.append(flow)
-        grids.append(naca_ogrid(ni, nj, thickness=t, seed=spec["seed"],
+        grids.append(naca_ogrid(ni, nj, thickness=t, seed=spec["seed"], spacing=spacing,
                                 first_spacing=first_spacing, name=f"B{config}_{k}_{ni}x{nj}")
                      if build else None)
     return grids, flows, specs
