@@ -16,6 +16,9 @@ FP64 -- the workload the headline metric is quoted on.  Grids are synthetic
             over its CUDA-event duration, against the measured HBM copy peak
   cpu_baseline  the oracle (C restatement of src_mpi_primal) on the host's
             cores, on a bounded sample of the same workload
+  fp32_mixed, adjoint, batch  the FP32-mixed loop on the same workload, the
+            reverse-mode cost against the primal, and the 64-instance batched
+            workload against one handle at a time
 
 ``--impl reference`` times that CPU restatement alone (the reference itself
 is Fortran + MPI + PETSc + HDF5 and cannot be built on these machines).
@@ -76,8 +79,8 @@ def measured_peaks() -> dict:
 
 
 def profiled_traffic(workload: str):
-    """dram bytes per launch of k_flux from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "k_flux_fp64_c2.md")
+    """dram bytes per launch of kb_flux from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "kb_flux_fp64_c2.md")
     if not os.path.exists(p):
         return None
     with open(p) as fh:
@@ -240,6 +243,64 @@ def adjoint_cost(args, stream, world, dist):
             "J": J, "grad_max": float(max(np.abs(dx).max(), np.abs(dy).max()))}
 
 
+def batch_leg(args, stream, world, rank, dist):
+    """The batched workload: 64 seeded instances (4k-256k points, M, aoa and
+    thickness drawn per instance), sharded across ranks with no exchange,
+    advanced together by one Batch for a bounded number of iterations (tol
+    -8 retires an instance early), device-timed on the stream; beside it the
+    same instances run one Solver at a time for the same iterations."""
+    import torch
+    from mfcfd_b200.batch import Batch
+    from mfcfd_b200.grid import batch_instances
+    from mfcfd_b200.solver import Solver
+    grids, flows, specs = batch_instances(args.batch_instances)
+    mine = list(range(rank, len(grids), world))
+    grids, flows = [grids[i] for i in mine], [flows[i] for i in mine]
+    n = args.batch_iters
+    with Batch(grids, flows) as b:
+        b.set_stream(stream.cuda_stream)
+        tuned_ms = b.tune(4)
+        b.run(args.warmup)
+        torch.cuda.synchronize()
+        l0 = b.launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = b.run(n, tol=-8.0)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        batch_ms = e0.elapsed_time(e1)
+        launches = b.launch_count() - l0
+        info = b.info()
+    work = sum(g.n * int(d) for g, d in zip(grids, r.iters_done))
+    seq_ms = 0.0
+    for g, f, d in zip(grids, flows, r.iters_done):
+        with Solver(g, **f) as s:
+            s.set_stream(stream.cuda_stream)
+            s.run(args.warmup)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            s.run(int(d))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            seq_ms += e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([batch_ms, seq_ms, float(work)], device="cuda", dtype=torch.float64)
+        tmax = t[:2].clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        tw = t[2:].clone()
+        dist.all_reduce(tw, op=dist.ReduceOp.SUM)
+        batch_ms, seq_ms, work = float(tmax[0]), float(tmax[1]), float(tw[0])
+    states = {k: r.state.count(k) for k in sorted(set(r.state))}
+    return {"config": (f"{args.batch_instances} NACA 00tt O-grids, N log-uniform in [4k, 256k] "
+                       f"(seeded draws), M in [0.5, 0.8], aoa in [-2, 4] deg, t in [0.08, 0.16], "
+                       f"FP64, retire at residue <= -8 or {n} iterations"),
+            "instances_per_rank": len(grids), "points_per_rank": int(sum(g.n for g in grids)),
+            "iterations": n, "value": work / (batch_ms / 1e3) / 1e6, "unit": UNIT,
+            "ms": batch_ms, "one_handle_at_a_time_ms": seq_ms,
+            "speedup_vs_one_at_a_time": seq_ms / batch_ms, "states_rank0": states,
+            "gpu_launches": launches, "launch_shape": info, "tuner_ms_per_iter": tuned_ms}
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -254,6 +315,9 @@ def main():
     ap.add_argument("--adjoint-iters", type=int, default=50,
                     help="iterations of the adjoint-cost leg (0 = skip)")
     ap.add_argument("--adjoint-config", default="C3")
+    ap.add_argument("--batch-iters", type=int, default=100,
+                    help="iterations of the batched-workload leg (0 = skip)")
+    ap.add_argument("--batch-instances", type=int, default=64)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "mfcfd":
         args.warmup = 3
@@ -356,7 +420,7 @@ def main():
     traffic = profiled_traffic(args.config)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
-                "kernel": "k_flux (flux residual + state update, one SSPRK stage)",
+                "kernel": "kb_flux (flux residual + state update, one SSPRK stage)",
                 "algorithmic_bytes_per_launch": flux_bytes,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6.65 TB/s",
                 "note": "the kernel is bound by FP64 issue (exp/erf/log/div), not HBM: see DESIGN.md"}
@@ -400,6 +464,10 @@ def main():
     if args.adjoint_iters > 0:
         adjoint = adjoint_cost(args, stream, world, dist)
 
+    batch = None
+    if args.batch_iters > 0:
+        batch = batch_leg(args, stream, world, rank, dist)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(grid, flow, args.cpu_seconds)
@@ -415,6 +483,7 @@ def main():
             "final_residue": float(res[-1]) if len(res) else None,
             "fp32_mixed": fp32,
             "adjoint": adjoint,
+            "batch": batch,
         }
         print(json.dumps(line), flush=True)
     solver.close()
