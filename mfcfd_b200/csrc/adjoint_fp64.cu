@@ -48,7 +48,10 @@ __device__ __forceinline__ KState kst_load(const double *e) {
 }
 
 // state_update_b (state_update.F90:10-141, reverse)
-__global__ void __launch_bounds__(BLK)
+#ifndef ADJ_MIN_BLOCKS
+#define ADJ_MIN_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(BLK, ADJ_MIN_BLOCKS)
 k_update_b(Geom g, Consts c, AdjConsts a, const R4 *__restrict__ prim_in,
            const R4 *__restrict__ prim_old, const R4 *__restrict__ fr,
            const double *__restrict__ pb_out, double *__restrict__ pb_in,
@@ -140,8 +143,11 @@ k_update_b(Geom g, Consts c, AdjConsts a, const R4 *__restrict__ prim_in,
     nyb[i] += nybv;
 }
 
-// cal_flux_residual_b: same lane layout as k_flux.
-__global__ void __launch_bounds__(BLK)
+// cal_flux_residual_b: same lane layout as the forward flux pass.
+#ifndef FLUXB_MIN_BLOCKS
+#define FLUXB_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(BLK, FLUXB_MIN_BLOCKS)
 k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict__ dq,
          const double *__restrict__ qm, const double *__restrict__ delta,
          const double *__restrict__ frb, double *__restrict__ qb, double *__restrict__ dqb,
@@ -313,13 +319,10 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
         deltab[i] += db;
     }
     __syncwarp();
-    // phase C: per slot reverse
+    // phase C: per slot reverse (the neighbour's side first, its record
+    // written before the point's own inputs are loaded, so the two sides'
+    // working sets are not live together)
     if (valid) {
-        const R4 qv = ld4(q_in + i);
-        const double qi[4] = {qv.a, qv.b, qv.c, qv.d};
-        double dxi[4], dyi[4], qmaxi[4], qmini[4];
-        ld8a(dq + 8 * (size_t)i, dxi, dyi);
-        ld8a(qm + 8 * (size_t)i, qmaxi, qmini);
         for (int r = lane; r < nb; r += LPP) {
             const int k = g.conn[r * g.n + i];
             const double2 pk = g.xy[k];
@@ -383,10 +386,6 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
                    qmaxkb[4] = {0, 0, 0, 0}, qminkb[4] = {0, 0, 0, 0};
             reconstruct_b(qk, dxk, dyk, qmaxk, qmink, g.eps2[k], delx, dely, c.gm1, pr_[6], pku1b,
                           pku2b, pkrb, pkpb, qkb, dxkb, dykb, qmaxkb, qminkb, delxb, delyb);
-            double qib[4] = {0, 0, 0, 0}, dxib[4] = {0, 0, 0, 0}, dyib[4] = {0, 0, 0, 0},
-                   qmaxib[4] = {0, 0, 0, 0}, qminib[4] = {0, 0, 0, 0};
-            reconstruct_b(qi, dxi, dyi, qmaxi, qmini, g.eps2[i], delx, dely, c.gm1, pr_[2], piu1b,
-                          piu2b, pirb, pipb, qib, dxib, dyib, qmaxib, qminib, delxb, delyb);
             double *cb = contrib + ((size_t)i * g.kp + r) * ADJ_CW;
             for (int m = 0; m < 4; ++m) {
                 cb[m] = qkb[m];
@@ -395,6 +394,15 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
                 cb[12 + m] = qmaxkb[m];
                 cb[16 + m] = qminkb[m];
             }
+            const R4 qv = ld4(q_in + i);
+            const double qi[4] = {qv.a, qv.b, qv.c, qv.d};
+            double dxi[4], dyi[4], qmaxi[4], qmini[4];
+            ld8a(dq + 8 * (size_t)i, dxi, dyi);
+            ld8a(qm + 8 * (size_t)i, qmaxi, qmini);
+            double qib[4] = {0, 0, 0, 0}, dxib[4] = {0, 0, 0, 0}, dyib[4] = {0, 0, 0, 0},
+                   qmaxib[4] = {0, 0, 0, 0}, qminib[4] = {0, 0, 0, 0};
+            reconstruct_b(qi, dxi, dyi, qmaxi, qmini, g.eps2[i], delx, dely, c.gm1, pr_[2], piu1b,
+                          piu2b, pirb, pipb, qib, dxib, dyib, qmaxib, qminib, delxb, delyb);
             cb[20] = delxb;
             cb[21] = delyb;
             // self contribution of this slot, summed in slot order below
@@ -428,7 +436,7 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
 
 // eval_q_inner_loop_b: one inner iteration; dqb_out is the adjoint of its
 // output, dqb_in receives the point's own share of the input adjoint.
-__global__ void __launch_bounds__(BLK)
+__global__ void __launch_bounds__(BLK, ADJ_MIN_BLOCKS)
 k_inner_b(Geom g, const R4 *__restrict__ q, const double *__restrict__ dq_in,
           const double *__restrict__ dqb_out, double *__restrict__ dqb_in, double *__restrict__ qb,
           double *__restrict__ xb, double *__restrict__ yb, double *__restrict__ contrib) {
@@ -519,7 +527,7 @@ k_inner_b(Geom g, const R4 *__restrict__ q, const double *__restrict__ dq_in,
 }
 
 // eval_q_derivatives_b (+ func_delta_b on the first stage)
-__global__ void __launch_bounds__(BLK)
+__global__ void __launch_bounds__(BLK, ADJ_MIN_BLOCKS)
 k_grad_b(Geom g, Consts c, const R4 *__restrict__ q, const R4 *__restrict__ primA,
          const double *__restrict__ dqb, const double *__restrict__ qmb,
          const double *__restrict__ deltab, int with_delta, double *__restrict__ qb,
@@ -633,34 +641,48 @@ k_grad_b(Geom g, Consts c, const R4 *__restrict__ q, const R4 *__restrict__ prim
 }
 
 // Adds the neighbour contributions per point in the fixed transposed order.
+// MODE fixes the record width (22 flux, 14 inner, 10 grad fields) so the
+// accumulators stay in registers; records are read as 16-byte pairs.
+template <int MODE>
 __global__ void __launch_bounds__(256)
-k_gather(int n, int kp, const int *__restrict__ tptr, const int *__restrict__ tlist,
-         const double *__restrict__ contrib, int mode, double *__restrict__ a4,
-         double *__restrict__ a8, double *__restrict__ b8, double *__restrict__ xb,
-         double *__restrict__ yb) {
+k_gather(int n, const int *__restrict__ tptr, const int *__restrict__ tlist,
+         const double *__restrict__ contrib, double *__restrict__ a4, double *__restrict__ a8,
+         double *__restrict__ b8, double *__restrict__ xb, double *__restrict__ yb) {
+    constexpr int NF = MODE == ADJ_GATHER_FLUX ? 22 : (MODE == ADJ_GATHER_INNER ? 14 : 10);
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    double acc[22];
-    const int nf = mode == ADJ_GATHER_FLUX ? 22 : (mode == ADJ_GATHER_INNER ? 14 : 10);
-    for (int f = 0; f < 22; ++f) acc[f] = 0.0;
-    for (int e = tptr[k]; e < tptr[k + 1]; ++e) {
-        const double *cb = contrib + (size_t)tlist[e] * ADJ_CW;
-        for (int f = 0; f < nf; ++f) acc[f] = acc[f] + cb[f];
+    double acc[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) acc[f] = 0.0;
+    const int e1 = tptr[k + 1];
+    for (int e = tptr[k]; e < e1; ++e) {
+        const double2 *cb = reinterpret_cast<const double2 *>(contrib + (size_t)tlist[e] * ADJ_CW);
+#pragma unroll
+        for (int f = 0; f < NF / 2; ++f) {
+            const double2 v = __ldg(cb + f);
+            acc[2 * f] = acc[2 * f] + v.x;
+            acc[2 * f + 1] = acc[2 * f + 1] + v.y;
+        }
     }
+#pragma unroll
     for (int m = 0; m < 4; ++m) a4[4 * (size_t)k + m] += acc[m];
-    if (mode == ADJ_GATHER_FLUX) {
+    if (MODE == ADJ_GATHER_FLUX) {
+#pragma unroll
         for (int m = 0; m < 8; ++m) a8[8 * (size_t)k + m] += acc[4 + m];
+#pragma unroll
         for (int m = 0; m < 8; ++m) b8[8 * (size_t)k + m] += acc[12 + m];
-        xb[k] += acc[20];
-        yb[k] += acc[21];
-    } else if (mode == ADJ_GATHER_INNER) {
+        xb[k] += acc[NF - 2];
+        yb[k] += acc[NF - 1];
+    } else if (MODE == ADJ_GATHER_INNER) {
+#pragma unroll
         for (int m = 0; m < 8; ++m) a8[8 * (size_t)k + m] += acc[4 + m];
-        xb[k] += acc[12];
-        yb[k] += acc[13];
+        xb[k] += acc[NF - 2];
+        yb[k] += acc[NF - 1];
     } else {
+#pragma unroll
         for (int m = 0; m < 4; ++m) b8[4 * (size_t)k + m] += acc[4 + m];
-        xb[k] += acc[8];
-        yb[k] += acc[9];
+        xb[k] += acc[NF - 2];
+        yb[k] += acc[NF - 1];
     }
 }
 
@@ -777,7 +799,16 @@ void launch_grad_b(const Geom &g, const Consts &c, const R4 *q, const R4 *primA,
 void launch_gather(int n, int kp, const int *tptr, const int *tlist, const double *contrib,
                    int mode, double *a4, double *a8, double *b8, double *xb, double *yb,
                    cudaStream_t s) {
-    k_gather<<<nblk(n, 256), 256, 0, s>>>(n, kp, tptr, tlist, contrib, mode, a4, a8, b8, xb, yb);
+    (void)kp;
+    if (mode == ADJ_GATHER_FLUX)
+        k_gather<ADJ_GATHER_FLUX><<<nblk(n, 256), 256, 0, s>>>(n, tptr, tlist, contrib, a4, a8, b8,
+                                                              xb, yb);
+    else if (mode == ADJ_GATHER_INNER)
+        k_gather<ADJ_GATHER_INNER><<<nblk(n, 256), 256, 0, s>>>(n, tptr, tlist, contrib, a4, a8,
+                                                               b8, xb, yb);
+    else
+        k_gather<ADJ_GATHER_GRAD><<<nblk(n, 256), 256, 0, s>>>(n, tptr, tlist, contrib, a4, a8, b8,
+                                                              xb, yb);
 }
 
 void launch_qvar_b(int n, const R4 *prim, const double *qb, double *pb, cudaStream_t s) {
