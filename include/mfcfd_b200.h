@@ -107,6 +107,18 @@ typedef struct mfcfd mfcfd_t;
 int mfcfd_adjoint(mfcfd_t *h, int objective, int n_iters, size_t ckpt_bytes, double *J,
                   double *dJdx, double *dJdy, int *n_forward);
 
+/* Forward-mode (tangent) derivative of the loop (the reference's Q_LSKUM_D,
+ * src_mpi_forward/sensitivity_files/q_lskum_d.F90:28-89, which seeds
+ * pointd%x(1) = 1).  From the handle's current state (held fixed) it runs
+ * n_iters iterations with the grid moved along the direction (dx, dy) per
+ * point (caller order; NULL = 0) and writes J = sum over shapes of Cl
+ * (objective 0) or Cd (objective 1) of the final state and dJ/de along the
+ * direction.  For the gradient of mfcfd_adjoint over the same iterations,
+ * dJ/de = sum_i dJdx_i dx_i + dJdy_i dy_i.  The handle's state is left
+ * unchanged.  FP64 handles with power == 0 only (else MFCFD_ERR_ARG). */
+int mfcfd_tangent(mfcfd_t *h, int objective, int n_iters, const double *dx, const double *dy,
+                  double *J, double *dJ);
+
 /* Sets the default parameters of the reference's readcase (cfl 0,
  * power 0, vl_const 150, ssprk43, no inner iterations, legacy format) with
  * Mach 0.63 and aoa 2 (parameter.F90:5-6). */

@@ -55,14 +55,18 @@ struct Consts {
 
 // ---------------------------------------------------------------------------
 // q_variables.F90:8-37 eval_q_variables
-__device__ __forceinline__ void q_from_prim(double rho, double u1, double u2, double pr,
-                                            double q[4]) {
-    double beta = 0.5 * rho / pr;
-    q[0] = (log(rho) + (log(beta) * 2.5)) - beta * (u1 * u1 + u2 * u2);
-    double two_times_beta = 2.0 * beta;
+template <class T>
+__device__ __forceinline__ void q_from_prim_t(T rho, T u1, T u2, T pr, T q[4]) {
+    T beta = T(0.5) * rho / pr;
+    q[0] = (log(rho) + (log(beta) * T(2.5))) - beta * (u1 * u1 + u2 * u2);
+    T two_times_beta = T(2.0) * beta;
     q[1] = two_times_beta * u1;
     q[2] = two_times_beta * u2;
     q[3] = -two_times_beta;
+}
+__device__ __forceinline__ void q_from_prim(double rho, double u1, double u2, double pr,
+                                            double q[4]) {
+    q_from_prim_t<double>(rho, u1, u2, pr, q);
 }
 
 // q_variables.F90:230-256 qtilde_to_primitive.  T is double on the FP64
@@ -198,42 +202,51 @@ __device__ __forceinline__ void flux_quad(const KStateT<T> &s, T s1, T s2, T G[4
 }
 
 // state_update.F90:144-163 primitive_to_conserved
-__device__ __forceinline__ void prim_to_conserved(double rho, double u1, double u2, double pr,
-                                                  double nx, double ny, double U[4]) {
+template <class T>
+__device__ __forceinline__ void prim_to_conserved_t(T rho, T u1, T u2, T pr, T nx, T ny, T U[4]) {
     U[0] = rho;
-    double temp1 = rho * u1;
-    double temp2 = rho * u2;
-    U[3] = 2.5 * pr + 0.5 * (temp1 * temp1 + temp2 * temp2) / rho;
+    T temp1 = rho * u1;
+    T temp2 = rho * u2;
+    U[3] = T(2.5) * pr + T(0.5) * (temp1 * temp1 + temp2 * temp2) / rho;
     U[1] = temp1 * ny - temp2 * nx;
     U[2] = temp1 * nx + temp2 * ny;
+}
+__device__ __forceinline__ void prim_to_conserved(double rho, double u1, double u2, double pr,
+                                                  double nx, double ny, double U[4]) {
+    prim_to_conserved_t<double>(rho, u1, u2, pr, nx, ny, U);
 }
 
 // state_update.F90:239-294 conserved_vector_Ubar.  The freestream half
 // (inf[0..4] = u1_inf_rot, u2_inf_rot, e_inf, A2n_inf, B2_inf) depends only on
 // the geometry and is computed once on the host.
-__device__ __forceinline__ void conserved_ubar(double rho, double u1, double u2, double pr,
-                                               double nx, double ny, const double *inf,
-                                               double pi, double gm1, double Ubar[4]) {
-    const double rho_inf = 1.0;
-    double u1_inf_rot = inf[0], u2_inf_rot = inf[1], e_inf = inf[2], A2n_inf = inf[3],
-           B2_inf = inf[4];
-    double tx = ny, ty = -nx;
-    double u1_rot = u1 * tx + u2 * ty;
-    double u2_rot = u1 * nx + u2 * ny;
-    double temp1 = (u1_rot * u1_rot + u2_rot * u2_rot);
-    double e = pr / (rho * gm1) + 0.5 * (temp1);
-    double beta = (rho) / (2.0 * pr);
-    double S2 = u2_rot * sqrt(beta);
-    double B2 = exp(-S2 * S2) / (2.0 * sqrt(pi * beta));
-    double A2p = 0.5 * (1.0 + erf(S2));
+template <class T>
+__device__ __forceinline__ void conserved_ubar_t(T rho, T u1, T u2, T pr, T nx, T ny,
+                                                 const T *inf, T pi, T gm1, T Ubar[4]) {
+    const T rho_inf = T(1.0);
+    T u1_inf_rot = inf[0], u2_inf_rot = inf[1], e_inf = inf[2], A2n_inf = inf[3],
+      B2_inf = inf[4];
+    T tx = ny, ty = -nx;
+    T u1_rot = u1 * tx + u2 * ty;
+    T u2_rot = u1 * nx + u2 * ny;
+    T temp1 = (u1_rot * u1_rot + u2_rot * u2_rot);
+    T e = pr / (rho * gm1) + T(0.5) * (temp1);
+    T beta = (rho) / (T(2.0) * pr);
+    T S2 = u2_rot * sqrt(beta);
+    T B2 = exp(-S2 * S2) / (T(2.0) * sqrt(pi * beta));
+    T A2p = T(0.5) * (T(1.0) + erf(S2));
     Ubar[0] = (rho_inf * A2n_inf) + (rho * A2p);
     Ubar[1] = (rho_inf * u1_inf_rot * A2n_inf) + (rho * u1_rot * A2p);
     temp1 = rho_inf * (u2_inf_rot * A2n_inf - B2_inf);
-    double temp2 = rho * (u2_rot * A2p + B2);
+    T temp2 = rho * (u2_rot * A2p + B2);
     Ubar[2] = temp1 + temp2;
-    temp1 = (rho_inf * A2n_inf * e_inf - 0.5 * rho_inf * u2_inf_rot * B2_inf);
-    temp2 = (rho * A2p * e + 0.5 * rho * u2_rot * B2);
+    temp1 = (rho_inf * A2n_inf * e_inf - T(0.5) * rho_inf * u2_inf_rot * B2_inf);
+    temp2 = (rho * A2p * e + T(0.5) * rho * u2_rot * B2);
     Ubar[3] = temp1 + temp2;
+}
+__device__ __forceinline__ void conserved_ubar(double rho, double u1, double u2, double pr,
+                                               double nx, double ny, const double *inf,
+                                               double pi, double gm1, double Ubar[4]) {
+    conserved_ubar_t<double>(rho, u1, u2, pr, nx, ny, inf, pi, gm1, Ubar);
 }
 
 }  // namespace lskum

@@ -137,6 +137,21 @@ class Solver:
         self.it = (self.it or 0) + n_iters
         return J.value, dx, dy, nf.value
 
+    def tangent(self, n_iters: int, dx=None, dy=None, objective: str = "cd"):
+        """Forward-mode derivative: (J, dJ/de) after ``n_iters`` iterations
+        from the current state with the grid moved along (dx, dy) per point
+        (forward mode; the state is left unchanged)."""
+        def arr(a):
+            return None if a is None else _dptr(np.ascontiguousarray(a, dtype=np.float64))
+        keep = [np.ascontiguousarray(a, dtype=np.float64) for a in (dx, dy) if a is not None]
+        J, dJ = C.c_double(0.0), C.c_double(0.0)
+        obj = {"cl": 0, "cd": 1}[objective.lower()]
+        pdx = _dptr(keep[0]) if dx is not None else None
+        pdy = _dptr(keep[-1]) if dy is not None else None
+        _lib.check(self.lib.mfcfd_tangent(self.h, obj, int(n_iters), pdx, pdy, C.byref(J),
+                                          C.byref(dJ)), self.h, "mfcfd_tangent")
+        return J.value, dJ.value
+
     # diagnostics -----------------------------------------------------------
     def keep_diagnostics(self, on: bool = True) -> None:
         _lib.check(self.lib.mfcfd_keep_diagnostics(self.h, 1 if on else 0), self.h,
