@@ -155,6 +155,16 @@ int mfcfd_forces(mfcfd_t *h, double *cl, double *cd, double *cm, double *cp);
 /* Uses the given cudaStream_t (NULL = the handle's own stream). */
 int mfcfd_set_stream(mfcfd_t *h, void *stream);
 
+/* The CUDA tree's post-processing fields of the current state, per point in
+ * caller order (any may be NULL): the Mach number as print_primal_output
+ * forms it, sqrt(|u|^2 / c) (src_cuda/post_processing.F90:24-27); the entropy
+ * |log(p/rho^gamma) - log(pr_inf)| and their sum over the points
+ * (src_cuda/compute_entropy.F90:10-30); the D2-distance adaptation sensor
+ * normalised by its maximum (src_cuda/adaptation_sensors.F90:7-101) -- the
+ * last three columns of output.dat. */
+int mfcfd_output_fields(mfcfd_t *h, double *mach, double *entropy, double *sensor,
+                        double *total_entropy);
+
 /* Copies an internal per-point array out in caller order, for stage-level
  * checks: "q" (4/pt, the last stage's input), "dq" (8/pt: d/dx of q1..q4 then
  * d/dy), "qm" (8/pt: max of q1..q4 then min), "delta" (1), "nx", "ny" (1),

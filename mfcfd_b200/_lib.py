@@ -29,7 +29,8 @@ EXPORTS = ("mfcfd_default_params", "mfcfd_create", "mfcfd_destroy", "mfcfd_set_s
            "mfcfd_get_state", "mfcfd_run", "mfcfd_forces", "mfcfd_set_stream",
            "mfcfd_get_array", "mfcfd_keep_diagnostics", "mfcfd_info", "mfcfd_strerror",
            "mfcfd_last_error", "mfcfd_launch_count", "mfcfd_profile_iteration",
-           "mfcfd_run_noalloc", "mfcfd_adjoint", "mfcfd_tangent", "mfcfd_batch_create", "mfcfd_batch_destroy",
+           "mfcfd_run_noalloc", "mfcfd_adjoint", "mfcfd_tangent", "mfcfd_output_fields",
+           "mfcfd_batch_create", "mfcfd_batch_destroy",
            "mfcfd_batch_set_stream", "mfcfd_batch_set_state", "mfcfd_batch_get_state",
            "mfcfd_batch_run", "mfcfd_batch_forces", "mfcfd_batch_tune", "mfcfd_batch_set_launch",
            "mfcfd_batch_info", "mfcfd_batch_last_error", "mfcfd_batch_launch_count")
@@ -97,6 +98,7 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     lib.mfcfd_run_noalloc.argtypes = [P, C.c_int, C.c_int, D, I]
     lib.mfcfd_adjoint.argtypes = [P, C.c_int, C.c_int, C.c_size_t, D, D, D, I]
     lib.mfcfd_tangent.argtypes = [P, C.c_int, C.c_int, D, D, D, D]
+    lib.mfcfd_output_fields.argtypes = [P, D, D, D, D]
     lib.mfcfd_batch_create.argtypes = [C.c_int, C.POINTER(C.POINTER(Grid)), C.POINTER(Params),
                                        C.POINTER(P)]
     lib.mfcfd_batch_destroy.argtypes = [P]

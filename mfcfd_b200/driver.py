@@ -5,8 +5,9 @@
 
 reads CASE_DIR/case.in (or input.nml), the grid CASE_DIR/point/partGrid,
 optionally CASE_DIR/restart/sol.dat, runs max_iters iterations on the GPU and
-writes CASE_DIR/residue, CASE_DIR/cp/cp-file and, every nsave iterations,
-CASE_DIR/solution/sol.dat, in the reference's formats.
+writes CASE_DIR/residue, CASE_DIR/cp/cp-file, every nsave iterations
+CASE_DIR/solution/sol.dat, and at the end the CUDA tree's CASE_DIR/output.dat
+(with Mach number, entropy and adaptation sensor), in the reference's formats.
 """
 from __future__ import annotations
 
@@ -53,13 +54,18 @@ def run_case(case_dir: str, grid=None, quiet: bool = False, chunk: int = 100) ->
                                   s.get_state(), it + 1, res_old)
         cl, cd, cm, cp = s.forces()
         prim = s.get_state()
+        # the CUDA tree's final output (meshfree_solver.F90:100-107 of src_cuda):
+        # adaptation sensor, entropy, output.dat
+        mach, ent, sen, total_entropy = s.output_fields()
+        io.write_output_dat(os.path.join(case_dir, "output.dat"), grid, prim, mach, ent, sen,
+                            it, res_old)
     run_time = time.perf_counter() - t0
     io.write_residue(os.path.join(case_dir, "residue"), its, res)
     io.write_cp(os.path.join(case_dir, "cp", "cp-file"), grid, cp)
     log(f" Vector function is {cd[0]:.17g}")
     log(f" Run time: {run_time:.6f} seconds")
     return dict(iterations=len(res), residue=res, cl=cl, cd=cd, cm=cm, cp=cp, prim=prim,
-                run_time=run_time)
+                run_time=run_time, total_entropy=total_entropy)
 
 
 if __name__ == "__main__":

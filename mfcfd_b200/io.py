@@ -217,6 +217,22 @@ def write_solution(path: str, grid: Grid, prim, it: int, res_old: float) -> None
                      + "".join(fortran_e(v) for v in (grid.x[i], grid.y[i], *prim[i])) + "\n")
 
 
+def write_output_dat(path: str, grid: Grid, prim, mach, entropy, sensor, it: int,
+                     res_old: float) -> None:
+    """The CUDA tree's output.dat (src_cuda/post_processing.F90:7-36): first
+    line ``max_points, it, res_old`` (list-directed), then
+    ``(2e30.20,2i4,7e30.20)`` rows: x, y, flag_1, qtdepth, rho, u1, u2, pr,
+    Mach number, entropy, sensor.  read_restart reads it back (11 columns)."""
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    with open(path, "w") as fh:
+        fh.write(f"{fortran_list_int(grid.n)}{fortran_list_int(it)}{fortran_list_real(res_old)}\n")
+        for i in range(grid.n):
+            fh.write(fortran_e(grid.x[i]) + fortran_e(grid.y[i])
+                     + f"{int(grid.flag_1[i]):4d}{int(grid.qtdepth[i]):4d}"
+                     + "".join(fortran_e(v) for v in (*prim[i], mach[i], entropy[i], sensor[i]))
+                     + "\n")
+
+
 def write_sensitivity(path: str, grid: Grid, dJdx, dJdy, it: int) -> None:
     """``local_points, it-1`` then ``(1i8, 2e30.20)``: id, dJ/dx, dJ/dy."""
     os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)

@@ -137,6 +137,16 @@ class Solver:
         self.it = (self.it or 0) + n_iters
         return J.value, dx, dy, nf.value
 
+    def output_fields(self):
+        """(mach, entropy, sensor, total entropy) of the current state: the
+        CUDA tree's output.dat columns (post_processing.F90:7-36,
+        compute_entropy.F90:10-30, adaptation_sensors.F90:7-101)."""
+        mach, ent, sen = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
+        tot = C.c_double(0.0)
+        _lib.check(self.lib.mfcfd_output_fields(self.h, _dptr(mach), _dptr(ent), _dptr(sen),
+                                                C.byref(tot)), self.h, "mfcfd_output_fields")
+        return mach, ent, sen, tot.value
+
     def tangent(self, n_iters: int, dx=None, dy=None, objective: str = "cd"):
         """Forward-mode derivative: (J, dJ/de) after ``n_iters`` iterations
         from the current state with the grid moved along (dx, dy) per point

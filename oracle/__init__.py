@@ -62,6 +62,8 @@ def _lib(variant: str = "") -> C.CDLL:
     lib.orc_get.restype = C.c_int
     lib.orc_get_split_counts.argtypes = [P, I]
     lib.orc_sum_res_sqr.argtypes = [P]
+    lib.orc_output_fields.argtypes = [P, D, D, D]
+    lib.orc_output_fields.restype = C.c_double
     lib.orc_sum_res_sqr.restype = C.c_double
     lib.orc_num_threads.restype = C.c_int
     _LIBS[name] = lib
@@ -144,6 +146,15 @@ class Oracle:
         return cl, cd, cm, cp
 
     # stage-level access
+    def output_fields(self):
+        """(mach, entropy, sensor, total entropy) of the current state: the CUDA
+        tree's post-processing fields (src_cuda/post_processing.F90:7-36,
+        compute_entropy.F90:10-30, adaptation_sensors.F90:7-101)."""
+        n = self.grid.n
+        mach, ent, sen = np.zeros(n), np.zeros(n), np.zeros(n)
+        tot = self.lib.orc_output_fields(self.h, _d(mach), _d(ent), _d(sen))
+        return mach, ent, sen, tot
+
     def func_delta(self): self.lib.orc_func_delta(self.h)
     def q_variables(self): self.lib.orc_eval_q_variables(self.h)
     def q_derivatives(self): self.lib.orc_eval_q_derivatives(self.h)

@@ -788,6 +788,56 @@ int orc_run(orc_t *h, int it_first, int n_iters, double *residue, int *n_done) {
 }
 
 /* compute_force_coeffs.F90:11-102 */
+/* src_cuda/adaptation_sensors.F90:35-101 sensor_D2_distance, one point */
+static double d2_distance(const orc_t *h, int i) {
+    double u1_i = PRIM(2, i), u2_i = PRIM(3, i), rho_i = PRIM(1, i), pr_i = PRIM(4, i);
+    double maxi = 0.0;
+    for (int r = 1; r <= NBHS(i); ++r) {
+        int j = CONN(i, r);
+        double u1_j = PRIM(2, j), u2_j = PRIM(3, j), rho_j = PRIM(1, j), pr_j = PRIM(4, j);
+        double temp1 = (pr_i * pr_i * rho_j) / (pr_j * pr_j * rho_i);
+        temp1 = log(temp1);
+        temp1 = (rho_j - rho_i) * temp1;
+        double u_sqr = (u1_j - u1_i) * (u1_j - u1_i) + (u2_j - u2_i) * (u2_j - u2_i);
+        double temp2 = (rho_j / rho_i) + (pr_i * rho_j) / (pr_j * rho_i);
+        temp2 = temp2 * u_sqr;
+        temp2 = (0.5 * rho_i * rho_i / pr_i) * temp2;
+        double temp3 = rho_i * (((pr_i * rho_j) / (pr_j * rho_i)) - 1);
+        temp3 = temp3 + rho_j * (((pr_j * rho_i) / (pr_i * rho_j)) - 1);
+        temp3 = 2 * temp3;
+        double D2_dist = temp1 + temp2 + temp3;
+        if (D2_dist > maxi) maxi = D2_dist;
+    }
+    return maxi;
+}
+
+double orc_output_fields(const orc_t *h, double *mach, double *entropy, double *sensor) {
+    const double gamma = GAMMA;
+    double total_entropy = 0.0, max_sensor = 0.0;
+    double temp2 = log(PR_INF);
+    double *d2 = malloc(sizeof(double) * (size_t)h->n);
+    for (int k = 1; k <= h->n; ++k) {
+        /* post_processing.F90:24-27 */
+        double sos = sqrt(gamma * PRIM(4, k) / PRIM(1, k));
+        double vel_mag = PRIM(2, k) * PRIM(2, k) + PRIM(3, k) * PRIM(3, k);
+        if (mach) mach[k - 1] = sqrt(vel_mag / sos);
+        /* compute_entropy.F90:21-27 */
+        double temp1 = pow(PRIM(1, k), gamma);
+        temp1 = PRIM(4, k) / temp1;
+        temp1 = log(temp1);
+        if (entropy) entropy[k - 1] = fabs(temp1 - temp2);
+        total_entropy = total_entropy + fabs(temp1 - temp2);
+        d2[k - 1] = d2_distance(h, k);
+    }
+    /* adaptation_sensors.F90:18-30 */
+    for (int k = 0; k < h->n; ++k)
+        if (d2[k] >= max_sensor) max_sensor = d2[k];
+    if (sensor)
+        for (int k = 0; k < h->n; ++k) sensor[k] = d2[k] / max_sensor;
+    free(d2);
+    return total_entropy;
+}
+
 void orc_forces(orc_t *h, double *cl, double *cd, double *cm, double *cp_out) {
     int shapes = h->p.shapes;
     double *H = calloc((size_t)shapes, sizeof(double));

@@ -73,6 +73,14 @@ void orc_state_update(orc_t *h, int rk);
 void orc_save_prim_old(orc_t *h);
 double orc_sum_res_sqr(const orc_t *h);
 
+/* The CUDA tree's post-processing fields of the current state, per point:
+ * the Mach number as print_primal_output forms it, sqrt(|u|^2 / c)
+ * (src_cuda/post_processing.F90:24-27), the entropy |log(p/rho^gamma) -
+ * log(pr_inf)| (src_cuda/compute_entropy.F90:10-30) and the D2-distance
+ * adaptation sensor normalised by its maximum (src_cuda/adaptation_sensors.F90:
+ * 7-101).  Any output may be NULL; returns the total entropy. */
+double orc_output_fields(const orc_t *h, double *mach, double *entropy, double *sensor);
+
 /* copies an internal array out: name is one of
  * "prim","prim_old","q","dq","qm","flux_res","delta","nx","ny","temp" */
 int orc_get(const orc_t *h, const char *name, double *out);
