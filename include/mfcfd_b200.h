@@ -93,11 +93,25 @@ typedef struct mfcfd_params {
 
 typedef struct mfcfd mfcfd_t;
 
+/* objectives J (mfcfd_objective, mfcfd_adjoint, mfcfd_tangent) */
+#define MFCFD_OBJ_CL          0  /* sum over shapes of Cl (compute_force_coeffs.F90)   */
+#define MFCFD_OBJ_CD          1  /* sum over shapes of Cd: the reference's J            */
+#define MFCFD_OBJ_ENTROPY     2  /* sum |log(p/rho^gamma) - log(pr_inf)|
+                                    (compute_entropy.F90:10-40)                         */
+#define MFCFD_OBJ_ENSTROPHY   3  /* sum (du2/dx - du1/dy)^2, least-squares gradients
+                                    (compute_enstrophy.F90:9-89)                        */
+#define MFCFD_OBJ_STAGNATION  4  /* sum (p0_inf - p0)^2 / (p0_inf^2 N), stagnation-
+                                    pressure loss (stagnation_values.F90:43-76)         */
+
+/* J of the current state (the reference's objective routines of
+ * src_mpi_primal; Cl/Cd summed over shapes). */
+int mfcfd_objective(mfcfd_t *h, int objective, double *J);
+
 /* Reverse-mode derivative of the loop (the reference's checkpointed adjoint
  * q_lskum_chkpts_b + FPI_SOLVER_B, src_mpi_adjoint/sensitivity_files/
  * q_lskum_chkpts_b.F90:23-300).  From the handle's current state (held
- * fixed) it runs n_iters iterations, J = sum over shapes of Cl (objective 0)
- * or Cd (objective 1) of the final state, and writes dJ/dx, dJ/dy per point
+ * fixed) it runs n_iters iterations, J = an MFCFD_OBJ_* objective of the final
+ * state (the reference's J is Cd), and writes dJ/dx, dJ/dy per point
  * (caller order) -- the content of sensitivity/sensitivity.dat.  min_dist is
  * data (not a function of x, y), as in the reference.  prim snapshots are
  * kept in HBM within ckpt_bytes (32 bytes a point each, binomial placement);
@@ -111,9 +125,8 @@ int mfcfd_adjoint(mfcfd_t *h, int objective, int n_iters, size_t ckpt_bytes, dou
  * src_mpi_forward/sensitivity_files/q_lskum_d.F90:28-89, which seeds
  * pointd%x(1) = 1).  From the handle's current state (held fixed) it runs
  * n_iters iterations with the grid moved along the direction (dx, dy) per
- * point (caller order; NULL = 0) and writes J = sum over shapes of Cl
- * (objective 0) or Cd (objective 1) of the final state and dJ/de along the
- * direction.  For the gradient of mfcfd_adjoint over the same iterations,
+ * point (caller order; NULL = 0) and writes J = an MFCFD_OBJ_* objective of
+ * the final state and dJ/de along the direction.  For the gradient of mfcfd_adjoint over the same iterations,
  * dJ/de = sum_i dJdx_i dx_i + dJdy_i dy_i.  The handle's state is left
  * unchanged.  FP64 handles with power == 0 only (else MFCFD_ERR_ARG). */
 int mfcfd_tangent(mfcfd_t *h, int objective, int n_iters, const double *dx, const double *dy,

@@ -20,6 +20,7 @@
 
 #include "adjoint.h"
 #include "handle.h"
+#include "objective.h"
 
 using namespace lskum;
 using lskum_host::cuda_fail;
@@ -261,9 +262,19 @@ int reverse_iteration(mfcfd_t *h, AdjointState *a, int k, const R4 *state) {
         const int n = a->n;
         cudaStream_t s = h->stream;
         CK(cudaMemsetAsync(a->pb[0], 0, sizeof(double) * 4 * n, s));
-        AdjShape t{a->nshape, a->d_sidx, a->d_sleft, a->d_sright, a->d_snx, a->d_sny};
-        launch_forces_b(t, a->tprim[a->rks], h->d_xy, h->p.mach, h->cos_t, h->sin_t,
-                        a->objective, a->pb[0], a->xb, a->yb, a->nxb, a->nyb, s);
+        if (a->objective == MFCFD_OBJ_CL || a->objective == MFCFD_OBJ_CD) {
+            AdjShape t{a->nshape, a->d_sidx, a->d_sleft, a->d_sright, a->d_snx, a->d_sny};
+            launch_forces_b(t, a->tprim[a->rks], h->d_xy, h->p.mach, h->cos_t, h->sin_t,
+                            a->objective, a->pb[0], a->xb, a->yb, a->nxb, a->nyb, s);
+        } else {
+            lskum_host::launch_objective_b(h, a->objective, a->tprim[a->rks], a->pb[0], a->xb,
+                                           a->yb, a->contrib, s);
+            if (a->objective == MFCFD_OBJ_ENSTROPHY) {
+                launch_gather(n, a->kp, a->d_tptr, a->d_tlist, a->contrib, ADJ_GATHER_GRAD, a->qb,
+                              nullptr, a->pb[0], a->xb, a->yb, s);
+                h->launches += 1;
+            }
+        }
         // keep the final state: the handle holds it at the end, as after mfcfd_run
         CK(cudaMemcpyAsync(a->fin, a->tprim[a->rks], sizeof(R4) * (size_t)n,
                            cudaMemcpyDeviceToDevice, s));
@@ -334,7 +345,8 @@ void lskum_host::free_adjoint(mfcfd_t *h) {
 
 extern "C" int mfcfd_adjoint(mfcfd_t *h, int objective, int n_iters, size_t ckpt_bytes,
                              double *J, double *dJdx, double *dJdy, int *n_forward) {
-    if (!h || n_iters < 1 || (objective != 0 && objective != 1) || !dJdx || !dJdy)
+    if (!h || n_iters < 1 || objective < MFCFD_OBJ_CL || objective > MFCFD_OBJ_STAGNATION ||
+        !dJdx || !dJdy)
         return MFCFD_ERR_ARG;
     if (h->fp32) return fail(h, MFCFD_ERR_ARG, "mfcfd_adjoint: FP64 handles only");
     if (h->p.power != 0.0)
@@ -386,13 +398,7 @@ extern "C" int mfcfd_adjoint(mfcfd_t *h, int objective, int n_iters, size_t ckpt
         dJdx[h->perm[p]] = xb[p];
         dJdy[h->perm[p]] = yb[p];
     }
-    if (J) {
-        std::vector<double> cl(h->shapes), cd(h->shapes), cm(h->shapes);
-        if ((st = mfcfd_forces(h, cl.data(), cd.data(), cm.data(), nullptr))) return st;
-        double s = 0.0;
-        for (int k = 0; k < h->shapes; ++k) s += objective == 1 ? cd[k] : cl[k];
-        *J = s;
-    }
+    if (J && (st = lskum_host::objective_value(h, objective, h->d_prim[h->cur], J))) return st;
     if (n_forward) *n_forward = (int)a->forward_iters;
     return MFCFD_OK;
 }

@@ -24,6 +24,7 @@
 // overloads, and the Dual ones are found by argument-dependent lookup.
 #include "handle.h"
 #include "dual.cuh"
+#include "objective.h"
 
 using namespace lskum;
 using lskum_host::cuda_fail;
@@ -346,6 +347,54 @@ __global__ void k_t_forces(Geom g, TanState s, TanShape t, int cur, double mach,
     out[1] = J.d;
 }
 
+// Per-point terms of the secondary objectives (compute_entropy.F90:21-27,
+// compute_enstrophy.F90:27-79, stagnation_values.F90:60-67), as Duals.
+__global__ void k_t_obj_terms(Geom g, TanState s, int cur, int kind, double gamma_power,
+                              double p0_inf, double *__restrict__ tv, double *__restrict__ td) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.n) return;
+    const Dual gamma(1.4), pr_inf(1.0 / 1.4);
+    Dual P[4];
+    ld_dual4(s.pv[cur], s.pt[cur], i, P);
+    Dual t;
+    if (kind == MFCFD_OBJ_ENTROPY) {
+        // rho**gamma = exp(gamma log rho)
+        Dual temp1 = exp(gamma * log(P[0]));
+        temp1 = P[3] / temp1;
+        temp1 = log(temp1);
+        t = fabs(temp1 - log(pr_inf));
+    } else if (kind == MFCFD_OBJ_STAGNATION) {
+        const Dual m2 = (P[1] * P[1] + P[2] * P[2]) / (gamma * P[3] / P[0]);
+        const Dual A = Dual(1.0) + Dual((1.4 - 1) / 2) * m2;
+        const Dual d = Dual(p0_inf) - P[3] * exp(Dual(gamma_power) * log(A));
+        t = d * d;
+    } else {
+        Dual xi, yi;
+        xy_dual(g, s, i, xi, yi);
+        Dual sxx, syy, sxy, sxu1, sxu2, syu1, syu2;
+        const int nb = g.nbhs[i];
+        for (int r = 0; r < nb; ++r) {
+            const int k = g.conn[r * g.n + i];
+            Dual xk, yk, Q[4];
+            xy_dual(g, s, k, xk, yk);
+            ld_dual4(s.pv[cur], s.pt[cur], k, Q);
+            const Dual delx = xk - xi, dely = yk - yi;
+            sxx = sxx + delx * delx;
+            syy = syy + dely * dely;
+            sxy = sxy + delx * dely;
+            sxu1 = sxu1 + delx * (Q[1] - P[1]);
+            sxu2 = sxu2 + delx * (Q[2] - P[2]);
+            syu1 = syu1 + dely * (Q[1] - P[1]);
+            syu2 = syu2 + dely * (Q[2] - P[2]);
+        }
+        const Dual one_by_det = Dual(1.0) / (sxx * syy - sxy * sxy);
+        const Dual w = (sxu2 * syy - syu2 * sxy) * one_by_det - (syu1 * sxx - sxu1 * sxy) * one_by_det;
+        t = w * w;
+    }
+    tv[i] = t.v;
+    td[i] = t.d;
+}
+
 inline int nblk(int n, int b) { return (n + b - 1) / b; }
 
 }  // namespace
@@ -353,7 +402,8 @@ inline int nblk(int n, int b) { return (n + b - 1) / b; }
 extern "C" int mfcfd_tangent(mfcfd_t *h, int objective, int n_iters, const double *dx,
                              const double *dy, double *J, double *dJ) {
     if (!h) return MFCFD_ERR_ARG;
-    if (objective != 0 && objective != 1) return fail(h, MFCFD_ERR_ARG, "objective must be 0 or 1");
+    if (objective < MFCFD_OBJ_CL || objective > MFCFD_OBJ_STAGNATION)
+        return fail(h, MFCFD_ERR_ARG, "objective must be 0..4");
     if (n_iters < 0) return fail(h, MFCFD_ERR_ARG, "n_iters < 0");
     if (h->fp32 || h->p.power != 0.0)
         return fail(h, MFCFD_ERR_ARG, "mfcfd_tangent needs an FP64 handle with power = 0");
@@ -487,7 +537,35 @@ extern "C" int mfcfd_tangent(mfcfd_t *h, int objective, int n_iters, const doubl
             cudaError_t le = cudaGetLastError();
             if (le != cudaSuccess) st = cuda_fail(h, le, "mfcfd_tangent launch");
         }
-        if (st == MFCFD_OK) {
+        if (st == MFCFD_OK && objective >= MFCFD_OBJ_ENTROPY) {
+            // secondary objectives: per-point Dual terms, summed in caller order
+            double *d_tv = nullptr, *d_td = nullptr;
+            cudaError_t c2 = take(&d_tv, n);
+            if (c2 == cudaSuccess) c2 = take(&d_td, n);
+            const double gp = lskum_host::stagnation_gamma_power();
+            const double p0_inf = lskum_host::stagnation_p0_inf(h->p.mach);
+            if (c2 == cudaSuccess) {
+                k_t_obj_terms<<<nblk(n, 256), 256, 0, str>>>(h->geom, s, cur, objective, gp, p0_inf,
+                                                             d_tv, d_td);
+                h->launches += 1;
+                c2 = cudaGetLastError();
+            }
+            std::vector<double> tv(n), td(n);
+            if (c2 == cudaSuccess)
+                c2 = cudaMemcpyAsync(tv.data(), d_tv, sizeof(double) * n, cudaMemcpyDeviceToHost, str);
+            if (c2 == cudaSuccess)
+                c2 = cudaMemcpyAsync(td.data(), d_td, sizeof(double) * n, cudaMemcpyDeviceToHost, str);
+            if (c2 == cudaSuccess) c2 = cudaStreamSynchronize(str);
+            if (c2 != cudaSuccess) {
+                st = cuda_fail(h, c2, "mfcfd_tangent objective");
+            } else {
+                Dual sum;
+                for (int k = 0; k < n; ++k) sum = sum + Dual(tv[inv[k]], td[inv[k]]);
+                if (objective == MFCFD_OBJ_STAGNATION) sum = sum * Dual(1 / (p0_inf * p0_inf * n));
+                if (J) *J = sum.v;
+                if (dJ) *dJ = sum.d;
+            }
+        } else if (st == MFCFD_OK) {
             TanShape ts{(int)si.size(), h->shapes, d_si, d_sl, d_sr, d_ss};
             k_t_forces<<<1, 32, 0, str>>>(h->geom, s, ts, cur, h->p.mach, h->cos_t, h->sin_t,
                                           objective, d_out);

@@ -130,12 +130,20 @@ class Solver:
         dx, dy = np.zeros(self.n), np.zeros(self.n)
         J = C.c_double(0.0)
         nf = C.c_int(0)
-        obj = {"cl": 0, "cd": 1}[objective.lower()]
+        obj = _lib.OBJECTIVES[objective.lower()]
         _lib.check(self.lib.mfcfd_adjoint(self.h, obj, int(n_iters), int(ckpt_bytes),
                                           C.byref(J), _dptr(dx), _dptr(dy), C.byref(nf)),
                    self.h, "mfcfd_adjoint")
         self.it = (self.it or 0) + n_iters
         return J.value, dx, dy, nf.value
+
+    def objective(self, objective: str = "cd") -> float:
+        """J of the current state: "cl", "cd" (summed over shapes), "entropy",
+        "enstrophy" or "stagnation" (the reference's objective routines)."""
+        J = C.c_double(0.0)
+        _lib.check(self.lib.mfcfd_objective(self.h, _lib.OBJECTIVES[objective.lower()],
+                                            C.byref(J)), self.h, "mfcfd_objective")
+        return J.value
 
     def output_fields(self):
         """(mach, entropy, sensor, total entropy) of the current state: the
@@ -155,7 +163,7 @@ class Solver:
             return None if a is None else _dptr(np.ascontiguousarray(a, dtype=np.float64))
         keep = [np.ascontiguousarray(a, dtype=np.float64) for a in (dx, dy) if a is not None]
         J, dJ = C.c_double(0.0), C.c_double(0.0)
-        obj = {"cl": 0, "cd": 1}[objective.lower()]
+        obj = _lib.OBJECTIVES[objective.lower()]
         pdx = _dptr(keep[0]) if dx is not None else None
         pdy = _dptr(keep[-1]) if dy is not None else None
         _lib.check(self.lib.mfcfd_tangent(self.h, obj, int(n_iters), pdx, pdy, C.byref(J),

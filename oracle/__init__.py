@@ -64,6 +64,8 @@ def _lib(variant: str = "") -> C.CDLL:
     lib.orc_sum_res_sqr.argtypes = [P]
     lib.orc_output_fields.argtypes = [P, D, D, D]
     lib.orc_output_fields.restype = C.c_double
+    lib.orc_objective.argtypes = [P, C.c_int]
+    lib.orc_objective.restype = C.c_double
     lib.orc_sum_res_sqr.restype = C.c_double
     lib.orc_num_threads.restype = C.c_int
     _LIBS[name] = lib
@@ -154,6 +156,15 @@ class Oracle:
         mach, ent, sen = np.zeros(n), np.zeros(n), np.zeros(n)
         tot = self.lib.orc_output_fields(self.h, _d(mach), _d(ent), _d(sen))
         return mach, ent, sen, tot
+
+    def objective(self, kind: str):
+        """J of the current state: "cl"/"cd" (summed over shapes) or a
+        secondary objective "entropy", "enstrophy", "stagnation"."""
+        if kind in ("cl", "cd"):
+            cl, cd, _, _ = self.forces()
+            return float((cd if kind == "cd" else cl).sum())
+        k = {"entropy": 2, "enstrophy": 3, "stagnation": 4}[kind]
+        return float(self.lib.orc_objective(self.h, k))
 
     def func_delta(self): self.lib.orc_func_delta(self.h)
     def q_variables(self): self.lib.orc_eval_q_variables(self.h)

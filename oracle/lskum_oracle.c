@@ -838,6 +838,63 @@ double orc_output_fields(const orc_t *h, double *mach, double *entropy, double *
     return total_entropy;
 }
 
+double orc_objective(const orc_t *h, int kind) {
+    const double gamma = GAMMA;
+    if (kind == 2) {
+        /* compute_entropy.F90:19-30 */
+        double total_entropy = 0.0, temp2 = log(PR_INF);
+        for (int k = 1; k <= h->n; ++k) {
+            double temp1 = pow(PRIM(1, k), gamma);
+            temp1 = PRIM(4, k) / temp1;
+            temp1 = log(temp1);
+            total_entropy = total_entropy + fabs(temp1 - temp2);
+        }
+        return total_entropy;
+    }
+    if (kind == 3) {
+        /* compute_enstrophy.F90:25-79 */
+        double total_enstrophy = 0.0;
+        for (int i = 1; i <= h->n; ++i) {
+            double x_i = X(i), y_i = Y(i);
+            double sum_delx_sqr = 0.0, sum_dely_sqr = 0.0, sum_delx_dely = 0.0;
+            double sum_delx_delu1 = 0.0, sum_dely_delu1 = 0.0, sum_delx_delu2 = 0.0,
+                   sum_dely_delu2 = 0.0;
+            for (int k = 1; k <= NBHS(i); ++k) {
+                int nbh = CONN(i, k);
+                double delx = X(nbh) - x_i, dely = Y(nbh) - y_i;
+                double dist = sqrt(delx * delx + dely * dely);
+                double weights = pow(dist, h->p.power);
+                sum_delx_sqr = sum_delx_sqr + delx * delx * weights;
+                sum_dely_sqr = sum_dely_sqr + dely * dely * weights;
+                sum_delx_dely = sum_delx_dely + delx * dely * weights;
+                sum_delx_delu1 = sum_delx_delu1 + weights * delx * (PRIM(2, nbh) - PRIM(2, i));
+                sum_delx_delu2 = sum_delx_delu2 + weights * delx * (PRIM(3, nbh) - PRIM(3, i));
+                sum_dely_delu1 = sum_dely_delu1 + weights * dely * (PRIM(2, nbh) - PRIM(2, i));
+                sum_dely_delu2 = sum_dely_delu2 + weights * dely * (PRIM(3, nbh) - PRIM(3, i));
+            }
+            double det = sum_delx_sqr * sum_dely_sqr - sum_delx_dely * sum_delx_dely;
+            double one_by_det = 1.0 / det;
+            double du2_dx = (sum_delx_delu2 * sum_dely_sqr - sum_dely_delu2 * sum_delx_dely) * one_by_det;
+            double du1_dy = (sum_dely_delu1 * sum_delx_sqr - sum_delx_delu1 * sum_delx_dely) * one_by_det;
+            double temp = du2_dx - du1_dy;
+            total_enstrophy = total_enstrophy + temp * temp;
+        }
+        return total_enstrophy;
+    }
+    /* stagnation_values.F90:52-73 objective_function_J */
+    double gammaPower = gamma / (gamma - 1);
+    double p0_inf = PR_INF * pow(1 + ((gamma - 1) / 2) * h->p.mach * h->p.mach, gammaPower);
+    double constant = 1 / (p0_inf * p0_inf * h->n);
+    double p0_sum = 0.0;
+    for (int i = 1; i <= h->n; ++i) {
+        double angle = sqrt(gamma * PRIM(4, i) / PRIM(1, i));
+        double mach_t = sqrt(PRIM(2, i) * PRIM(2, i) + PRIM(3, i) * PRIM(3, i)) / angle;
+        double p0 = PRIM(4, i) * pow(1 + ((gamma - 1) / 2) * mach_t * mach_t, gammaPower);
+        p0_sum = p0_sum + (p0_inf - p0) * (p0_inf - p0);
+    }
+    return p0_sum * constant;
+}
+
 void orc_forces(orc_t *h, double *cl, double *cd, double *cm, double *cp_out) {
     int shapes = h->p.shapes;
     double *H = calloc((size_t)shapes, sizeof(double));

@@ -81,6 +81,12 @@ double orc_sum_res_sqr(const orc_t *h);
  * 7-101).  Any output may be NULL; returns the total entropy. */
 double orc_output_fields(const orc_t *h, double *mach, double *entropy, double *sensor);
 
+/* Secondary objectives of the current state (src_mpi_primal): kind 2 total
+ * entropy (compute_entropy.F90:10-40), 3 total enstrophy
+ * (compute_enstrophy.F90:9-89), 4 stagnation-pressure loss
+ * (stagnation_values.F90:43-76, objective_function_J). */
+double orc_objective(const orc_t *h, int kind);
+
 /* copies an internal array out: name is one of
  * "prim","prim_old","q","dq","qm","flux_res","delta","nx","ny","temp" */
 int orc_get(const orc_t *h, const char *name, double *out);
