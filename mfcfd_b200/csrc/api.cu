@@ -67,7 +67,8 @@ void free_all(mfcfd_t *h) {
                     h->d_dq[1], h->d_qm, h->d_delta, h->d_spd, h->d_res_part, h->d_flux_dbg,
                     h->d_hist, h->d_forces, h->d_ctl, h->d_sh_idx, h->d_sh_shape, h->d_sh_geo,
                     h->d_sh_my, h->f_prim[0], h->f_prim[1], h->f_q[0], h->f_q[1],
-                    h->f_dq[0], h->f_dq[1], h->f_qm, h->f_eps2, h->d_inst, h->d_sched,
+                    h->f_dq[0], h->f_dq[1], h->f_qm, h->f_eps2, h->f_dxy, h->f_w, h->f_lsq,
+                    h->f_flsq, h->d_inst, h->d_sched,
                     h->d_run};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -141,11 +142,11 @@ void launch_stage(mfcfd_t *h, cudaStream_t s, int rk, int A, int B, F after) {
         after();
     } else {
         const float4 *q_in = h->f_q[h->qcur];
-        launch_grad32(h->geom, h->consts, h->sched, q_in, h->d_spd, h->f_dq[0], h->f_qm,
-                      h->d_delta, rk == 1, h->point_block, h->point_grid, s);
+        launch_grad32(h->geom, h->consts, h->geom32, h->sched, q_in, h->d_spd, h->f_dq[0],
+                      h->f_qm, h->d_delta, rk == 1, h->point_block, h->point_grid, s);
         after();
         for (int t = 1; t <= m; ++t) {
-            launch_inner32(h->geom, h->consts, h->sched, q_in, h->f_dq[(t - 1) & 1],
+            launch_inner32(h->geom, h->consts, h->geom32, h->sched, q_in, h->f_dq[(t - 1) & 1],
                            h->f_dq[t & 1], h->point_block, h->point_grid, s);
             after();
         }
@@ -162,6 +163,7 @@ void launch_stage(mfcfd_t *h, cudaStream_t s, int rk, int A, int B, F after) {
         b.spd = h->d_spd;
         b.res_part = h->d_res_part;
         b.flux_dbg = h->keep_diag ? h->d_flux_dbg : nullptr;
+        b.f = h->geom32;
         launch_flux32(h->geom, h->consts, h->sched, b, rk, last, h->flux_grid, s);
         after();
     }
@@ -276,6 +278,65 @@ int mfcfd_default_params(mfcfd_params *p) {
 }
 
 }  // extern "C"
+
+namespace {
+
+// Geometry of the FP32-mixed passes, formed once in FP64 with the
+// reference's sums and rounded to FP32: per stencil slot the offset (and
+// weight); per point the inverse of the normal matrix of eval_q_derivatives
+// (q_variables.F90:84-110: dx = a Sx + b Sy, dy = b Sx + c Sy); per point and
+// split list the two coefficients of the flux least-squares solve
+// (interior_fluxes.F90: x lists G = a Sx + b Sy, y lists G = a Sy + b Sx,
+// with Sx, Sy the sums of dG dels_w, dG deln_w).
+void build_geom32(HostGrid &hg, int nw, int no, double power) {
+    const int n = hg.n, kp = hg.kp;
+    hg.dxy.assign((size_t)kp * n, make_float2(0.f, 0.f));
+    hg.wslot.assign(power != 0.0 ? (size_t)kp * n : 0, 0.f);
+    hg.lsq.assign(n, make_float4(0.f, 0.f, 0.f, 0.f));
+    hg.flsq.assign(2 * (size_t)n, make_float4(0.f, 0.f, 0.f, 0.f));
+    for (int p = 0; p < n; ++p) {
+        const double xi = hg.xy[p].x, yi = hg.xy[p].y, nx = hg.nrm[p].x, ny = hg.nrm[p].y;
+        const int kind = p < nw ? 0 : (p < nw + no ? 2 : 1);
+        double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
+        double ls[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int r = 0; r < hg.nbhs[p]; ++r) {
+            const int k = hg.conn[(size_t)r * n + p];
+            const double delx = hg.xy[k].x - xi, dely = hg.xy[k].y - yi;
+            double w = 1.0;
+            if (power != 0.0) w = pow(sqrt(delx * delx + dely * dely), power);
+            hg.dxy[(size_t)r * n + p] = make_float2((float)delx, (float)dely);
+            if (power != 0.0) hg.wslot[(size_t)r * n + p] = (float)w;
+            sdx2 = sdx2 + delx * delx * w;
+            sdy2 = sdy2 + dely * dely * w;
+            sdxy = sdxy + delx * dely * w;
+            const double tx = ny, ty = -nx;
+            const double dels = delx * tx + dely * ty, deln = delx * nx + dely * ny;
+            double wl = 1.0;
+            if (power != 0.0) wl = pow(sqrt(dels * dels + deln * deln), power);
+            const double dels_w = dels * wl, deln_w = deln * wl;
+            for (int L = 0; L < 4; ++L) {
+                const unsigned long long bits = L < 2 ? hg.mx[p] : hg.my[p];
+                if (!((bits >> (r + ((L & 1) ? 32 : 0))) & 1ull)) continue;
+                ls[L][0] = ls[L][0] + dels * dels_w;
+                ls[L][1] = ls[L][1] + deln * deln_w;
+                ls[L][2] = ls[L][2] + dels * deln_w;
+            }
+        }
+        const double obd = 1.0 / (sdx2 * sdy2 - sdxy * sdxy);
+        hg.lsq[p] = make_float4((float)(sdy2 * obd), (float)(-sdxy * obd), (float)(sdx2 * obd), 0.f);
+        float co[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        for (int L = 0; L < 4; ++L) {
+            if ((kind == 0 && L == 2) || (kind == 2 && L == 3)) continue;
+            const double ob = 1.0 / (ls[L][0] * ls[L][1] - ls[L][2] * ls[L][2]);
+            co[2 * L] = (float)((L < 2 ? ls[L][1] : ls[L][0]) * ob);
+            co[2 * L + 1] = (float)(-ls[L][2] * ob);
+        }
+        hg.flsq[2 * (size_t)p] = make_float4(co[0], co[1], co[2], co[3]);
+        hg.flsq[2 * (size_t)p + 1] = make_float4(co[4], co[5], co[6], co[7]);
+    }
+}
+
+}  // namespace
 
 // Host half of mfcfd_create: checks of the grid and parameters, normals,
 // split membership, renumbering and the renumbered arrays, all in caller
@@ -482,7 +543,7 @@ int lskum_host::prepare_grid(const mfcfd_grid &G, const mfcfd_params &P, HostGri
         smy.push_back(myy);
     }
     hg.nshape = (int)sidx.size();
-
+    if (P.precision == MFCFD_FP32_MIXED) build_geom32(hg, nw, no, P.power);
     return MFCFD_OK;
 }
 
@@ -584,6 +645,10 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
         }
         ALLOC(h->f_qm, (size_t)8 * n);
         ALLOC(h->f_eps2, n);
+        ALLOC(h->f_dxy, (size_t)kp * n);
+        if (!hg.wslot.empty()) ALLOC(h->f_w, (size_t)kp * n);
+        ALLOC(h->f_lsq, n);
+        ALLOC(h->f_flsq, 2 * (size_t)n);
     }
     ALLOC(h->d_delta, n);
     ALLOC(h->d_spd, n);
@@ -614,7 +679,11 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
         goto fail_create;
     if (h->fp32) {
         std::vector<float> feps(heps.begin(), heps.end());
-        if ((st = up(h->f_eps2, feps))) goto fail_create;
+        if ((st = up(h->f_eps2, feps)) || (st = up(h->f_dxy, hg.dxy)) ||
+            (st = up(h->f_lsq, hg.lsq)) || (st = up(h->f_flsq, hg.flsq)))
+            goto fail_create;
+        if (h->f_w && (st = up(h->f_w, hg.wslot))) goto fail_create;
+        h->geom32 = Geom32{h->f_dxy, h->f_w, h->f_lsq, h->f_flsq};
     }
     if (h->nshape > 0) {
         if ((st = up(h->d_sh_idx, sidx)) || (st = up(h->d_sh_shape, sshape)) ||

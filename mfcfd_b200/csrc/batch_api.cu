@@ -67,6 +67,10 @@ struct mfcfd_batch {
     float4 *f_prim[2] = {nullptr, nullptr}, *f_q[2] = {nullptr, nullptr};
     float *f_dq[2] = {nullptr, nullptr};
     float *f_qm = nullptr, *f_eps2 = nullptr;
+    float2 *f_dxy = nullptr;
+    float *f_w = nullptr;
+    float4 *f_lsq = nullptr, *f_flsq = nullptr;
+    Geom32 geom32{};
     double *d_delta = nullptr, *d_spd = nullptr, *d_res_part = nullptr, *d_hist = nullptr;
     double *d_forces = nullptr;
     int hist_cap = 0;
@@ -131,7 +135,8 @@ void free_batch(mfcfd_batch_t *b) {
     void *bufs[] = {b->d_xy, b->d_nrm, b->d_eps2, b->d_obc, b->d_conn, b->d_nbhs, b->d_mx,
                     b->d_my, b->d_prim[0], b->d_prim[1], b->d_q[0], b->d_q[1], b->d_dq[0],
                     b->d_dq[1], b->d_qm, b->f_prim[0], b->f_prim[1], b->f_q[0], b->f_q[1],
-                    b->f_dq[0], b->f_dq[1], b->f_qm, b->f_eps2, b->d_delta, b->d_spd,
+                    b->f_dq[0], b->f_dq[1], b->f_qm, b->f_eps2, b->f_dxy, b->f_w, b->f_lsq,
+                    b->f_flsq, b->d_delta, b->d_spd,
                     b->d_res_part, b->d_hist, b->d_forces, b->d_inst, b->d_sched, b->d_run,
                     b->d_ctl, b->d_sh_idx, b->d_sh_shape, b->d_sh_geo, b->d_sh_my};
     for (void *p : bufs)
@@ -194,10 +199,10 @@ void batch_stage(mfcfd_batch_t *b, cudaStream_t s, int rk, int A, int B) {
         launch_flux(b->geom, b->consts, b->sched, sb, rk, last, fg, s);
     } else {
         const float4 *q_in = b->f_q[b->qcur];
-        launch_grad32(b->geom, b->consts, b->sched, q_in, b->d_spd, b->f_dq[0], b->f_qm,
-                      b->d_delta, rk == 1, pb, pg, s);
+        launch_grad32(b->geom, b->consts, b->geom32, b->sched, q_in, b->d_spd, b->f_dq[0],
+                      b->f_qm, b->d_delta, rk == 1, pb, pg, s);
         for (int t = 1; t <= m; ++t)
-            launch_inner32(b->geom, b->consts, b->sched, q_in, b->f_dq[(t - 1) & 1],
+            launch_inner32(b->geom, b->consts, b->geom32, b->sched, q_in, b->f_dq[(t - 1) & 1],
                            b->f_dq[t & 1], pb, pg, s);
         StageBufs32 sb;
         sb.prim_in = rk == 1 ? b->f_prim[A] : b->f_prim[B];
@@ -212,6 +217,7 @@ void batch_stage(mfcfd_batch_t *b, cudaStream_t s, int rk, int A, int B) {
         sb.spd = b->d_spd;
         sb.res_part = b->d_res_part;
         sb.flux_dbg = nullptr;
+        sb.f = b->geom32;
         launch_flux32(b->geom, b->consts, b->sched, sb, rk, last, fg, s);
     }
     b->qcur ^= 1;
@@ -471,6 +477,12 @@ int mfcfd_batch_create(int n_inst, const mfcfd_grid *const *grids, const mfcfd_p
     std::vector<unsigned long long> mx(N, 0), my(N, 0);
     std::vector<int> sidx, sshape;
     std::vector<double> sgeo, smy;
+    // FP32-mixed geometry (per slot [kp][N], per point, per point and list)
+    const bool weighted = b->fp32 && P0.power != 0.0;
+    std::vector<float2> dxy(b->fp32 ? (size_t)kp * N : 0, make_float2(0.f, 0.f));
+    std::vector<float> wslot(weighted ? (size_t)kp * N : 0, 0.f);
+    std::vector<float4> lsq(b->fp32 ? N : 0, make_float4(0.f, 0.f, 0.f, 0.f));
+    std::vector<float4> flsq(b->fp32 ? 2 * (size_t)N : 0, make_float4(0.f, 0.f, 0.f, 0.f));
     for (int p = 0; p < N; ++p)
         for (int r = 0; r < kp; ++r) conn[(size_t)r * N + p] = p;
     for (int i = 0; i < n_inst; ++i) {
@@ -485,6 +497,15 @@ int mfcfd_batch_create(int n_inst, const mfcfd_grid *const *grids, const mfcfd_p
             my[base + p] = h.my[p];
             for (int r = 0; r < h.kp; ++r)
                 conn[(size_t)r * N + base + p] = base + h.conn[(size_t)r * h.n + p];
+            if (b->fp32) {
+                for (int r = 0; r < h.kp; ++r) {
+                    dxy[(size_t)r * N + base + p] = h.dxy[(size_t)r * h.n + p];
+                    if (weighted) wslot[(size_t)r * N + base + p] = h.wslot[(size_t)r * h.n + p];
+                }
+                lsq[base + p] = h.lsq[p];
+                flsq[2 * (size_t)(base + p)] = h.flsq[2 * (size_t)p];
+                flsq[2 * (size_t)(base + p) + 1] = h.flsq[2 * (size_t)p + 1];
+            }
         }
         std::copy(h.obc.begin(), h.obc.begin() + (size_t)8 * h.no,
                   obc.begin() + (size_t)8 * info[i].obc_off);
@@ -544,6 +565,10 @@ int mfcfd_batch_create(int n_inst, const mfcfd_grid *const *grids, const mfcfd_p
         }
         BALLOC(b->f_qm, (size_t)8 * N);
         BALLOC(b->f_eps2, N);
+        BALLOC(b->f_dxy, (size_t)kp * N);
+        if (weighted) BALLOC(b->f_w, (size_t)kp * N);
+        BALLOC(b->f_lsq, N);
+        BALLOC(b->f_flsq, 2 * (size_t)N);
     }
     BALLOC(b->d_delta, N);
     BALLOC(b->d_spd, N);
@@ -579,7 +604,11 @@ int mfcfd_batch_create(int n_inst, const mfcfd_grid *const *grids, const mfcfd_p
         goto fail_create;
     if (b->fp32) {
         std::vector<float> feps(eps2.begin(), eps2.end());
-        if ((st = up(b->f_eps2, feps))) goto fail_create;
+        if ((st = up(b->f_eps2, feps)) || (st = up(b->f_dxy, dxy)) || (st = up(b->f_lsq, lsq)) ||
+            (st = up(b->f_flsq, flsq)))
+            goto fail_create;
+        if (weighted && (st = up(b->f_w, wslot))) goto fail_create;
+        b->geom32 = Geom32{b->f_dxy, b->f_w, b->f_lsq, b->f_flsq};
     }
     b->geom = Geom{N, kp, 0, 0, b->d_xy, b->d_nrm, b->d_eps2, b->d_conn, b->d_nbhs,
                    b->d_mx, b->d_my, b->d_obc};

@@ -44,6 +44,10 @@ struct mfcfd {
     float4 *f_prim[2] = {nullptr, nullptr}, *f_q[2] = {nullptr, nullptr};
     float *f_dq[2] = {nullptr, nullptr};
     float *f_qm = nullptr, *f_eps2 = nullptr;
+    float2 *f_dxy = nullptr;
+    float *f_w = nullptr;
+    float4 *f_lsq = nullptr, *f_flsq = nullptr;
+    Geom32 geom32{};
 
     // the handle's grid as a schedule of one instance (kernels are shared
     // with batched runs)
@@ -81,6 +85,11 @@ struct HostGrid {
     std::vector<unsigned long long> mx, my;
     std::vector<int> sidx, sshape;  // shape points in caller order
     std::vector<double> sgeo, smy;
+    // FP32-mixed geometry (precision MFCFD_FP32_MIXED only)
+    std::vector<float2> dxy;    // [kp][n] offsets to the stencil neighbours
+    std::vector<float> wslot;   // [kp][n] least-squares weights (power != 0 only)
+    std::vector<float4> lsq;    // [n] inverse normal matrix of the full stencil
+    std::vector<float4> flsq;   // [2n] per split list, two solve coefficients
 };
 
 namespace lskum_host {

@@ -129,6 +129,18 @@ int wave_blocks(int dev, int kind, int block, size_t smem, bool fp32);
 // q and spd from prim (set_state)
 void launch_init_state(const Geom &g, const R4 *prim, R4 *q, double *spd, cudaStream_t s);
 
+// FP32-mixed geometry, precomputed once per grid in FP64 and rounded:
+// offsets to the stencil neighbours [slot][point] (and weights when power
+// != 0, else w == nullptr), the inverse normal matrix of each point's full
+// stencil (a, b, c: dx = a Sx + b Sy, dy = b Sx + c Sy) and per split list
+// the two coefficients of the flux solve ([2i] lists 0-1, [2i+1] lists 2-3).
+struct Geom32 {
+    const float2 *dxy;
+    const float *w;
+    const float4 *lsq;
+    const float4 *flsq;
+};
+
 // FP32-mixed stage buffers: FP32 prim/q/dq/qm, FP64 delta/spd/partials.
 struct StageBufs32 {
     const float4 *prim_in;
@@ -143,13 +155,15 @@ struct StageBufs32 {
     double *spd;
     double *res_part;
     double *flux_dbg;
+    Geom32 f;
 };
 cudaError_t init_kernels32();
-void launch_grad32(const Geom &g, const Consts &c, const Sched &s, const float4 *q,
-                   const double *spd, float *dq, float *qm, double *delta, bool with_delta,
-                   int block, int grid, cudaStream_t st);
-void launch_inner32(const Geom &g, const Consts &c, const Sched &s, const float4 *q,
-                    const float *dq_in, float *dq_out, int block, int grid, cudaStream_t st);
+void launch_grad32(const Geom &g, const Consts &c, const Geom32 &f, const Sched &s,
+                   const float4 *q, const double *spd, float *dq, float *qm, double *delta,
+                   bool with_delta, int block, int grid, cudaStream_t st);
+void launch_inner32(const Geom &g, const Consts &c, const Geom32 &f, const Sched &s,
+                    const float4 *q, const float *dq_in, float *dq_out, int block, int grid,
+                    cudaStream_t st);
 void launch_flux32(const Geom &g, const Consts &c, const Sched &s, const StageBufs32 &b, int rk,
                    bool last, int grid, cudaStream_t st);
 void launch_init_state32(const Geom &g, const float4 *prim, float4 *q, double *spd,

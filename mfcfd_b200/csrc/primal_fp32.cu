@@ -1,13 +1,15 @@
 // FP32-mixed kernels of the LSKUM pseudo-time loop on sm_100a.
 //
 // Stored per point in FP32: prim, q, dq, qm (half the FP64 gather traffic).
-// Computed in FP32: the per-neighbour work of the flux pass -- limiter,
-// qtilde -> primitive (log, exp), the Maxwellian moments (exp, erf, sqrt)
-// and the split fluxes -- with the flux contributions summed by compensated
-// (Kahan) FP32 addition in slot order.  Kept in FP64: coordinates and every
-// 2x2 least-squares normal equation (ill-conditioned on stretched near-wall
-// stencils), the sums of the q-derivative passes, the state update, the
-// residual norm and the force coefficients.
+// Computed in FP32: the q-derivative sums of the D and I passes, the
+// per-neighbour work of the flux pass -- limiter, qtilde -> primitive (log,
+// exp), the Maxwellian moments (exp, erf, sqrt) and the split fluxes -- with
+// the flux contributions summed by compensated (Kahan) FP32 addition in slot
+// order.  The 2x2 least-squares normal matrices, ill-conditioned on
+// stretched near-wall stencils, are pure geometry: they are formed and
+// inverted once per grid in FP64 (Geom32) and only applied per iteration.
+// Kept in FP64: the local time step, the state update, the residual norm and
+// the force coefficients.
 #include <cuda_runtime.h>
 
 #include "batch.cuh"
@@ -21,9 +23,9 @@ constexpr int GRAD_BLOCK = 256;
 constexpr int LPP = 8;
 constexpr int FLUX_BLOCK = 128;
 constexpr int GROUPS = FLUX_BLOCK / LPP;
-constexpr int FREC = 11;  // dGxp..dGyn as 16 floats (8 doubles of storage), dels deln w
+constexpr int FREC = 9;   // dGxp..dGyn as 16 floats, then dels*w, deln*w (18 floats)
 #ifndef FLUX32_MIN_BLOCKS
-#define FLUX32_MIN_BLOCKS 5
+#define FLUX32_MIN_BLOCKS 8              // 64 registers: 32 warps per SM
 #endif
 constexpr double OBT = 1.0 / 3.0;
 constexpr double TBT = 2.0 / 3.0;
@@ -35,73 +37,68 @@ __device__ __forceinline__ void ldf8(const float *p, float a[4], float b[4]) {
     b[0] = y.x; b[1] = y.y; b[2] = y.z; b[3] = y.w;
 }
 
-__device__ __forceinline__ void stf8(float *p, const double a[4], const double b[4]) {
+__device__ __forceinline__ void stf8(float *p, const float a[4], const float b[4]) {
     float4 *v = reinterpret_cast<float4 *>(p);
-    v[0] = make_float4((float)a[0], (float)a[1], (float)a[2], (float)a[3]);
-    v[1] = make_float4((float)b[0], (float)b[1], (float)b[2], (float)b[3]);
+    v[0] = make_float4(a[0], a[1], a[2], a[3]);
+    v[1] = make_float4(b[0], b[1], b[2], b[3]);
 }
 
-// eval_q_derivatives (q_variables.F90:41-112) with FP32 q and FP64 sums, and
-// func_delta (state_update.F90:190-236).
+// eval_q_derivatives (q_variables.F90:41-112) with FP32 sums and the
+// precomputed inverse normal matrix, and func_delta (state_update.F90:190-236)
+// in FP64 from the coordinates.
 __device__ __forceinline__ void
-grad32_point(const Geom &g, const Consts &c, const float4 *__restrict__ q,
+grad32_point(const Geom &g, const Consts &c, const Geom32 &f, const float4 *__restrict__ q,
              const double *__restrict__ spd, float *__restrict__ dq, float *__restrict__ qm,
              double *__restrict__ delta, int with_delta, int i) {
-    double2 pi_ = g.xy[i];
-    float4 qv = __ldg(q + i);
-    float qi[4] = {qv.x, qv.y, qv.z, qv.w};
+    const float4 qv = __ldg(q + i);
+    const float qi[4] = {qv.x, qv.y, qv.z, qv.w};
     float qmax[4] = {qi[0], qi[1], qi[2], qi[3]};
     float qmin[4] = {qi[0], qi[1], qi[2], qi[3]};
-    double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
-    double sdxq[4] = {0.0, 0.0, 0.0, 0.0}, sdyq[4] = {0.0, 0.0, 0.0, 0.0};
+    float sx[4] = {0.f, 0.f, 0.f, 0.f}, sy[4] = {0.f, 0.f, 0.f, 0.f};
+    double2 pi_ = make_double2(0.0, 0.0);
+    if (with_delta) pi_ = g.xy[i];
     double min_delt = 1.0;
-    int nb = g.nbhs[i];
+    const int nb = g.nbhs[i];
     for (int r = 0; r < nb; ++r) {
-        int k = g.conn[r * g.n + i];
-        float4 kv = __ldg(q + k);
-        float qk[4] = {kv.x, kv.y, kv.z, kv.w};
+        const int k = g.conn[r * g.n + i];
+        const float2 d = __ldg(f.dxy + r * g.n + i);
+        const float w = f.w ? __ldg(f.w + r * g.n + i) : 1.0f;
+        const float4 kv = __ldg(q + k);
+        const float qk[4] = {kv.x, kv.y, kv.z, kv.w};
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
             if (qk[m] > qmax[m]) qmax[m] = qk[m];
             if (qk[m] < qmin[m]) qmin[m] = qk[m];
         }
-        double2 pk = g.xy[k];
-        double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
-        double w = 1.0, dist = 0.0;
-        if (!c.power_zero || with_delta) dist = sqrt(delx * delx + dely * dely);
-        if (!c.power_zero) w = pow(dist, c.power);
-        sdx2 = sdx2 + delx * delx * w;
-        sdy2 = sdy2 + dely * dely * w;
-        sdxy = sdxy + delx * dely * w;
+        const float wdx = w * d.x, wdy = w * d.y;
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-            double dqm = (double)qk[m] - (double)qi[m];
-            sdxq[m] = sdxq[m] + w * delx * dqm;
-            sdyq[m] = sdyq[m] + w * dely * dqm;
+            const float dqm = qk[m] - qi[m];
+            sx[m] = sx[m] + wdx * dqm;
+            sy[m] = sy[m] + wdy * dqm;
         }
         if (with_delta) {
-            double delta_t = dist / spd[k];
+            const double2 pk = g.xy[k];
+            const double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
+            double delta_t = sqrt(delx * delx + dely * dely) / spd[k];
             delta_t = c.cfl * delta_t;
             if (min_delt > delta_t) min_delt = delta_t;
         }
     }
-    double det = sdx2 * sdy2 - sdxy * sdxy;
-    double one_by_det = 1.0 / det;
-    double dx[4], dy[4], mx[4], mn[4];
+    const float4 L = __ldg(f.lsq + i);
+    float dx[4], dy[4];
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
-        dx[m] = (sdxq[m] * sdy2 - sdyq[m] * sdxy) * one_by_det;
-        dy[m] = (sdyq[m] * sdx2 - sdxq[m] * sdxy) * one_by_det;
-        mx[m] = qmax[m];
-        mn[m] = qmin[m];
+        dx[m] = L.x * sx[m] + L.y * sy[m];
+        dy[m] = L.y * sx[m] + L.z * sy[m];
     }
     stf8(dq + 8 * (size_t)i, dx, dy);
-    stf8(qm + 8 * (size_t)i, mx, mn);
+    stf8(qm + 8 * (size_t)i, qmax, qmin);
     if (with_delta) delta[i] = min_delt;
 }
 
 __global__ void __launch_bounds__(GRAD_BLOCK)
-kb_grad32(Geom g, Consts c, Sched s, const float4 *__restrict__ q,
+kb_grad32(Geom g, Consts c, Geom32 f, Sched s, const float4 *__restrict__ q,
           const double *__restrict__ spd, float *__restrict__ dq, float *__restrict__ qm,
           double *__restrict__ delta, int with_delta) {
     __shared__ SchedSmem ss;
@@ -110,56 +107,50 @@ kb_grad32(Geom g, Consts c, Sched s, const float4 *__restrict__ q,
     for (int vp = blockIdx.x * blockDim.x + threadIdx.x; vp < total;
          vp += gridDim.x * blockDim.x) {
         const int i = sched_point(s, ss, vp);
-        if (i >= 0) grad32_point(g, c, q, spd, dq, qm, delta, with_delta, i);
+        if (i >= 0) grad32_point(g, c, f, q, spd, dq, qm, delta, with_delta, i);
     }
 }
 
-// eval_q_inner_loop + eval_update_innerloop (q_variables.F90:115-227).
+// eval_q_inner_loop + eval_update_innerloop (q_variables.F90:115-227) with
+// FP32 sums and the precomputed inverse normal matrix.
 __device__ __forceinline__ void
-inner32_point(const Geom &g, const Consts &c, const float4 *__restrict__ q,
+inner32_point(const Geom &g, const Geom32 &f, const float4 *__restrict__ q,
               const float *__restrict__ dq_in, float *__restrict__ dq_out, int i) {
-    double2 pi_ = g.xy[i];
-    float4 qv = __ldg(q + i);
-    double qi[4] = {qv.x, qv.y, qv.z, qv.w};
-    float dxf[4], dyf[4];
-    ldf8(dq_in + 8 * (size_t)i, dxf, dyf);
-    double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
-    double sdxq[4] = {0.0, 0.0, 0.0, 0.0}, sdyq[4] = {0.0, 0.0, 0.0, 0.0};
-    int nb = g.nbhs[i];
+    const float4 qv = __ldg(q + i);
+    const float qi[4] = {qv.x, qv.y, qv.z, qv.w};
+    float dxi[4], dyi[4];
+    ldf8(dq_in + 8 * (size_t)i, dxi, dyi);
+    float sx[4] = {0.f, 0.f, 0.f, 0.f}, sy[4] = {0.f, 0.f, 0.f, 0.f};
+    const int nb = g.nbhs[i];
     for (int r = 0; r < nb; ++r) {
-        int k = g.conn[r * g.n + i];
-        float4 kv = __ldg(q + k);
+        const int k = g.conn[r * g.n + i];
+        const float2 d = __ldg(f.dxy + r * g.n + i);
+        const float w = f.w ? __ldg(f.w + r * g.n + i) : 1.0f;
+        const float4 kv = __ldg(q + k);
+        const float qk[4] = {kv.x, kv.y, kv.z, kv.w};
         float dxk[4], dyk[4];
         ldf8(dq_in + 8 * (size_t)k, dxk, dyk);
-        double qk[4] = {kv.x, kv.y, kv.z, kv.w};
-        double2 pk = g.xy[k];
-        double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
-        double w = 1.0;
-        if (!c.power_zero) w = pow(sqrt(delx * delx + dely * dely), c.power);
-        sdx2 = sdx2 + delx * delx * w;
-        sdy2 = sdy2 + dely * dely * w;
-        sdxy = sdxy + delx * dely * w;
+        const float wdx = w * d.x, wdy = w * d.y;
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-            double temp1 = qi[m] - 0.5 * (delx * dxf[m] + dely * dyf[m]);
-            double temp2 = qk[m] - 0.5 * (delx * dxk[m] + dely * dyk[m]);
-            sdxq[m] = sdxq[m] + (w * delx * (temp2 - temp1));
-            sdyq[m] = sdyq[m] + (w * dely * (temp2 - temp1));
+            const float temp1 = qi[m] - 0.5f * (d.x * dxi[m] + d.y * dyi[m]);
+            const float temp2 = qk[m] - 0.5f * (d.x * dxk[m] + d.y * dyk[m]);
+            sx[m] = sx[m] + wdx * (temp2 - temp1);
+            sy[m] = sy[m] + wdy * (temp2 - temp1);
         }
     }
-    double det = sdx2 * sdy2 - sdxy * sdxy;
-    double one_by_det = 1.0 / det;
-    double dx[4], dy[4];
+    const float4 L = __ldg(f.lsq + i);
+    float dx[4], dy[4];
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
-        dx[m] = one_by_det * (sdxq[m] * sdy2 - sdyq[m] * sdxy);
-        dy[m] = one_by_det * (sdyq[m] * sdx2 - sdxq[m] * sdxy);
+        dx[m] = L.x * sx[m] + L.y * sy[m];
+        dy[m] = L.y * sx[m] + L.z * sy[m];
     }
     stf8(dq_out + 8 * (size_t)i, dx, dy);
 }
 
 __global__ void __launch_bounds__(GRAD_BLOCK)
-kb_inner32(Geom g, Consts c, Sched s, const float4 *__restrict__ q,
+kb_inner32(Geom g, Geom32 f, Sched s, const float4 *__restrict__ q,
            const float *__restrict__ dq_in, float *__restrict__ dq_out) {
     __shared__ SchedSmem ss;
     load_sched(s, ss);
@@ -167,7 +158,7 @@ kb_inner32(Geom g, Consts c, Sched s, const float4 *__restrict__ q,
     for (int vp = blockIdx.x * blockDim.x + threadIdx.x; vp < total;
          vp += gridDim.x * blockDim.x) {
         const int i = sched_point(s, ss, vp);
-        if (i >= 0) inner32_point(g, c, q, dq_in, dq_out, i);
+        if (i >= 0) inner32_point(g, f, q, dq_in, dq_out, i);
     }
 }
 
@@ -204,10 +195,8 @@ flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, int la
         const float s2q = kind == KIND_WALL ? -1.0f : 1.0f;
         for (int r = lane; r < nb; r += LPP) {
             const int k = g.conn[r * g.n + i];
-            const double2 pi_ = g.xy[i];
-            const double2 pk = g.xy[k];
-            const double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
-            const float dxf = (float)delx, dyf = (float)dely;
+            const float2 d = __ldg(b.f.dxy + r * g.n + i);
+            const float dxf = d.x, dyf = d.y;
             KStateT<float> sk, si;
             {
                 const float4 kv = __ldg(b.q_in + k);
@@ -231,11 +220,9 @@ flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, int la
                                    rho, pr);
                 si = kstate<float>(u1, u2, rho, pr, nxf, nyf, pif);
             }
-            const double tx = ny, ty = -nx;
-            const double dels = delx * tx + dely * ty;
-            const double deln = delx * nx + dely * ny;
-            double w = 1.0;
-            if (!c.power_zero) w = pow(sqrt(dels * dels + deln * deln), c.power);
+            const float dels = dxf * nyf - dyf * nxf;
+            const float deln = dxf * nxf + dyf * nyf;
+            const float w = b.f.w ? __ldg(b.f.w + r * g.n + i) : 1.0f;
             double *e = rec + r * FREC;
             float *ef = reinterpret_cast<float *>(e);
             float Gi[4], Gk[4];
@@ -259,9 +246,8 @@ flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, int la
 #pragma unroll
                 for (int m = 0; m < 4; ++m) ef[4 * L + m] = Gk[m] - Gi[m];
             }
-            e[8] = dels;
-            e[9] = deln;
-            e[10] = w;
+            ef[16] = dels * w;
+            ef[17] = deln * w;
         }
     }
     __syncwarp();
@@ -272,35 +258,29 @@ flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, int la
         const bool used = !((kind == KIND_WALL && L == 2) || (kind == KIND_OUTER && L == 3));
         const unsigned long long bits = ((L < 2) ? mx : my) >> ((L & 1) ? 32 : 0);
         if (used) {
-            double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
             float fx0 = 0.f, fx1 = 0.f, fy0 = 0.f, fy1 = 0.f;
             float cx0 = 0.f, cx1 = 0.f, cy0 = 0.f, cy1 = 0.f;
             for (int r = 0; r < nb; ++r) {
                 if (!((bits >> r) & 1ull)) continue;
-                const double *e = rec + r * FREC;
-                const float *ef = reinterpret_cast<const float *>(e);
-                const double dels = e[8], deln = e[9], w = e[10];
-                const double dels_w = dels * w, deln_w = deln * w;
-                sdx2 = sdx2 + dels * dels_w;
-                sdy2 = sdy2 + deln * deln_w;
-                sdxy = sdxy + dels * deln_w;
+                const float *ef = reinterpret_cast<const float *>(rec + r * FREC);
                 const float d0 = ef[4 * L + c0], d1 = ef[4 * L + c0 + 1];
-                const float sw = (float)dels_w, nw = (float)deln_w;
+                const float sw = ef[16], nw = ef[17];
                 kahan_add(fx0, cx0, d0 * sw);
                 kahan_add(fy0, cy0, d0 * nw);
                 kahan_add(fx1, cx1, d1 * sw);
                 kahan_add(fy1, cy1, d1 * nw);
             }
-            const double det = sdx2 * sdy2 - sdxy * sdxy;
-            const double one_by_det = 1.0 / det;
+            // the list's precomputed solve: x lists a Sx + b Sy, y lists a Sy + b Sx
+            const float4 co = __ldg(b.f.flsq + 2 * (size_t)i + (L >> 1));
+            const double a = (L & 1) ? co.z : co.x, bb = (L & 1) ? co.w : co.y;
             const double X0 = (double)fx0 - cx0, X1 = (double)fx1 - cx1;
             const double Y0 = (double)fy0 - cy0, Y1 = (double)fy1 - cy1;
             if (L < 2) {
-                Gv0 = (X0 * sdy2 - Y0 * sdxy) * one_by_det;
-                Gv1 = (X1 * sdy2 - Y1 * sdxy) * one_by_det;
+                Gv0 = a * X0 + bb * Y0;
+                Gv1 = a * X1 + bb * Y1;
             } else {
-                Gv0 = (Y0 * sdx2 - X0 * sdxy) * one_by_det;
-                Gv1 = (Y1 * sdx2 - X1 * sdxy) * one_by_det;
+                Gv0 = a * Y0 + bb * X0;
+                Gv1 = a * Y1 + bb * X1;
             }
         }
     }
@@ -444,16 +424,18 @@ int wave32(int kind, int block, size_t smem, int grid) {
 }
 }  // namespace
 
-void launch_grad32(const Geom &g, const Consts &c, const Sched &s, const float4 *q,
-                         const double *spd, float *dq, float *qm, double *delta, bool with_delta,
-                         int block, int grid, cudaStream_t st) {
-    kb_grad32<<<wave32(0, block, 0, grid), block, 0, st>>>(g, c, s, q, spd, dq, qm,
-                                                                     delta, with_delta ? 1 : 0);
+void launch_grad32(const Geom &g, const Consts &c, const Geom32 &f, const Sched &s,
+                   const float4 *q, const double *spd, float *dq, float *qm, double *delta,
+                   bool with_delta, int block, int grid, cudaStream_t st) {
+    kb_grad32<<<wave32(0, block, 0, grid), block, 0, st>>>(g, c, f, s, q, spd, dq, qm, delta,
+                                                           with_delta ? 1 : 0);
 }
 
-void launch_inner32(const Geom &g, const Consts &c, const Sched &s, const float4 *q,
-                          const float *dq_in, float *dq_out, int block, int grid, cudaStream_t st) {
-    kb_inner32<<<wave32(1, block, 0, grid), block, 0, st>>>(g, c, s, q, dq_in, dq_out);
+void launch_inner32(const Geom &g, const Consts &c, const Geom32 &f, const Sched &s,
+                    const float4 *q, const float *dq_in, float *dq_out, int block, int grid,
+                    cudaStream_t st) {
+    (void)c;
+    kb_inner32<<<wave32(1, block, 0, grid), block, 0, st>>>(g, f, s, q, dq_in, dq_out);
 }
 
 void launch_flux32(const Geom &g, const Consts &c, const Sched &s, const StageBufs32 &b,
