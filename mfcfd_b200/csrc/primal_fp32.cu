@@ -8,8 +8,9 @@
 // order.  The 2x2 least-squares normal matrices, ill-conditioned on
 // stretched near-wall stencils, are pure geometry: they are formed and
 // inverted once per grid in FP64 (Geom32) and only applied per iteration.
-// Kept in FP64: the local time step, the state update, the residual norm and
-// the force coefficients.
+// The state update runs in FP32 too (the state is stored in FP32); kept in
+// FP64: the local time step, the list derivatives and flux residual, the
+// residual norm (from the FP64 increment) and the force coefficients.
 #include <cuda_runtime.h>
 
 #include "batch.cuh"
@@ -305,47 +306,50 @@ flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, int la
             else fr[m] = delta * (G[0][m] + G[1][m] + G[2][m] + G[3][m]);
         }
         if (b.flux_dbg) st4(reinterpret_cast<R4 *>(b.flux_dbg) + i, fr[0], fr[1], fr[2], fr[3]);
+        // state_update in FP32 (the state is stored in FP32); the residual
+        // from the increment itself, 0.5 euler fr(1), in FP64, which FP32
+        // differences of U(1) would cancel (last stage: rk != 3)
+        if (kind != KIND_OUTER) res_sqr = (0.5 * c.euler * fr[0]) * (0.5 * c.euler * fr[0]);
+        const float nxf = (float)nx, nyf = (float)ny, pif = (float)c.pi, gm1f = (float)c.gm1;
+        float frf[4] = {(float)fr[0], (float)fr[1], (float)fr[2], (float)fr[3]};
         const float4 P = b.prim_in[i];
-        double U[4], Uo[4] = {0.0, 0.0, 0.0, 0.0};
+        float U[4], Uo[4] = {0.f, 0.f, 0.f, 0.f};
         if (kind == KIND_OUTER) {
             const double *inf = g.obc + 8 * (size_t)orow;
-            conserved_ubar(P.x, P.y, P.z, P.w, nx, ny, inf, c.pi, c.gm1, U);
+            const float inff[5] = {(float)inf[0], (float)inf[1], (float)inf[2], (float)inf[3],
+                                   (float)inf[4]};
+            conserved_ubar_t<float>(P.x, P.y, P.z, P.w, nxf, nyf, inff, pif, gm1f, U);
             if (rk == 3) {
                 const float4 O = b.prim_old[i];
-                conserved_ubar(O.x, O.y, O.z, O.w, nx, ny, inf, c.pi, c.gm1, Uo);
+                conserved_ubar_t<float>(O.x, O.y, O.z, O.w, nxf, nyf, inff, pif, gm1f, Uo);
             }
         } else {
-            prim_to_conserved(P.x, P.y, P.z, P.w, nx, ny, U);
+            prim_to_conserved_t<float>(P.x, P.y, P.z, P.w, nxf, nyf, U);
             if (rk == 3) {
                 const float4 O = b.prim_old[i];
-                prim_to_conserved(O.x, O.y, O.z, O.w, nx, ny, Uo);
+                prim_to_conserved_t<float>(O.x, O.y, O.z, O.w, nxf, nyf, Uo);
             }
         }
-        double temp = U[0];
+        const float half_euler = (float)(0.5 * c.euler);
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-            if (rk != 3) U[m] = U[m] - (0.5 * c.euler * fr[m]);
-            else U[m] = TBT * Uo[m] + OBT * (U[m] - 0.5 * fr[m]);
+            if (rk != 3) U[m] = U[m] - half_euler * frf[m];
+            else U[m] = (float)TBT * Uo[m] + (float)OBT * (U[m] - 0.5f * frf[m]);
         }
-        if (kind == KIND_WALL) U[2] = 0.0;
-        double U2_rot = U[1], U3_rot = U[2];
-        U[1] = U2_rot * ny + U3_rot * nx;
-        U[2] = U3_rot * ny - U2_rot * nx;
-        if (kind != KIND_OUTER) res_sqr = (U[0] - temp) * (U[0] - temp);
-        double rho = U[0];
-        temp = 1.0 / U[0];
-        double u1 = U[1] * temp;
-        double u2 = U[2] * temp;
-        double pr = 0.4 * (U[3] - (0.5 * temp) * (U[1] * U[1] + U[2] * U[2]));
-        b.prim_out[i] = make_float4((float)rho, (float)u1, (float)u2, (float)pr);
-        double qn[4];
-        q_from_prim((double)(float)rho, (double)(float)u1, (double)(float)u2, (double)(float)pr,
-                    qn);
-        b.q_out[i] = make_float4((float)qn[0], (float)qn[1], (float)qn[2], (float)qn[3]);
-        if (last) {
-            double fu1 = (float)u1, fu2 = (float)u2, frho = (float)rho, fpr = (float)pr;
-            b.spd[i] = sqrt(fu1 * fu1 + fu2 * fu2) + 3.0 * sqrt(fpr / frho);
-        }
+        if (kind == KIND_WALL) U[2] = 0.f;
+        const float U2_rot = U[1], U3_rot = U[2];
+        U[1] = U2_rot * nyf + U3_rot * nxf;
+        U[2] = U3_rot * nyf - U2_rot * nxf;
+        const float rho = U[0];
+        const float temp = 1.0f / U[0];
+        const float u1 = U[1] * temp;
+        const float u2 = U[2] * temp;
+        const float pr = 0.4f * (U[3] - (0.5f * temp) * (U[1] * U[1] + U[2] * U[2]));
+        b.prim_out[i] = make_float4(rho, u1, u2, pr);
+        float qn[4];
+        q_from_prim_t<float>(rho, u1, u2, pr, qn);
+        b.q_out[i] = make_float4(qn[0], qn[1], qn[2], qn[3]);
+        if (last) b.spd[i] = (double)(sqrtf(u1 * u1 + u2 * u2) + 3.0f * sqrtf(pr / rho));
     }
     if (last) {
         if (lane == 0) sres[grp] = res_sqr;
