@@ -33,9 +33,11 @@ void launch_flux_b(const Geom &g, const Consts &c, const R4 *q_in, const double 
 void launch_inner_b(const Geom &g, const R4 *q, const double *dq_in, const double *dqb_out,
                     double *dqb_in, double *qb, double *xb, double *yb, double *contrib,
                     cudaStream_t s);
+// spdA: |u| + 3 sqrt(p/rho) of primA as the forward pass used it (taped)
 void launch_grad_b(const Geom &g, const Consts &c, const R4 *q, const R4 *primA,
-                   const double *dqb, const double *qmb, const double *deltab, bool with_delta,
-                   double *qb, double *xb, double *yb, double *contrib, cudaStream_t s);
+                   const double *spdA, const double *dqb, const double *qmb,
+                   const double *deltab, bool with_delta, double *qb, double *xb, double *yb,
+                   double *contrib, cudaStream_t s);
 void launch_gather(int n, int kp, const int *tptr, const int *tlist, const double *contrib,
                    int mode, double *a4, double *a8, double *b8, double *xb, double *yb,
                    cudaStream_t s);

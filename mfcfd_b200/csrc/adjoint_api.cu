@@ -198,7 +198,10 @@ int record(mfcfd_t *h, AdjointState *a, const R4 *from) {
         b.dq = dq_at(a, rk, m);
         b.qm = qm_at(a, rk);
         b.delta = a->tdelta;
-        b.spd = a->tspd;
+        // tspd keeps the input state's spd for the reverse of func_delta; the
+        // last stage's spd of the output goes to the handle's own buffer
+        // (rebuilt when the adjoint restores the state)
+        b.spd = h->d_spd;
         b.res_part = h->d_res_part;
         b.flux_dbg = reinterpret_cast<double *>(a->tfr[rk - 1]);
         launch_flux(h->geom, h->consts, h->sched, b, rk, rk == rks, h->flux_grid, h->stream);
@@ -239,8 +242,8 @@ int reverse_taped(mfcfd_t *h, AdjointState *a) {
             launch_gather(n, a->kp, a->d_tptr, a->d_tlist, a->contrib, ADJ_GATHER_INNER, a->qb,
                           a->dqb[(t - 1) & 1], nullptr, a->xb, a->yb, s);
         }
-        launch_grad_b(h->geom, h->consts, a->tq[rk - 1], a->tprim[0], a->dqb[0], a->qmb,
-                      a->deltab, rk == 1, a->qb, a->xb, a->yb, a->contrib, s);
+        launch_grad_b(h->geom, h->consts, a->tq[rk - 1], a->tprim[0], a->tspd, a->dqb[0],
+                      a->qmb, a->deltab, rk == 1, a->qb, a->xb, a->yb, a->contrib, s);
         launch_gather(n, a->kp, a->d_tptr, a->d_tlist, a->contrib, ADJ_GATHER_GRAD, a->qb,
                       nullptr, a->pbA, a->xb, a->yb, s);
         launch_qvar_b(n, a->tprim[rk - 1], a->qb, pb_in, s);

@@ -529,7 +529,8 @@ k_inner_b(Geom g, const R4 *__restrict__ q, const double *__restrict__ dq_in,
 // eval_q_derivatives_b (+ func_delta_b on the first stage)
 __global__ void __launch_bounds__(BLK, ADJ_MIN_BLOCKS)
 k_grad_b(Geom g, Consts c, const R4 *__restrict__ q, const R4 *__restrict__ primA,
-         const double *__restrict__ dqb, const double *__restrict__ qmb,
+         const double *__restrict__ spdA, const double *__restrict__ dqb,
+         const double *__restrict__ qmb,
          const double *__restrict__ deltab, int with_delta, double *__restrict__ qb,
          double *__restrict__ xb, double *__restrict__ yb, double *__restrict__ contrib) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -561,10 +562,9 @@ k_grad_b(Geom g, Consts c, const R4 *__restrict__ q, const R4 *__restrict__ prim
             sy[m] = sy[m] + dely * (qk[m] - qi[m]);
         }
         if (with_delta) {
-            const R4 P = ld4(primA + k);
-            const double spd = sqrt(P.b * P.b + P.c * P.c) + 3.0 * sqrt(P.d / P.a);
+            // the taped spd of the stage's input state: the forward's own values
             const double dist = sqrt(delx * delx + dely * dely);
-            double delta_t = dist / spd;
+            double delta_t = dist / spdA[k];
             delta_t = c.cfl * delta_t;
             if (min_delt > delta_t) { min_delt = delta_t; amd = r; }
         }
@@ -790,10 +790,11 @@ void launch_inner_b(const Geom &g, const R4 *q, const double *dq_in, const doubl
 }
 
 void launch_grad_b(const Geom &g, const Consts &c, const R4 *q, const R4 *primA,
-                   const double *dqb, const double *qmb, const double *deltab, bool with_delta,
-                   double *qb, double *xb, double *yb, double *contrib, cudaStream_t s) {
-    k_grad_b<<<nblk(g.n, BLK), BLK, 0, s>>>(g, c, q, primA, dqb, qmb, deltab, with_delta ? 1 : 0,
-                                           qb, xb, yb, contrib);
+                   const double *spdA, const double *dqb, const double *qmb,
+                   const double *deltab, bool with_delta, double *qb, double *xb, double *yb,
+                   double *contrib, cudaStream_t s) {
+    k_grad_b<<<nblk(g.n, BLK), BLK, 0, s>>>(g, c, q, primA, spdA, dqb, qmb, deltab,
+                                           with_delta ? 1 : 0, qb, xb, yb, contrib);
 }
 
 void launch_gather(int n, int kp, const int *tptr, const int *tlist, const double *contrib,
