@@ -41,6 +41,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from mfcfd_b200.replicas import max_over_ranks, shard, sum_over_ranks  # noqa: E402
+
 METRIC = "Mpoint-iters/s @1M pts FP32-mix vs FP64 at |ΔCl|≤1e-5; adjoint/primal cost"
 UNIT = "Mpoint-iters/s"
 FALLBACK_HBM_GBS = 6650.0
@@ -239,10 +241,7 @@ def adjoint_cost(args, stream, world, dist):
         e1.record(stream)
         torch.cuda.synchronize()
         adj_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([primal_ms, adj_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        primal_ms, adj_ms = (float(v) for v in t.tolist())
+    primal_ms, adj_ms = max_over_ranks([primal_ms, adj_ms], dist)
     return {"config": f"{args.adjoint_config}: {grid.n:,} points, J = Cd, {n} iterations reversed",
             "primal_ms": primal_ms, "adjoint_ms": adj_ms, "cost_ratio": adj_ms / primal_ms,
             "forward_iterations": nf, "checkpoint_budget_bytes": 2 << 30,
@@ -260,7 +259,7 @@ def batch_leg(args, stream, world, rank, dist):
     from mfcfd_b200.grid import batch_instances
     from mfcfd_b200.solver import Solver
     grids, flows, specs = batch_instances(args.batch_instances)
-    mine = list(range(rank, len(grids), world))
+    mine = shard(len(grids), rank, world)
     grids, flows = [grids[i] for i in mine], [flows[i] for i in mine]
     n = args.batch_iters
     with Batch(grids, flows) as b:
@@ -289,13 +288,8 @@ def batch_leg(args, stream, world, rank, dist):
             e1.record(stream)
             torch.cuda.synchronize()
             seq_ms += e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([batch_ms, seq_ms, float(work)], device="cuda", dtype=torch.float64)
-        tmax = t[:2].clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tw = t[2:].clone()
-        dist.all_reduce(tw, op=dist.ReduceOp.SUM)
-        batch_ms, seq_ms, work = float(tmax[0]), float(tmax[1]), float(tw[0])
+    batch_ms, seq_ms = max_over_ranks([batch_ms, seq_ms], dist)
+    work = sum_over_ranks([work], dist)[0]
     states = {k: r.state.count(k) for k in sorted(set(r.state))}
     return {"config": (f"{args.batch_instances} NACA 00tt O-grids, N log-uniform in [4k, 256k] "
                        f"(seeded draws), M in [0.5, 0.8], aoa in [-2, 4] deg, t in [0.08, 0.16], "
@@ -374,10 +368,8 @@ def main():
         torch.cuda.synchronize()
     launches = solver.launch_count() - launches0
     ms = t_start.elapsed_time(t_end)
+    ms = max_over_ranks([ms], dist)[0]
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     clocks = clk.summary()
     value = world * grid.n * args.steps / (ms / 1e3) / 1e6
@@ -398,10 +390,7 @@ def main():
         f_end.record(stream)
         torch.cuda.synchronize()
         ms32 = f_start.elapsed_time(f_end)
-        if dist:
-            t = torch.tensor([ms32], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms32 = float(t.item())
+        ms32 = max_over_ranks([ms32], dist)[0]
         cl32, cd32, _, _ = s32.forces()
         kt32 = s32.profile_iteration()
         s32.close()
@@ -455,10 +444,7 @@ def main():
         e_ms = e_start.elapsed_time(e_end)
         wall_ms = (time.perf_counter() - t0) * 1e3
         e_ms = max(e_ms, wall_ms)
-        if dist:
-            t = torch.tensor([e_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = float(t.item())
+        e_ms = max_over_ranks([e_ms], dist)[0]
         state_bytes = 32 * grid.n
         e2e = {"value": world * grid.n * args.steps / (e_ms / 1e3) / 1e6, "unit": UNIT,
                "h2d_bytes_per_step": state_bytes / args.steps,
