@@ -80,17 +80,22 @@ def measured_peaks() -> dict:
     return {}
 
 
-def profiled_traffic(workload: str):
-    """dram bytes per launch of kb_flux from the committed ncu summary."""
+def _profile_value(key: str):
+    """A figure of the committed ncu summary of kb_flux (``key: value`` line)."""
     p = os.path.join(ROOT, "profiles", "kb_flux_fp64_c2.md")
     if not os.path.exists(p):
         return None
     with open(p) as fh:
         for line in fh:
-            m = re.match(r"\s*dram_bytes_per_launch_full_size:\s*([0-9.eE+]+)", line)
+            m = re.match(r"\s*" + key + r":\s*([0-9.eE+]+)", line)
             if m:
                 return float(m.group(1))
     return None
+
+
+def profiled_traffic(workload: str):
+    """dram bytes per launch of kb_flux from the committed ncu summary."""
+    return _profile_value("dram_bytes_per_launch_full_size")
 
 
 class ClockSampler:
@@ -418,7 +423,9 @@ def main():
                 "kernel": "kb_flux (flux residual + state update, one SSPRK stage)",
                 "algorithmic_bytes_per_launch": flux_bytes,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6.65 TB/s",
-                "note": "the kernel is bound by FP64 issue (exp/erf/log/div), not HBM: see DESIGN.md"}
+                "fp64_pipe_active_frac": _profile_value("fp64_pipe_active_frac"),
+                "note": ("the kernel is bound by FP64 issue (exp/erf/log/div), not HBM: its "
+                         "FP64 pipe is busy fp64_pipe_active_frac of its active cycles (ncu)")}
     iter_bytes = ab["iteration"] * grid.n
     iteration_roof = {"algorithmic_bytes_per_iteration": iter_bytes,
                       "achieved_gbs": iter_bytes / (ms / args.steps / 1e3) / 1e9,
