@@ -8,6 +8,8 @@ optionally CASE_DIR/restart/sol.dat, runs max_iters iterations on the GPU and
 writes CASE_DIR/residue, CASE_DIR/cp/cp-file, every nsave iterations
 CASE_DIR/solution/sol.dat, and at the end the CUDA tree's CASE_DIR/output.dat
 (with Mach number, entropy and adaptation sensor), in the reference's formats.
+With ``-adjoint_mode`` in case.in it runs the reference's adjoint case instead
+and writes CASE_DIR/sensitivity/sensitivity.dat.
 """
 from __future__ import annotations
 
@@ -33,6 +35,8 @@ def run_case(case_dir: str, grid=None, quiet: bool = False, chunk: int = 100) ->
         itr, res_old, prim0 = io.read_restart(os.path.join(case_dir, "restart", "sol.dat"), grid.n)
         params["res_old"] = res_old
     log = (lambda *a: None) if quiet else print
+    if "adjoint_mode" in opts:
+        return _run_adjoint_case(case_dir, grid, params, opts, itr, res_old, prim0, log)
     t0 = time.perf_counter()
     its, res = [], []
     with Solver(grid, **params) as s:
@@ -66,6 +70,33 @@ def run_case(case_dir: str, grid=None, quiet: bool = False, chunk: int = 100) ->
     log(f" Run time: {run_time:.6f} seconds")
     return dict(iterations=len(res), residue=res, cl=cl, cd=cd, cm=cm, cp=cp, prim=prim,
                 run_time=run_time, total_entropy=total_entropy)
+
+
+def _run_adjoint_case(case_dir, grid, params, opts, itr, res_old, prim0, log) -> dict:
+    """The reference's adjoint run (src_mpi_adjoint/meshfree_solver.F90:90-104):
+    ``-adjoint_mode blackbox`` keeps every iteration's state, ``checkpoints``
+    keeps ``-chkpts`` snapshots (q_lskum_chkpts_b.F90:65-91); dCd/dx, dCd/dy
+    go to sensitivity/sensitivity.dat (post_processing.F90:41-66)."""
+    max_iters = int(opts["max_iters"])
+    n_rows = max_iters + 1 if opts["adjoint_mode"] == "blackbox" else int(opts.get("chkpts", 0)) + 1
+    ckpt_bytes = 32 * grid.n * max(n_rows, 1)
+    t0 = time.perf_counter()
+    with Solver(grid, **params) as s:
+        if prim0 is not None:
+            s.set_state(prim0)
+        J, dJdx, dJdy, n_forward = s.adjoint(max_iters, "cd", ckpt_bytes=ckpt_bytes)
+        cl, cd, cm, cp = s.forces()
+        prim = s.get_state()
+    run_time = time.perf_counter() - t0
+    it = itr + max_iters + 1
+    io.write_sensitivity(os.path.join(case_dir, "sensitivity", "sensitivity.dat"), grid, dJdx,
+                         dJdy, it)
+    io.write_solution(os.path.join(case_dir, "solution", "sol.dat"), grid, prim, it, res_old)
+    io.write_cp(os.path.join(case_dir, "cp", "cp-file"), grid, cp)
+    log(f" Vector function is {J:.17g}")
+    log(f" Run time: {run_time:.6f} seconds ({n_forward} forward iterations)")
+    return dict(iterations=max_iters, J=J, dJdx=dJdx, dJdy=dJdy, cl=cl, cd=cd, cm=cm, cp=cp,
+                prim=prim, run_time=run_time, n_forward=n_forward)
 
 
 if __name__ == "__main__":

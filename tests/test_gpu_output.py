@@ -52,3 +52,25 @@ def test_driver_runs_a_case_directory(gpu, tmp_path):
     itr, _, prim12 = io.read_restart(str(tmp_path / "output.dat"), g.n)
     assert itr == 12 and np.array_equal(prim12, out["prim"])
     assert (tmp_path / "cp" / "cp-file").exists()
+
+
+@pytest.mark.parametrize("mode", ["blackbox", "checkpoints"])
+def test_driver_runs_an_adjoint_case(gpu, tmp_path, mode):
+    # src_mpi_adjoint's run: -adjoint_mode, -chkpts; sensitivity/sensitivity.dat out
+    from mfcfd_b200 import io
+    from mfcfd_b200.driver import run_case
+    g = naca_ogrid(24, 10, seed=10, first_spacing=5e-3)
+    (tmp_path / "point").mkdir()
+    io.write_partgrid(g, str(tmp_path / "point" / "partGrid"))
+    (tmp_path / "case.in").write_text(f"-cfl 0.2\n-max_iters 6\n-vl_const 5\n-adjoint_mode {mode}\n"
+                                      "-chkpts 2\n")
+    out = run_case(str(tmp_path), quiet=True)
+    gg = io.read_partgrid(str(tmp_path / "point" / "partGrid"))
+    with Solver(gg, cfl=0.2, vl_const=5.0) as s:
+        J, dx, dy, nf = s.adjoint(6, "cd")
+    assert out["J"] == J
+    rows = np.loadtxt(tmp_path / "sensitivity" / "sensitivity.dat", skiprows=1)
+    assert np.array_equal(rows[:, 0].astype(int), np.arange(1, g.n + 1))
+    np.testing.assert_allclose(rows[:, 1], dx, rtol=1e-15, atol=0)
+    np.testing.assert_allclose(rows[:, 2], dy, rtol=1e-15, atol=0)
+    assert (out["n_forward"] > nf) == (mode == "checkpoints")
