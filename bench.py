@@ -372,6 +372,9 @@ def main():
         t_end.record(stream)
         torch.cuda.synchronize()
     launches = solver.launch_count() - launches0
+    if solver.halted or len(res) != args.steps:
+        raise RuntimeError(f"FP64 run stopped on a non-finite residue after {len(res)} of "
+                           f"{args.steps} timed iterations: no throughput to report")
     ms = t_start.elapsed_time(t_end)
     ms = max_over_ranks([ms], dist)[0]
     if dist:
@@ -391,13 +394,14 @@ def main():
         f_start = torch.cuda.Event(enable_timing=True)
         f_end = torch.cuda.Event(enable_timing=True)
         f_start.record(stream)
-        s32.run(args.steps)
+        res32 = s32.run(args.steps)
         f_end.record(stream)
         torch.cuda.synchronize()
         ms32 = f_start.elapsed_time(f_end)
         ms32 = max_over_ranks([ms32], dist)[0]
+        halted32 = bool(s32.halted) or len(res32) != args.steps
         cl32, cd32, _, _ = s32.forces()
-        kt32 = s32.profile_iteration()
+        kt32 = {} if halted32 else s32.profile_iteration()
         s32.close()
         v32 = world * grid.n * args.steps / (ms32 / 1e3) / 1e6
         fp32 = {"value": v32, "unit": UNIT, "ms_per_step": ms32 / args.steps,
@@ -405,9 +409,13 @@ def main():
                 "dCl": abs(float(cl32[0] - cl64[0])), "dCd": abs(float(cd32[0] - cd64[0])),
                 "Cl_fp64": float(cl64[0]), "Cd_fp64": float(cd64[0]),
                 "kernel_ms": {k: float(v) for k, v in kt32.items()},
-                "note": "FP32 state and per-neighbour flux work, FP64 least squares, "
-                        "update, residual and forces; dCl/dCd against the FP64 run after "
-                        "the same iterations"}
+                "note": "FP32 state, fluxes, sums and state update; geometry (LSQ "
+                        "inverses) formed in FP64 once; FP64 residual and forces; dCl/dCd "
+                        "against the FP64 run after the same iterations"}
+        if halted32:
+            fp32.update(value=None, speedup_vs_fp64=None, ms_per_step=None,
+                        nonfinite=True, iterations_done=len(res32),
+                        note="FP32-mixed run stopped on a non-finite residue")
 
     # per-kernel CUDA-event durations on the same stream (extra iterations)
     prof = [solver.profile_iteration() for _ in range(3)]

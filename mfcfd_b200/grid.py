@@ -161,8 +161,12 @@ def split_conditioning(g: "Grid", chunk: int = 1 << 20):
     return rel, cnt
 
 
-def _list_rel_det(g, p, d, tx, ty, nx, ny):
+def _list_rel_det(g, p, d, tx, ty, nx, ny, extra=None):
+    """Relative determinant of list d of point p, with point ``extra``
+    (0-based) appended to the stencil when given."""
     nb = g.conn[:g.nbhs[p], p] - 1
+    if extra is not None:
+        nb = np.append(nb, extra)
     dx, dy = g.x[nb] - g.x[p], g.y[nb] - g.y[p]
     ds, dn = dx * tx + dy * ty, dx * nx + dy * ny
     m = _split_membership(np.full(nb.shape, g.flag_1[p]), ds, dn)[d]
@@ -212,6 +216,71 @@ def _augment_stencils(g: "Grid", ni: int, nj: int, min_rel: float) -> int:
     return int(bad.size)
 
 
+def _repair_stencils(g: "Grid", ni: int, nj: int, min_rel: float) -> int:
+    """Rebuilds the stencils that _augment_stencils left singular.
+
+    Nearest-first filling fails where every close candidate of a list lies on
+    one line through the point: at the wall points next to a sharp trailing
+    edge, whose (i, j>=1) neighbours all sit behind them along straight rays,
+    so that one list holds only (collinear) wall points while the others use
+    up the MAX_NBHS slots.  Such a point restarts from its base stencil (8
+    interior, 5 ring) and, while a used list is below ``min_rel``, gives the
+    worst list one point of the (i+-w, j+-3) block (w = 3, 8, 16, 32, 48):
+    the nearest candidate that makes the list well-posed, else the one that
+    raises its relative determinant most (at least tenfold).  Points whose
+    lists were all well-posed after the first pass are left untouched.
+    Returns the number of points rebuilt."""
+    rel, _ = split_conditioning(g)
+    bad = np.where((rel < min_rel).any(1))[0]
+    if bad.size == 0:
+        return 0
+    nx, ny = reference_normals(g)
+    for p in bad:
+        p = int(p)
+        j, i = divmod(p, ni)
+        tx, ty = ny[p], -nx[p]
+        base = 8 if g.flag_1[p] == INTERIOR else 5
+        g.conn[base:, p] = 0
+        g.nbhs[p] = base
+        lists = [d for d in range(4)
+                 if not ((g.flag_1[p] == WALL and d == 2) or (g.flag_1[p] == OUTER and d == 3))]
+        given_up = set()
+        while g.nbhs[p] < MAX_NBHS:
+            cur = {d: _list_rel_det(g, p, d, tx, ty, nx[p], ny[p])
+                   for d in lists if d not in given_up}
+            low = [d for d in cur if cur[d] < min_rel]
+            if not low:
+                break
+            d = min(low, key=lambda e: cur[e])
+            present = set((g.conn[:g.nbhs[p], p] - 1).tolist())
+            pick = None
+            for w in (3, 8, 16, 32, 48):
+                cand = {jj * ni + (i + di) % ni for jj in range(max(0, j - 3), min(nj, j + 4))
+                        for di in range(-w, w + 1)}
+                cand = np.array(sorted(cand - {p} - present), dtype=np.int64)
+                cdx, cdy = g.x[cand] - g.x[p], g.y[cand] - g.y[p]
+                cds, cdn = cdx * tx + cdy * ty, cdx * nx[p] + cdy * ny[p]
+                inlist = _split_membership(np.full(cand.shape, g.flag_1[p]), cds, cdn)[d]
+                order = [c for c in np.argsort(np.hypot(cdx, cdy), kind="stable") if inlist[c]]
+                if not order:
+                    continue
+                after = [_list_rel_det(g, p, d, tx, ty, nx[p], ny[p], cand[c]) for c in order]
+                good = [k for k, a in enumerate(after) if a >= min_rel]
+                if good:
+                    pick = cand[order[good[0]]]
+                    break
+                best = int(np.argmax(after))
+                if after[best] > 10.0 * max(cur[d], 0.0) and after[best] > 1e-8:
+                    pick = cand[order[best]]
+                    break
+            if pick is None:
+                given_up.add(d)
+                continue
+            g.conn[g.nbhs[p], p] = pick + 1
+            g.nbhs[p] += 1
+    return int(bad.size)
+
+
 def naca_ogrid(ni: int, nj: int, thickness: float = 0.12, radius: float = 20.0,
                first_spacing: float = 1e-3, jitter: float = 0.1, seed: int = 0,
                name: str = "", spacing: str = "cosine", rays: str = "straight",
@@ -239,7 +308,9 @@ def naca_ogrid(ni: int, nj: int, thickness: float = 0.12, radius: float = 20.0,
     is singular -- relative determinant below ``min_rel_det`` -- gets the
     nearest extra points of its (i+-3, j+-2) block appended until the list is
     well-posed; near the sharp trailing edge this is unavoidable with a fixed
-    8/5 stencil.  Point ids run 1..N in (j, i) order.
+    8/5 stencil.  A point still singular after that is rebuilt by
+    _repair_stencils (worst list first, from a wider block).  Point ids run
+    1..N in (j, i) order.
     """
     if ni < 4 or nj < 3:
         raise ValueError("naca_ogrid needs ni >= 4 and nj >= 3")
@@ -392,6 +463,7 @@ def naca_ogrid(ni: int, nj: int, thickness: float = 0.12, radius: float = 20.0,
              name=name or f"naca00{int(round(thickness * 100)):02d}_{ni}x{nj}")
     if augment:
         _augment_stencils(g, ni, nj, min_rel_det)
+        _repair_stencils(g, ni, nj, min_rel_det)
     # min_dist: distance to the nearest stencil neighbour (the reference reads
     # it from the grid file and never recomputes it)
     kmax = int(g.nbhs.max())

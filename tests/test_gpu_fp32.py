@@ -46,3 +46,19 @@ def test_fp32_mixed_inner_iterations_and_state_io(gpu):
         dq32, dq64 = b.get_array("dq"), a.get_array("dq")
         scale = np.max(np.abs(dq64), axis=0)
         assert np.max(np.abs(dq32 - dq64) / np.maximum(scale, 1e-12)) < 1e-3
+
+
+def test_fp32_mixed_fine_trailing_edge(gpu):
+    # the C5 wall (2560 cosine-spaced points, first spacing 1e-3, M 0.8):
+    # with the trailing-edge stencils repaired every split list is
+    # well-posed and FP32-mixed runs as FP64 does
+    g = naca_ogrid(2560, 16, seed=5000, first_spacing=1e-3)
+    f = dict(config_flow("C5"))
+    with Solver(g, **f) as a, Solver(g, precision="fp32_mixed", **f) as b:
+        ra, rb = a.run(30), b.run(30)
+        assert not a.halted and not b.halted and len(rb) == 30
+        cla, cda, _, _ = a.forces()
+        clb, cdb, _, _ = b.forces()
+    assert np.isfinite(rb).all()
+    assert np.max(np.abs(ra - rb)) < 1e-3
+    assert abs(cla[0] - clb[0]) < 1e-5 and abs(cda[0] - cdb[0]) < 1e-5

@@ -47,6 +47,18 @@ def test_split_lists_well_posed(ni, nj):
     assert (cnt[used] >= 2).all()
 
 
+def test_split_lists_well_posed_at_fine_trailing_edge():
+    # 2560 cosine-spaced wall points with a 1e-3 first spacing (the C5 wall
+    # and spacing): nearest-first augmentation leaves trailing-edge wall
+    # points with a list of collinear wall points; the repair pass rebuilds
+    # them within MAX_NBHS
+    g = naca_ogrid(2560, 16, seed=5000, first_spacing=1e-3)
+    rel, cnt = split_conditioning(g)
+    assert rel.min() >= 1e-4
+    assert (cnt[np.isfinite(rel)] >= 2).all()
+    assert int(g.nbhs.max()) <= 20
+
+
 def test_config_c1_size():
     g = config_grid("C1")
     assert g.n == 16000
