@@ -19,6 +19,8 @@ FP64 -- the workload the headline metric is quoted on.  Grids are synthetic
   fp32_mixed, adjoint, batch  the FP32-mixed loop on the same workload, the
             reverse-mode cost against the primal, and the 64-instance batched
             workload against one handle at a time
+  adjoint_batch  the adjoint of Cd over 16 instances of 16k-1M points in one
+            mfcfd_adjoint_many call against one mfcfd_adjoint at a time
 
 ``--impl reference`` times that CPU restatement alone (the reference itself
 is Fortran + MPI + PETSc + HDF5 and cannot be built on these machines).
@@ -253,6 +255,64 @@ def adjoint_cost(args, stream, world, dist):
             "J": J, "grad_max": float(max(np.abs(dx).max(), np.abs(dy).max()))}
 
 
+def adjoint_batch_leg(args, world, rank, dist):
+    """The batched adjoint: 16 seeded instances of 16k-1M points (thickness,
+    M and aoa drawn per instance as for the batched primal), sharded across
+    ranks, each developed for the warm-up iterations and then reversed over
+    n iterations for J = Cd (2 GB of snapshots each).  Timed twice from the
+    same states, after an untimed call that allocates every buffer: one
+    mfcfd_adjoint per instance in turn, and one mfcfd_adjoint_many call
+    (each instance on its own stream and host thread).  Both calls are
+    synchronous, so each is timed on the host around the call (gradients to
+    host included); max over ranks."""
+    import torch
+    from mfcfd_b200.grid import batch_instances, naca_ogrid
+    from mfcfd_b200.solver import Solver, adjoint_many
+    grids, flows, _ = batch_instances(args.adjoint_batch_instances, config=5, n_min=16000,
+                                      n_max=1_000_000)
+    mine = shard(len(grids), rank, world)
+    grids, flows = [grids[i] for i in mine], [flows[i] for i in mine]
+    n = args.adjoint_batch_iters
+    budget = 2 << 30
+    with Solver(naca_ogrid(32, 12, seed=1, first_spacing=5e-3), **flows[0]) as w:
+        w.adjoint(2, "cd")  # untimed: module loading
+    solvers = [Solver(g, **f) for g, f in zip(grids, flows)]
+    try:
+        for s in solvers:
+            s.run(args.warmup)
+        start = [s.get_state() for s in solvers]
+        # untimed: allocates every handle's tape and snapshot pool, so that
+        # neither timed pass pays for allocation
+        adjoint_many(solvers, n, "cd", ckpt_bytes=budget)
+        for s, p in zip(solvers, start):
+            s.set_state(p)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        single = [s.adjoint(n, "cd", ckpt_bytes=budget) for s in solvers]
+        seq_s = time.perf_counter() - t0
+        for s, p in zip(solvers, start):
+            s.set_state(p)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        many = adjoint_many(solvers, n, "cd", ckpt_bytes=budget)
+        many_s = time.perf_counter() - t0
+        same = all(np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2]) and a[0] == b[0]
+                   for a, b in zip(single, many))
+    finally:
+        for s in solvers:
+            s.close()
+    seq_s, many_s = max_over_ranks([seq_s, many_s], dist)
+    points = sum_over_ranks([sum(g.n for g in grids)], dist)[0]
+    return {"config": (f"{args.adjoint_batch_instances} NACA 00tt O-grids, N log-uniform in "
+                       f"[16k, 1M] (seeded draws), M in [0.5, 0.8], aoa in [-2, 4] deg, t in "
+                       f"[0.08, 0.16], FP64, J = Cd, {n} iterations reversed each"),
+            "instances_per_rank": len(grids), "points": int(points),
+            "one_call_s": many_s, "one_handle_at_a_time_s": seq_s,
+            "speedup_vs_one_at_a_time": seq_s / many_s,
+            "value": points * n / many_s / 1e6, "unit": "Mpoint-iters reversed/s",
+            "bitwise_equal_to_single": bool(same)}
+
+
 def batch_leg(args, stream, world, rank, dist):
     """The batched workload: 64 seeded instances (4k-256k points, M, aoa and
     thickness drawn per instance), sharded across ranks with no exchange,
@@ -323,6 +383,9 @@ def main():
     ap.add_argument("--batch-iters", type=int, default=100,
                     help="iterations of the batched-workload leg (0 = skip)")
     ap.add_argument("--batch-instances", type=int, default=64)
+    ap.add_argument("--adjoint-batch-iters", type=int, default=20,
+                    help="iterations reversed by the batched-adjoint leg (0 = skip)")
+    ap.add_argument("--adjoint-batch-instances", type=int, default=16)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "mfcfd":
         args.warmup = 3
@@ -475,6 +538,10 @@ def main():
     if args.batch_iters > 0:
         batch = batch_leg(args, stream, world, rank, dist)
 
+    adjoint_batch = None
+    if args.adjoint_batch_iters > 0:
+        adjoint_batch = adjoint_batch_leg(args, world, rank, dist)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(grid, flow, args.cpu_seconds)
@@ -491,6 +558,7 @@ def main():
             "fp32_mixed": fp32,
             "adjoint": adjoint,
             "batch": batch,
+            "adjoint_batch": adjoint_batch,
         }
         print(json.dumps(line), flush=True)
     solver.close()

@@ -121,6 +121,22 @@ int mfcfd_objective(mfcfd_t *h, int objective, double *J);
 int mfcfd_adjoint(mfcfd_t *h, int objective, int n_iters, size_t ckpt_bytes, double *J,
                   double *dJdx, double *dJdy, int *n_forward);
 
+/* mfcfd_adjoint of n_handles independent solvers (grids of any sizes) in one
+ * call: the adjoint a batch of cases needs, the reference running one case
+ * per process.  Each handle's buffers and snapshot pool (ckpt_bytes each) are
+ * allocated first, one handle after the other; then each handle's reverse
+ * sweep is enqueued by a host thread of its own on the handle's own stream,
+ * so that the sweeps of small grids run side by side on the GPU.  Results
+ * per handle are those of mfcfd_adjoint on it (bit for bit): J[i] (J may be
+ * NULL), dJdx[i], dJdy[i] (caller order), n_forward[i] (may be NULL),
+ * status[i] (may be NULL; MFCFD_OK or that handle's error).  Handles must be
+ * distinct and on distinct streams.  Returns MFCFD_OK or the first
+ * handle's error. */
+#define MFCFD_ADJOINT_MANY_MAX 256
+int mfcfd_adjoint_many(int n_handles, mfcfd_t *const *handles, int objective, int n_iters,
+                       size_t ckpt_bytes, double *J, double *const *dJdx, double *const *dJdy,
+                       int *n_forward, int *status);
+
 /* Forward-mode (tangent) derivative of the loop (the reference's Q_LSKUM_D,
  * src_mpi_forward/sensitivity_files/q_lskum_d.F90:28-89, which seeds
  * pointd%x(1) = 1).  From the handle's current state (held fixed) it runs

@@ -29,13 +29,15 @@ EXPORTS = ("mfcfd_default_params", "mfcfd_create", "mfcfd_destroy", "mfcfd_set_s
            "mfcfd_get_state", "mfcfd_run", "mfcfd_forces", "mfcfd_set_stream",
            "mfcfd_get_array", "mfcfd_keep_diagnostics", "mfcfd_info", "mfcfd_strerror",
            "mfcfd_last_error", "mfcfd_launch_count", "mfcfd_profile_iteration",
-           "mfcfd_run_noalloc", "mfcfd_adjoint", "mfcfd_tangent", "mfcfd_output_fields",
+           "mfcfd_run_noalloc", "mfcfd_adjoint", "mfcfd_adjoint_many", "mfcfd_tangent",
+           "mfcfd_output_fields",
            "mfcfd_objective",
            "mfcfd_batch_create", "mfcfd_batch_destroy",
            "mfcfd_batch_set_stream", "mfcfd_batch_set_state", "mfcfd_batch_get_state",
            "mfcfd_batch_run", "mfcfd_batch_forces", "mfcfd_batch_tune", "mfcfd_batch_set_launch",
            "mfcfd_batch_info", "mfcfd_batch_last_error", "mfcfd_batch_launch_count")
 MFCFD_BATCH_MAX = 256
+MFCFD_ADJOINT_MANY_MAX = 256
 OBJECTIVES = {"cl": 0, "cd": 1, "entropy": 2, "enstrophy": 3, "stagnation": 4}
 BATCH_STATES = {0: "running", 1: "converged", 2: "max_iters", 3: "nonfinite"}
 MFCFD_NOALLOC_MAX_ITERS = 65536
@@ -99,6 +101,8 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     lib.mfcfd_profile_iteration.argtypes = [P, C.c_int, D]
     lib.mfcfd_run_noalloc.argtypes = [P, C.c_int, C.c_int, D, I]
     lib.mfcfd_adjoint.argtypes = [P, C.c_int, C.c_int, C.c_size_t, D, D, D, I]
+    lib.mfcfd_adjoint_many.argtypes = [C.c_int, C.POINTER(P), C.c_int, C.c_int, C.c_size_t, D,
+                                       C.POINTER(D), C.POINTER(D), I, I]
     lib.mfcfd_tangent.argtypes = [P, C.c_int, C.c_int, D, D, D, D]
     lib.mfcfd_output_fields.argtypes = [P, D, D, D, D]
     lib.mfcfd_objective.argtypes = [P, C.c_int, D]

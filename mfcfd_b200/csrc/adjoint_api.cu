@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <thread>
 #include <vector>
 
 #include "adjoint.h"
@@ -346,19 +347,23 @@ void lskum_host::free_adjoint(mfcfd_t *h) {
     h->adj = nullptr;
 }
 
-extern "C" int mfcfd_adjoint(mfcfd_t *h, int objective, int n_iters, size_t ckpt_bytes,
-                             double *J, double *dJdx, double *dJdy, int *n_forward) {
-    if (!h || n_iters < 1 || objective < MFCFD_OBJ_CL || objective > MFCFD_OBJ_STAGNATION ||
-        !dJdx || !dJdy)
-        return MFCFD_ERR_ARG;
+namespace {
+
+bool adjoint_args_ok(const mfcfd_t *h, int objective, int n_iters) {
+    return h && n_iters >= 1 && objective >= MFCFD_OBJ_CL && objective <= MFCFD_OBJ_STAGNATION;
+}
+
+// Allocation half of mfcfd_adjoint: the tape, the transposed stencil, the
+// residue history and the snapshot pool (within ckpt_bytes, the initial state
+// counting); returns the number of snapshot rows in *nsnap.
+int adjoint_prepare(mfcfd_t *h, int objective, int n_iters, size_t ckpt_bytes, int *nsnap) {
     if (h->fp32) return fail(h, MFCFD_ERR_ARG, "mfcfd_adjoint: FP64 handles only");
     if (h->p.power != 0.0)
         return fail(h, MFCFD_ERR_ARG, "mfcfd_adjoint: LSQ weights with power != 0 are not differentiated");
     int st = adj_setup(h);
     if (st) return st;
     AdjointState *a = h->adj;
-    const int n = h->n;
-    const size_t row = sizeof(R4) * (size_t)n;
+    const size_t row = sizeof(R4) * (size_t)h->n;
     a->n_iters = n_iters;
     a->objective = objective;
     a->forward_iters = 0;
@@ -368,14 +373,23 @@ extern "C" int mfcfd_adjoint(mfcfd_t *h, int objective, int n_iters, size_t ckpt
         CK(dmalloc(&a->hist, (size_t)n_iters));
         a->hist_cap = n_iters;
     }
-    // snapshot pool within the byte budget (the initial state counts)
     const long long want = ckpt_bytes > row ? (long long)(ckpt_bytes / row) - 1 : 0;
-    const int nsnap = (int)std::min<long long>(want, n_iters - 1);
-    while ((int)a->snaps.size() < nsnap + 1) {  // + one scratch row
+    *nsnap = (int)std::min<long long>(want, n_iters - 1);
+    while ((int)a->snaps.size() < *nsnap + 1) {  // + one scratch row
         R4 *p = nullptr;
-        CK(dmalloc(&p, (size_t)n));
+        CK(dmalloc(&p, (size_t)h->n));
         a->snaps.push_back(p);
     }
+    return MFCFD_OK;
+}
+
+// Run half: allocates no device memory (the objective values 2-4 excepted);
+// everything is ordered on the handle's stream.
+int adjoint_execute(mfcfd_t *h, int nsnap, double *J, double *dJdx, double *dJdy,
+                    int *n_forward) {
+    AdjointState *a = h->adj;
+    const int n = h->n;
+    const size_t row = sizeof(R4) * (size_t)n;
     std::vector<R4 *> free_slots(a->snaps.begin(), a->snaps.begin() + nsnap);
     R4 *scratch = a->snaps[nsnap];
     CK(cudaStreamSynchronize(h->stream));
@@ -384,7 +398,7 @@ extern "C" int mfcfd_adjoint(mfcfd_t *h, int objective, int n_iters, size_t ckpt
     CK(cudaMemsetAsync(a->yb, 0, sizeof(double) * n, h->stream));
     CK(cudaMemsetAsync(a->nxb, 0, sizeof(double) * n, h->stream));
     CK(cudaMemsetAsync(a->nyb, 0, sizeof(double) * n, h->stream));
-    st = reverse_range(h, a, 0, n_iters, a->snap0, free_slots, scratch);
+    int st = reverse_range(h, a, 0, a->n_iters, a->snap0, free_slots, scratch);
     if (st) return st;
     launch_normals_b(a->nbnd, a->d_bleft, a->d_bright, h->d_xy, a->nxb, a->nyb, a->xb, a->yb,
                      h->stream);
@@ -401,7 +415,60 @@ extern "C" int mfcfd_adjoint(mfcfd_t *h, int objective, int n_iters, size_t ckpt
         dJdx[h->perm[p]] = xb[p];
         dJdy[h->perm[p]] = yb[p];
     }
-    if (J && (st = lskum_host::objective_value(h, objective, h->d_prim[h->cur], J))) return st;
+    if (J && (st = lskum_host::objective_value(h, a->objective, h->d_prim[h->cur], J)))
+        return st;
     if (n_forward) *n_forward = (int)a->forward_iters;
     return MFCFD_OK;
+}
+
+}  // namespace
+
+extern "C" int mfcfd_adjoint(mfcfd_t *h, int objective, int n_iters, size_t ckpt_bytes,
+                             double *J, double *dJdx, double *dJdy, int *n_forward) {
+    if (!adjoint_args_ok(h, objective, n_iters) || !dJdx || !dJdy) return MFCFD_ERR_ARG;
+    int nsnap = 0;
+    int st = adjoint_prepare(h, objective, n_iters, ckpt_bytes, &nsnap);
+    if (st) return st;
+    return adjoint_execute(h, nsnap, J, dJdx, dJdy, n_forward);
+}
+
+extern "C" int mfcfd_adjoint_many(int n_handles, mfcfd_t *const *handles, int objective,
+                                  int n_iters, size_t ckpt_bytes, double *J,
+                                  double *const *dJdx, double *const *dJdy, int *n_forward,
+                                  int *status) {
+    if (n_handles < 1 || n_handles > MFCFD_ADJOINT_MANY_MAX || !handles || !dJdx || !dJdy)
+        return MFCFD_ERR_ARG;
+    for (int i = 0; i < n_handles; ++i) {
+        if (!adjoint_args_ok(handles[i], objective, n_iters) || !dJdx[i] || !dJdy[i])
+            return MFCFD_ERR_ARG;
+        for (int j = 0; j < i; ++j)
+            if (handles[j] == handles[i] || handles[j]->stream == handles[i]->stream)
+                return fail(handles[i], MFCFD_ERR_ARG,
+                            "mfcfd_adjoint_many: handles must be distinct, on distinct streams");
+    }
+    std::vector<int> st(n_handles, MFCFD_OK), nsnap(n_handles, 0);
+    // every allocation first, one handle after the other
+    for (int i = 0; i < n_handles; ++i) {
+        st[i] = adjoint_prepare(handles[i], objective, n_iters, ckpt_bytes, &nsnap[i]);
+        if (st[i]) {
+            if (status)
+                for (int k = 0; k < n_handles; ++k) status[k] = k == i ? st[i] : MFCFD_OK;
+            return st[i];
+        }
+    }
+    // then one host thread per handle, each enqueueing on its own stream
+    std::vector<std::thread> pool;
+    pool.reserve(n_handles);
+    for (int i = 0; i < n_handles; ++i)
+        pool.emplace_back([&, i] {
+            st[i] = adjoint_execute(handles[i], nsnap[i], J ? J + i : nullptr, dJdx[i], dJdy[i],
+                                    n_forward ? n_forward + i : nullptr);
+        });
+    for (auto &t : pool) t.join();
+    int first = MFCFD_OK;
+    for (int i = 0; i < n_handles; ++i) {
+        if (status) status[i] = st[i];
+        if (!first && st[i]) first = st[i];
+    }
+    return first;
 }

@@ -205,3 +205,33 @@ class Solver:
         v = [C.c_int() for _ in range(4)]
         _lib.check(self.lib.mfcfd_info(self.h, *[C.byref(x) for x in v]), self.h, "mfcfd_info")
         return tuple(x.value for x in v)
+
+
+def adjoint_many(solvers, n_iters: int, objective: str = "cd", ckpt_bytes: int = 2 << 30):
+    """``Solver.adjoint`` of many independent solvers in one call
+    (``mfcfd_adjoint_many``): their reverse sweeps run side by side, each on
+    its solver's own stream.  Returns one (J, dJdx, dJdy, forward iterations)
+    per solver, each equal to what ``Solver.adjoint`` gives on it."""
+    solvers = list(solvers)
+    n = len(solvers)
+    if n == 0:
+        return []
+    lib = solvers[0].lib
+    handles = (C.c_void_p * n)(*[s.h for s in solvers])
+    dx = [np.zeros(s.n) for s in solvers]
+    dy = [np.zeros(s.n) for s in solvers]
+    px = (C.POINTER(C.c_double) * n)(*[_dptr(a) for a in dx])
+    py = (C.POINTER(C.c_double) * n)(*[_dptr(a) for a in dy])
+    J = np.zeros(n)
+    nf = np.zeros(n, dtype=np.int32)
+    st = np.zeros(n, dtype=np.int32)
+    ip = C.POINTER(C.c_int)
+    rc = lib.mfcfd_adjoint_many(n, handles, _lib.OBJECTIVES[objective.lower()], int(n_iters),
+                                int(ckpt_bytes), _dptr(J), px, py, nf.ctypes.data_as(ip),
+                                st.ctypes.data_as(ip))
+    if rc != _lib.MFCFD_OK:
+        bad = [k for k in range(n) if st[k] != _lib.MFCFD_OK] or [0]
+        _lib.check(rc, solvers[bad[0]].h, f"mfcfd_adjoint_many (solver {bad[0]})")
+    for s in solvers:
+        s.it = (s.it or 0) + n_iters
+    return [(float(J[k]), dx[k], dy[k], int(nf[k])) for k in range(n)]
