@@ -192,7 +192,7 @@ flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, int la
         nx = nn.x;
         ny = nn.y;
         const float nxf = (float)nx, nyf = (float)ny;
-        const float gm1 = (float)c.gm1, pif = (float)c.pi;
+        const float inv_gm1 = (float)(1.0 / c.gm1), inv_sqrt_pi = (float)(1.0 / sqrt(c.pi));
         const float s2q = kind == KIND_WALL ? -1.0f : 1.0f;
         for (int r = lane; r < nb; r += LPP) {
             const int k = g.conn[r * g.n + i];
@@ -205,10 +205,8 @@ flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, int la
                 float dxk[4], dyk[4], qmaxk[4], qmink[4];
                 ldf8(b.dq + 8 * (size_t)k, dxk, dyk);
                 ldf8(b.qm + 8 * (size_t)k, qmaxk, qmink);
-                float u1, u2, rho, pr;
-                reconstruct<float>(qk, dxk, dyk, qmaxk, qmink, b.eps2f[k], dxf, dyf, gm1, u1, u2,
-                                   rho, pr);
-                sk = kstate<float>(u1, u2, rho, pr, nxf, nyf, pif);
+                sk = reconstruct_kstate<float>(qk, dxk, dyk, qmaxk, qmink, b.eps2f[k], dxf, dyf,
+                                               inv_gm1, nxf, nyf, inv_sqrt_pi);
             }
             {
                 const float4 qv = __ldg(b.q_in + i);
@@ -216,10 +214,8 @@ flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, int la
                 float dxi[4], dyi[4], qmaxi[4], qmini[4];
                 ldf8(b.dq + 8 * (size_t)i, dxi, dyi);
                 ldf8(b.qm + 8 * (size_t)i, qmaxi, qmini);
-                float u1, u2, rho, pr;
-                reconstruct<float>(qi, dxi, dyi, qmaxi, qmini, b.eps2f[i], dxf, dyf, gm1, u1, u2,
-                                   rho, pr);
-                si = kstate<float>(u1, u2, rho, pr, nxf, nyf, pif);
+                si = reconstruct_kstate<float>(qi, dxi, dyi, qmaxi, qmini, b.eps2f[i], dxf, dyf,
+                                               inv_gm1, nxf, nyf, inv_sqrt_pi);
             }
             const float dels = dxf * nyf - dyf * nxf;
             const float deln = dxf * nxf + dyf * nyf;

@@ -187,8 +187,8 @@ kb_inner(Geom g, Consts c, Sched s, const R4 *__restrict__ q, const double *__re
 //
 // Eight lanes share one point; lane l takes stencil slots l, l+8, l+16.  For
 // its neighbour k a lane reconstructs both states once (limiter + qtilde ->
-// primitive; the reference repeats this per direction list with identical
-// inputs, so sharing it is exact), evaluates the split fluxes of every list
+// kinetic state, reconstruct_kstate; the reference repeats this per direction
+// list with identical inputs, so sharing it is exact), evaluates the split fluxes of every list
 // the neighbour belongs to, and stores G_k - G_i with the geometry in shared
 // memory.  Then lane pair (2L, 2L+1) sums list L in slot order -- the
 // reference's loop order -- for components (0,1) and (2,3), and lane 0
@@ -202,6 +202,7 @@ flux_tile(const Geom &g, const Consts &c, const StageBufs &b, int rk, int last, 
           bool valid, int kind0, int orow, int part, double *sm, double *sres) {
     const int grp = threadIdx.x / LPP, lane = threadIdx.x % LPP;
     double *rec = sm + (size_t)grp * g.kp * REC;
+    const double inv_gm1 = 1.0 / c.gm1, inv_sqrt_pi = 1.0 / sqrt(c.pi);
 
     int nb = 0, kind = KIND_INTERIOR;
     unsigned long long mx = 0, my = 0;
@@ -232,10 +233,8 @@ flux_tile(const Geom &g, const Consts &c, const StageBufs &b, int rk, int last, 
                 double dxk[4], dyk[4], qmaxk[4], qmink[4];
                 ld8(b.dq + 8 * (size_t)k, dxk, dyk);
                 ld8(b.qm + 8 * (size_t)k, qmaxk, qmink);
-                double u1, u2, rho, pr;
-                reconstruct(qk, dxk, dyk, qmaxk, qmink, g.eps2[k], delx, dely, c.gm1, u1, u2, rho,
-                            pr);
-                sk = kstate(u1, u2, rho, pr, nx, ny, c.pi);
+                sk = reconstruct_kstate(qk, dxk, dyk, qmaxk, qmink, g.eps2[k], delx, dely,
+                                        inv_gm1, nx, ny, inv_sqrt_pi);
             }
             {
                 const R4 qv = ld4(b.q_in + i);
@@ -243,10 +242,8 @@ flux_tile(const Geom &g, const Consts &c, const StageBufs &b, int rk, int last, 
                 double dxi[4], dyi[4], qmaxi[4], qmini[4];
                 ld8(b.dq + 8 * (size_t)i, dxi, dyi);
                 ld8(b.qm + 8 * (size_t)i, qmaxi, qmini);
-                double u1, u2, rho, pr;
-                reconstruct(qi, dxi, dyi, qmaxi, qmini, g.eps2[i], delx, dely, c.gm1, u1, u2, rho,
-                            pr);
-                si = kstate(u1, u2, rho, pr, nx, ny, c.pi);
+                si = reconstruct_kstate(qi, dxi, dyi, qmaxi, qmini, g.eps2[i], delx, dely,
+                                        inv_gm1, nx, ny, inv_sqrt_pi);
             }
             const double tx = ny, ty = -nx;
             const double dels = delx * tx + dely * ty;
