@@ -191,15 +191,16 @@ kb_inner(Geom g, Consts c, Sched s, const R4 *__restrict__ q, const double *__re
 // list with identical inputs, so sharing it is exact), evaluates the split fluxes of every list
 // the neighbour belongs to, and stores G_k - G_i with the geometry in shared
 // memory.  Then lane pair (2L, 2L+1) sums list L in slot order -- the
-// reference's loop order -- for components (0,1) and (2,3), and lane 0
-// gathers the four list derivatives and updates the state.
+// reference's loop order -- for components (0,1) and (2,3) and leaves the
+// list derivatives in sG[16 grp + 4L + m]; update_point then runs once per
+// point on the first GROUPS threads of the block (one warp), so that the
+// update's serial chain does not hold four warps at one lane in eight.
 //
 // One call handles one tile of GROUPS points; point i of this thread's group
-// is valid or padding, kind0 is its kind, orow its row in g.obc (outer
-// points) and part the slot of the tile's res_sqr partial.
+// is valid or padding and kind0 is its kind.
 __device__ __forceinline__ void
-flux_tile(const Geom &g, const Consts &c, const StageBufs &b, int rk, int last, int i,
-          bool valid, int kind0, int orow, int part, double *sm, double *sres) {
+flux_tile(const Geom &g, const Consts &c, const StageBufs &b, int i, bool valid, int kind0,
+          double *sm, double *sG) {
     const int grp = threadIdx.x / LPP, lane = threadIdx.x % LPP;
     double *rec = sm + (size_t)grp * g.kp * REC;
     const double inv_gm1 = 1.0 / c.gm1, inv_sqrt_pi = 1.0 / sqrt(c.pi);
@@ -313,18 +314,25 @@ flux_tile(const Geom &g, const Consts &c, const StageBufs &b, int rk, int last, 
             }
         }
     }
+    // lane 2L+h holds G[L][2h], G[L][2h+1]
+    sG[grp * 16 + 2 * lane] = Gv0;
+    sG[grp * 16 + 2 * lane + 1] = Gv1;
+}
+
+// state_update.F90:10-141 of one point from its four list derivatives
+// Gs[4L+m]; returns its res_sqr term.
+__device__ __forceinline__ double
+update_point(const Geom &g, const Consts &c, const StageBufs &b, int rk, int last, int i,
+             int kind, int orow, const double *Gs) {
     double G[4][4];
 #pragma unroll
-    for (int L = 0; L < 4; ++L) {
+    for (int L = 0; L < 4; ++L)
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            G[L][2 * h] = __shfl_sync(0xffffffffu, Gv0, 2 * L + h, LPP);
-            G[L][2 * h + 1] = __shfl_sync(0xffffffffu, Gv1, 2 * L + h, LPP);
-        }
-    }
-
+        for (int m = 0; m < 4; ++m) G[L][m] = Gs[4 * L + m];
+    const double2 nn = g.nrm[i];
+    const double nx = nn.x, ny = nn.y;
     double res_sqr = 0.0;
-    if (valid && lane == 0) {
+    {
         const double delta = b.delta[i];
         double fr[4];
 #pragma unroll
@@ -372,15 +380,7 @@ flux_tile(const Geom &g, const Consts &c, const StageBufs &b, int rk, int last, 
         st4(b.q_out + i, qn[0], qn[1], qn[2], qn[3]);
         if (last) b.spd[i] = sqrt(u1 * u1 + u2 * u2) + 3.0 * sqrt(pr / rho);
     }
-    if (last) {
-        if (lane == 0) sres[grp] = res_sqr;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double s = 0.0;
-            for (int q = 0; q < GROUPS; ++q) s = s + sres[q];
-            b.res_part[part] = s;
-        }
-    }
+    return res_sqr;
 }
 
 // F pass: each block walks the scheduled tiles with a stride of the grid.  A
@@ -391,6 +391,7 @@ __global__ void __launch_bounds__(FLUX_BLOCK, FLUX_MIN_BLOCKS)
 kb_flux(Geom g, Consts c, Sched s, StageBufs b, int rk, int last) {
     extern __shared__ double sm[];
     __shared__ double sres[GROUPS];
+    __shared__ double sG[GROUPS * 16];
     __shared__ SchedSmem ss;
     load_sched(s, ss);
     const int total = ss.pre[ss.nact];
@@ -398,9 +399,28 @@ kb_flux(Geom g, Consts c, Sched s, StageBufs b, int rk, int last) {
         const TileRef t = sched_tile(s, ss, v);
         const int j = t.j0 + threadIdx.x / LPP;
         const int kind = j < t.nw ? KIND_WALL : (j < t.nw + t.no ? KIND_OUTER : KIND_INTERIOR);
-        flux_tile(g, c, b, rk, last, t.base + j, j < t.n, kind, t.obc_off + j - t.nw, t.tile,
-                  sm, sres);
-        __syncthreads();  // the next tile reuses sm and sres
+        flux_tile(g, c, b, t.base + j, j < t.n, kind, sm, sG);
+        __syncthreads();
+        if (threadIdx.x < GROUPS) {
+            const int jj = t.j0 + threadIdx.x;
+            double rs = 0.0;
+            if (jj < t.n) {
+                const int kk =
+                    jj < t.nw ? KIND_WALL : (jj < t.nw + t.no ? KIND_OUTER : KIND_INTERIOR);
+                rs = update_point(g, c, b, rk, last, t.base + jj, kk, t.obc_off + jj - t.nw,
+                                  sG + 16 * threadIdx.x);
+            }
+            if (last) {
+                sres[threadIdx.x] = rs;
+                __syncwarp(0xffffu);
+                if (threadIdx.x == 0) {
+                    double acc = 0.0;
+                    for (int q = 0; q < GROUPS; ++q) acc = acc + sres[q];
+                    b.res_part[t.tile] = acc;
+                }
+            }
+        }
+        __syncthreads();  // the next tile reuses sm, sG and sres
     }
 }
 
