@@ -124,9 +124,10 @@ int mfcfd_adjoint(mfcfd_t *h, int objective, int n_iters, size_t ckpt_bytes, dou
 /* mfcfd_adjoint of n_handles independent solvers (grids of any sizes) in one
  * call: the adjoint a batch of cases needs, the reference running one case
  * per process.  Each handle's buffers and snapshot pool (ckpt_bytes each) are
- * allocated first, one handle after the other; then each handle's reverse
- * sweep is enqueued by a host thread of its own on the handle's own stream,
- * so that the sweeps of small grids run side by side on the GPU.  Results
+ * allocated first, one handle after the other; then the reverse sweeps run,
+ * each on its handle's own stream: handles of 65,536 points or more one
+ * after another on one host thread (each fills the GPU alone), every
+ * smaller handle on a host thread of its own, side by side with them.  Results
  * per handle are those of mfcfd_adjoint on it (bit for bit): J[i] (J may be
  * NULL), dJdx[i], dJdy[i] (caller order), n_forward[i] (may be NULL),
  * status[i] (may be NULL; MFCFD_OK or that handle's error).  Handles must be

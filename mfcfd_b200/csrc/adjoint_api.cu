@@ -432,6 +432,9 @@ extern "C" int mfcfd_adjoint(mfcfd_t *h, int objective, int n_iters, size_t ckpt
     return adjoint_execute(h, nsnap, J, dJdx, dJdy, n_forward);
 }
 
+// Handles at least this large run their sweeps in sequence (see below).
+constexpr int ADJ_OVERLAP_POINTS = 65536;
+
 extern "C" int mfcfd_adjoint_many(int n_handles, mfcfd_t *const *handles, int objective,
                                   int n_iters, size_t ckpt_bytes, double *J,
                                   double *const *dJdx, double *const *dJdy, int *n_forward,
@@ -456,13 +459,25 @@ extern "C" int mfcfd_adjoint_many(int n_handles, mfcfd_t *const *handles, int ob
             return st[i];
         }
     }
-    // then one host thread per handle, each enqueueing on its own stream
+    // then the sweeps: a handle of ADJ_OVERLAP_POINTS points or more fills the
+    // GPU on its own (its flux launches are several waves deep), so those run
+    // one after another on one host thread; each smaller handle gets a thread
+    // of its own, and its latency-bound sweep overlaps that chain on its own
+    // stream.  Running all large sweeps at once only made them contend.
+    auto run = [&](int i) {
+        st[i] = adjoint_execute(handles[i], nsnap[i], J ? J + i : nullptr, dJdx[i], dJdy[i],
+                                n_forward ? n_forward + i : nullptr);
+    };
+    std::vector<int> large;
     std::vector<std::thread> pool;
     pool.reserve(n_handles);
-    for (int i = 0; i < n_handles; ++i)
-        pool.emplace_back([&, i] {
-            st[i] = adjoint_execute(handles[i], nsnap[i], J ? J + i : nullptr, dJdx[i], dJdy[i],
-                                    n_forward ? n_forward + i : nullptr);
+    for (int i = 0; i < n_handles; ++i) {
+        if (handles[i]->n >= ADJ_OVERLAP_POINTS) large.push_back(i);
+        else pool.emplace_back(run, i);
+    }
+    if (!large.empty())
+        pool.emplace_back([&] {
+            for (int i : large) run(i);
         });
     for (auto &t : pool) t.join();
     int first = MFCFD_OK;

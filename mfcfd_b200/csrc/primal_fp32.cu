@@ -172,11 +172,12 @@ __device__ __forceinline__ void kahan_add(float &s, float &cmp, float v) {
 }
 
 // cal_flux_residual + state_update + eval_q_variables of the new state, with
-// the per-neighbour work in FP32 (same lane layout as the FP64 kernel).
+// the per-neighbour work in FP32 (same lane layout as the FP64 kernel; the
+// list derivatives go to sG and update32_point runs on one warp per tile).
 // One call handles one tile of GROUPS points (arguments as in the FP64 pass).
 __device__ __forceinline__ void
-flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, int last, int i,
-            bool valid, int kind0, int orow, int part, double *sm, double *sres) {
+flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool valid,
+            int kind0, double *sm, double *sG) {
     const int grp = threadIdx.x / LPP, lane = threadIdx.x % LPP;
     double *rec = sm + (size_t)grp * g.kp * FREC;
 
@@ -281,18 +282,25 @@ flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, int la
             }
         }
     }
+    // lane 2L+h holds G[L][2h], G[L][2h+1]
+    sG[grp * 16 + 2 * lane] = Gv0;
+    sG[grp * 16 + 2 * lane + 1] = Gv1;
+}
+
+// state_update.F90:10-141 of one point from its four list derivatives
+// Gs[4L+m], in FP32; returns its res_sqr term (FP64).
+__device__ __forceinline__ double
+update32_point(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, int last, int i,
+               int kind, int orow, const double *Gs) {
     double G[4][4];
 #pragma unroll
-    for (int L = 0; L < 4; ++L) {
+    for (int L = 0; L < 4; ++L)
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            G[L][2 * h] = __shfl_sync(0xffffffffu, Gv0, 2 * L + h, LPP);
-            G[L][2 * h + 1] = __shfl_sync(0xffffffffu, Gv1, 2 * L + h, LPP);
-        }
-    }
-
+        for (int m = 0; m < 4; ++m) G[L][m] = Gs[4 * L + m];
+    const double2 nn = g.nrm[i];
+    const double nx = nn.x, ny = nn.y;
     double res_sqr = 0.0;
-    if (valid && lane == 0) {
+    {
         const double delta = b.delta[i];
         double fr[4];
 #pragma unroll
@@ -347,21 +355,14 @@ flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, int la
         b.q_out[i] = make_float4(qn[0], qn[1], qn[2], qn[3]);
         if (last) b.spd[i] = (double)(sqrtf(u1 * u1 + u2 * u2) + 3.0f * sqrtf(pr / rho));
     }
-    if (last) {
-        if (lane == 0) sres[grp] = res_sqr;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double s = 0.0;
-            for (int q = 0; q < GROUPS; ++q) s = s + sres[q];
-            b.res_part[part] = s;
-        }
-    }
+    return res_sqr;
 }
 
 __global__ void __launch_bounds__(FLUX_BLOCK, FLUX32_MIN_BLOCKS)
 kb_flux32(Geom g, Consts c, Sched s, StageBufs32 b, int rk, int last) {
     extern __shared__ double sm[];
     __shared__ double sres[GROUPS];
+    __shared__ double sG[GROUPS * 16];
     __shared__ SchedSmem ss;
     load_sched(s, ss);
     const int total = ss.pre[ss.nact];
@@ -369,9 +370,28 @@ kb_flux32(Geom g, Consts c, Sched s, StageBufs32 b, int rk, int last) {
         const TileRef t = sched_tile(s, ss, v);
         const int j = t.j0 + threadIdx.x / LPP;
         const int kind = j < t.nw ? KIND_WALL : (j < t.nw + t.no ? KIND_OUTER : KIND_INTERIOR);
-        flux32_tile(g, c, b, rk, last, t.base + j, j < t.n, kind, t.obc_off + j - t.nw, t.tile,
-                    sm, sres);
-        __syncthreads();  // the next tile reuses sm and sres
+        flux32_tile(g, c, b, t.base + j, j < t.n, kind, sm, sG);
+        __syncthreads();
+        if (threadIdx.x < GROUPS) {
+            const int jj = t.j0 + threadIdx.x;
+            double rs = 0.0;
+            if (jj < t.n) {
+                const int kk =
+                    jj < t.nw ? KIND_WALL : (jj < t.nw + t.no ? KIND_OUTER : KIND_INTERIOR);
+                rs = update32_point(g, c, b, rk, last, t.base + jj, kk, t.obc_off + jj - t.nw,
+                                    sG + 16 * threadIdx.x);
+            }
+            if (last) {
+                sres[threadIdx.x] = rs;
+                __syncwarp(0xffffu);
+                if (threadIdx.x == 0) {
+                    double acc = 0.0;
+                    for (int q = 0; q < GROUPS; ++q) acc = acc + sres[q];
+                    b.res_part[t.tile] = acc;
+                }
+            }
+        }
+        __syncthreads();  // the next tile reuses sm, sG and sres
     }
 }
 
