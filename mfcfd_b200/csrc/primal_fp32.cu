@@ -225,24 +225,30 @@ flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool va
             float *ef = reinterpret_cast<float *>(e);
             float Gi[4], Gk[4];
 #pragma unroll
-            for (int L = 0; L < 4; ++L) {
-                const unsigned long long bits = (L < 2) ? mx : my;
-                if (!((bits >> (r + ((L & 1) ? 32 : 0))) & 1ull)) continue;
-                const float sg = (L & 1) ? -1.0f : 1.0f;
-                if (L < 2) {
-                    if (kind == KIND_INTERIOR) {
-                        flux_gx<float>(si, sg, Gi);
-                        flux_gx<float>(sk, sg, Gk);
-                    } else {
-                        flux_quad<float>(si, sg, s2q, Gi);
-                        flux_quad<float>(sk, sg, s2q, Gk);
-                    }
-                } else {
-                    flux_gy<float>(si, sg, Gi);
-                    flux_gy<float>(sk, sg, Gk);
-                }
+            for (int d = 0; d < 2; ++d) {
+                // one converged evaluation per direction, as in the FP64 pass
+                const unsigned long long bits = d == 0 ? mx : my;
+                const bool in0 = (bits >> r) & 1ull, in1 = (bits >> (r + 32)) & 1ull;
 #pragma unroll
-                for (int m = 0; m < 4; ++m) ef[4 * L + m] = Gk[m] - Gi[m];
+                for (int pass = 0; pass < 2; ++pass) {
+                    if (pass == 0 ? !(in0 || in1) : !(in0 && in1)) continue;
+                    const int L = 2 * d + ((pass == 1 || !in0) ? 1 : 0);
+                    const float sg = (L & 1) ? -1.0f : 1.0f;
+                    if (d == 0) {
+                        if (kind == KIND_INTERIOR) {
+                            flux_gx<float>(si, sg, Gi);
+                            flux_gx<float>(sk, sg, Gk);
+                        } else {
+                            flux_quad<float>(si, sg, s2q, Gi);
+                            flux_quad<float>(sk, sg, s2q, Gk);
+                        }
+                    } else {
+                        flux_gy<float>(si, sg, Gi);
+                        flux_gy<float>(sk, sg, Gk);
+                    }
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) ef[4 * L + m] = Gk[m] - Gi[m];
+                }
             }
             ef[16] = dels * w;
             ef[17] = deln * w;

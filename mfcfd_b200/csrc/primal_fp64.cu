@@ -252,26 +252,37 @@ flux_tile(const Geom &g, const Consts &c, const StageBufs &b, int i, bool valid,
             double w = 1.0;
             if (!c.power_zero) w = pow(sqrt(dels * dels + deln * deln), c.power);
             double *e = rec + r * REC;
+            // Per direction the neighbour is in one list of the pair (in both
+            // only when its projection is exactly 0): one evaluation with the
+            // list's sign taken per lane keeps the warp converged where
+            // neighbours fall in different lists of the pair.
             double Gi[4], Gk[4];
 #pragma unroll
-            for (int L = 0; L < 4; ++L) {
-                const unsigned long long bits = (L < 2) ? mx : my;
-                if (!((bits >> (r + ((L & 1) ? 32 : 0))) & 1ull)) continue;
-                const double sg = (L & 1) ? -1.0 : 1.0;
-                if (L < 2) {
-                    if (kind == KIND_INTERIOR) {
-                        flux_gx(si, sg, Gi);
-                        flux_gx(sk, sg, Gk);
-                    } else {
-                        flux_quad(si, sg, s2q, Gi);
-                        flux_quad(sk, sg, s2q, Gk);
-                    }
-                } else {
-                    flux_gy(si, sg, Gi);
-                    flux_gy(sk, sg, Gk);
-                }
+            for (int d = 0; d < 2; ++d) {
+                const unsigned long long bits = d == 0 ? mx : my;
+                const bool in0 = (bits >> r) & 1ull, in1 = (bits >> (r + 32)) & 1ull;
 #pragma unroll
-                for (int m = 0; m < 4; ++m) e[4 * L + m] = Gk[m] - Gi[m];
+                for (int pass = 0; pass < 2; ++pass) {
+                    // pass 0: the first list holding the neighbour; pass 1:
+                    // the second list of a neighbour in both
+                    if (pass == 0 ? !(in0 || in1) : !(in0 && in1)) continue;
+                    const int L = 2 * d + ((pass == 1 || !in0) ? 1 : 0);
+                    const double sg = (L & 1) ? -1.0 : 1.0;
+                    if (d == 0) {
+                        if (kind == KIND_INTERIOR) {
+                            flux_gx(si, sg, Gi);
+                            flux_gx(sk, sg, Gk);
+                        } else {
+                            flux_quad(si, sg, s2q, Gi);
+                            flux_quad(sk, sg, s2q, Gk);
+                        }
+                    } else {
+                        flux_gy(si, sg, Gi);
+                        flux_gy(sk, sg, Gk);
+                    }
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) e[4 * L + m] = Gk[m] - Gi[m];
+                }
             }
             e[16] = dels;
             e[17] = deln;
