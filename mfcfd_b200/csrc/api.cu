@@ -67,7 +67,7 @@ void free_all(mfcfd_t *h) {
                     h->d_dq[1], h->d_qm, h->d_delta, h->d_spd, h->d_res_part, h->d_flux_dbg,
                     h->d_hist, h->d_forces, h->d_ctl, h->d_sh_idx, h->d_sh_shape, h->d_sh_geo,
                     h->d_sh_my, h->f_prim[0], h->f_prim[1], h->f_q[0], h->f_q[1],
-                    h->f_dq[0], h->f_dq[1], h->f_qm, h->f_eps2, h->f_dxy, h->f_w, h->f_lsq,
+                    h->f_dq[0], h->f_dq[1], h->f_dq[2], h->f_qm, h->f_eps2, h->f_dxy, h->f_w, h->f_lsq,
                     h->f_flsq, h->d_inst, h->d_sched,
                     h->d_run};
     for (void *b : bufs)
@@ -146,8 +146,9 @@ void launch_stage(mfcfd_t *h, cudaStream_t s, int rk, int A, int B, F after) {
                       h->f_qm, h->d_delta, rk == 1, h->point_block, h->point_grid, s);
         after();
         for (int t = 1; t <= m; ++t) {
-            launch_inner32(h->geom, h->consts, h->geom32, h->sched, q_in, h->f_dq[(t - 1) & 1],
-                           h->f_dq[t & 1], h->point_block, h->point_grid, s);
+            launch_inner32(h->geom, h->consts, h->geom32, h->sched, h->f_dq[0],
+                           h->f_dq[dq32_src(t)], h->f_dq[dq32_dst(t)], h->point_block,
+                           h->point_grid, s);
             after();
         }
         StageBufs32 b;
@@ -156,7 +157,7 @@ void launch_stage(mfcfd_t *h, cudaStream_t s, int rk, int A, int B, F after) {
         b.prim_old = h->f_prim[A];
         b.q_in = q_in;
         b.q_out = h->f_q[h->qcur ^ 1];
-        b.dq = h->f_dq[m & 1];
+        b.dq = h->f_dq[dq32_final(m)];
         b.qm = h->f_qm;
         b.eps2f = h->f_eps2;
         b.delta = h->d_delta;
@@ -641,8 +642,8 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
         for (int b = 0; b < 2; ++b) {
             ALLOC(h->f_prim[b], n);
             ALLOC(h->f_q[b], n);
-            ALLOC(h->f_dq[b], (size_t)8 * n);
         }
+        for (int b = 0; b < 3; ++b) ALLOC(h->f_dq[b], (size_t)8 * n);
         ALLOC(h->f_qm, (size_t)8 * n);
         ALLOC(h->f_eps2, n);
         ALLOC(h->f_dxy, (size_t)kp * n);
@@ -928,7 +929,7 @@ int mfcfd_get_array(mfcfd_t *h, const char *name, double *out) {
     const float *fsrc = nullptr;
     if (h->fp32) {
         if (s == "q") { fsrc = reinterpret_cast<const float *>(h->f_q[h->qcur ^ 1]); w = 4; }
-        else if (s == "dq") { fsrc = h->f_dq[h->p.inner_iterations & 1]; w = 8; }
+        else if (s == "dq") { fsrc = h->f_dq[dq32_final(h->p.inner_iterations)]; w = 8; }
         else if (s == "qm") { fsrc = h->f_qm; w = 8; }
     }
     if (fsrc) {

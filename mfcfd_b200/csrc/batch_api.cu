@@ -65,7 +65,7 @@ struct mfcfd_batch {
     double *d_dq[2] = {nullptr, nullptr};
     double *d_qm = nullptr;
     float4 *f_prim[2] = {nullptr, nullptr}, *f_q[2] = {nullptr, nullptr};
-    float *f_dq[2] = {nullptr, nullptr};
+    float *f_dq[3] = {nullptr, nullptr, nullptr};
     float *f_qm = nullptr, *f_eps2 = nullptr;
     float2 *f_dxy = nullptr;
     float *f_w = nullptr;
@@ -135,7 +135,7 @@ void free_batch(mfcfd_batch_t *b) {
     void *bufs[] = {b->d_xy, b->d_nrm, b->d_eps2, b->d_obc, b->d_conn, b->d_nbhs, b->d_mx,
                     b->d_my, b->d_prim[0], b->d_prim[1], b->d_q[0], b->d_q[1], b->d_dq[0],
                     b->d_dq[1], b->d_qm, b->f_prim[0], b->f_prim[1], b->f_q[0], b->f_q[1],
-                    b->f_dq[0], b->f_dq[1], b->f_qm, b->f_eps2, b->f_dxy, b->f_w, b->f_lsq,
+                    b->f_dq[0], b->f_dq[1], b->f_dq[2], b->f_qm, b->f_eps2, b->f_dxy, b->f_w, b->f_lsq,
                     b->f_flsq, b->d_delta, b->d_spd,
                     b->d_res_part, b->d_hist, b->d_forces, b->d_inst, b->d_sched, b->d_run,
                     b->d_ctl, b->d_sh_idx, b->d_sh_shape, b->d_sh_geo, b->d_sh_my};
@@ -202,15 +202,15 @@ void batch_stage(mfcfd_batch_t *b, cudaStream_t s, int rk, int A, int B) {
         launch_grad32(b->geom, b->consts, b->geom32, b->sched, q_in, b->d_spd, b->f_dq[0],
                       b->f_qm, b->d_delta, rk == 1, pb, pg, s);
         for (int t = 1; t <= m; ++t)
-            launch_inner32(b->geom, b->consts, b->geom32, b->sched, q_in, b->f_dq[(t - 1) & 1],
-                           b->f_dq[t & 1], pb, pg, s);
+            launch_inner32(b->geom, b->consts, b->geom32, b->sched, b->f_dq[0],
+                           b->f_dq[dq32_src(t)], b->f_dq[dq32_dst(t)], pb, pg, s);
         StageBufs32 sb;
         sb.prim_in = rk == 1 ? b->f_prim[A] : b->f_prim[B];
         sb.prim_out = b->f_prim[B];
         sb.prim_old = b->f_prim[A];
         sb.q_in = q_in;
         sb.q_out = b->f_q[b->qcur ^ 1];
-        sb.dq = b->f_dq[m & 1];
+        sb.dq = b->f_dq[dq32_final(m)];
         sb.qm = b->f_qm;
         sb.eps2f = b->f_eps2;
         sb.delta = b->d_delta;
@@ -561,8 +561,8 @@ int mfcfd_batch_create(int n_inst, const mfcfd_grid *const *grids, const mfcfd_p
         for (int k = 0; k < 2; ++k) {
             BALLOC(b->f_prim[k], N);
             BALLOC(b->f_q[k], N);
-            BALLOC(b->f_dq[k], (size_t)8 * N);
         }
+        for (int k = 0; k < 3; ++k) BALLOC(b->f_dq[k], (size_t)8 * N);
         BALLOC(b->f_qm, (size_t)8 * N);
         BALLOC(b->f_eps2, N);
         BALLOC(b->f_dxy, (size_t)kp * N);

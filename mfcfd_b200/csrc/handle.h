@@ -42,7 +42,7 @@ struct mfcfd {
     // FP32-mixed state (precision == MFCFD_FP32_MIXED)
     bool fp32 = false;
     float4 *f_prim[2] = {nullptr, nullptr}, *f_q[2] = {nullptr, nullptr};
-    float *f_dq[2] = {nullptr, nullptr};
+    float *f_dq[3] = {nullptr, nullptr, nullptr};
     float *f_qm = nullptr, *f_eps2 = nullptr;
     float2 *f_dxy = nullptr;
     float *f_w = nullptr;

@@ -161,9 +161,17 @@ cudaError_t init_kernels32();
 void launch_grad32(const Geom &g, const Consts &c, const Geom32 &f, const Sched &s,
                    const float4 *q, const double *spd, float *dq, float *qm, double *delta,
                    bool with_delta, int block, int grid, cudaStream_t st);
+// dq0: the D pass's derivatives of the stage, kept through its inner
+// iterations (the FP32 buffers rotate as dq32_src / dq32_dst say)
 void launch_inner32(const Geom &g, const Consts &c, const Geom32 &f, const Sched &s,
-                    const float4 *q, const float *dq_in, float *dq_out, int block, int grid,
+                    const float *dq0, const float *dq_in, float *dq_out, int block, int grid,
                     cudaStream_t st);
+// FP32 dq buffers of a stage: 0 holds the D pass's result for the whole
+// stage; inner iteration t (1-based) reads dq32_src(t), writes dq32_dst(t);
+// the flux pass reads dq32_final(m).
+inline int dq32_src(int t) { return t == 1 ? 0 : 1 + ((t - 2) & 1); }
+inline int dq32_dst(int t) { return 1 + ((t - 1) & 1); }
+inline int dq32_final(int m) { return m == 0 ? 0 : dq32_dst(m); }
 void launch_flux32(const Geom &g, const Consts &c, const Sched &s, const StageBufs32 &b, int rk,
                    bool last, int grid, cudaStream_t st);
 void launch_init_state32(const Geom &g, const float4 *prim, float4 *q, double *spd,

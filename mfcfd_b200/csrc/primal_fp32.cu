@@ -113,45 +113,47 @@ kb_grad32(Geom g, Consts c, Geom32 f, Sched s, const float4 *__restrict__ q,
 }
 
 // eval_q_inner_loop + eval_update_innerloop (q_variables.F90:115-227) with
-// FP32 sums and the precomputed inverse normal matrix.
+// FP32 sums, rearranged.  The reference's new derivative is
+//   L sum_k w d (qt_k - qt_i),  qt = q - (d . dq)/2,  L = M^-1,  M = sum_k w d d^T
+// (d = x_k - x_i).  q is fixed within a stage, so it splits into
+//   dq0 + dq_i/2 - L sum_k w d (d . dq_k) / 2,
+// where dq0 = L sum_k w d (q_k - q_i) is the D pass's result of this stage
+// and L M = I turns the point's own term into dq_i/2.  Equal in exact
+// arithmetic; only the neighbours' derivatives are gathered (no q).
 __device__ __forceinline__ void
-inner32_point(const Geom &g, const Geom32 &f, const float4 *__restrict__ q,
+inner32_point(const Geom &g, const Geom32 &f, const float *__restrict__ dq0,
               const float *__restrict__ dq_in, float *__restrict__ dq_out, int i) {
-    const float4 qv = __ldg(q + i);
-    const float qi[4] = {qv.x, qv.y, qv.z, qv.w};
-    float dxi[4], dyi[4];
-    ldf8(dq_in + 8 * (size_t)i, dxi, dyi);
-    float sx[4] = {0.f, 0.f, 0.f, 0.f}, sy[4] = {0.f, 0.f, 0.f, 0.f};
+    float tx[4] = {0.f, 0.f, 0.f, 0.f}, ty[4] = {0.f, 0.f, 0.f, 0.f};
     const int nb = g.nbhs[i];
     for (int r = 0; r < nb; ++r) {
         const int k = g.conn[r * g.n + i];
         const float2 d = __ldg(f.dxy + r * g.n + i);
         const float w = f.w ? __ldg(f.w + r * g.n + i) : 1.0f;
-        const float4 kv = __ldg(q + k);
-        const float qk[4] = {kv.x, kv.y, kv.z, kv.w};
         float dxk[4], dyk[4];
         ldf8(dq_in + 8 * (size_t)k, dxk, dyk);
         const float wdx = w * d.x, wdy = w * d.y;
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-            const float temp1 = qi[m] - 0.5f * (d.x * dxi[m] + d.y * dyi[m]);
-            const float temp2 = qk[m] - 0.5f * (d.x * dxk[m] + d.y * dyk[m]);
-            sx[m] = sx[m] + wdx * (temp2 - temp1);
-            sy[m] = sy[m] + wdy * (temp2 - temp1);
+            const float pk = d.x * dxk[m] + d.y * dyk[m];
+            tx[m] = tx[m] + wdx * pk;
+            ty[m] = ty[m] + wdy * pk;
         }
     }
+    float dxi[4], dyi[4], dx0[4], dy0[4];
+    ldf8(dq_in + 8 * (size_t)i, dxi, dyi);
+    ldf8(dq0 + 8 * (size_t)i, dx0, dy0);
     const float4 L = __ldg(f.lsq + i);
     float dx[4], dy[4];
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
-        dx[m] = L.x * sx[m] + L.y * sy[m];
-        dy[m] = L.y * sx[m] + L.z * sy[m];
+        dx[m] = dx0[m] + 0.5f * dxi[m] - 0.5f * (L.x * tx[m] + L.y * ty[m]);
+        dy[m] = dy0[m] + 0.5f * dyi[m] - 0.5f * (L.y * tx[m] + L.z * ty[m]);
     }
     stf8(dq_out + 8 * (size_t)i, dx, dy);
 }
 
 __global__ void __launch_bounds__(GRAD_BLOCK)
-kb_inner32(Geom g, Geom32 f, Sched s, const float4 *__restrict__ q,
+kb_inner32(Geom g, Geom32 f, Sched s, const float *__restrict__ dq0,
            const float *__restrict__ dq_in, float *__restrict__ dq_out) {
     __shared__ SchedSmem ss;
     load_sched(s, ss);
@@ -159,7 +161,7 @@ kb_inner32(Geom g, Geom32 f, Sched s, const float4 *__restrict__ q,
     for (int vp = blockIdx.x * blockDim.x + threadIdx.x; vp < total;
          vp += gridDim.x * blockDim.x) {
         const int i = sched_point(s, ss, vp);
-        if (i >= 0) inner32_point(g, f, q, dq_in, dq_out, i);
+        if (i >= 0) inner32_point(g, f, dq0, dq_in, dq_out, i);
     }
 }
 
@@ -458,10 +460,10 @@ void launch_grad32(const Geom &g, const Consts &c, const Geom32 &f, const Sched 
 }
 
 void launch_inner32(const Geom &g, const Consts &c, const Geom32 &f, const Sched &s,
-                    const float4 *q, const float *dq_in, float *dq_out, int block, int grid,
+                    const float *dq0, const float *dq_in, float *dq_out, int block, int grid,
                     cudaStream_t st) {
     (void)c;
-    kb_inner32<<<wave32(1, block, 0, grid), block, 0, st>>>(g, f, s, q, dq_in, dq_out);
+    kb_inner32<<<wave32(1, block, 0, grid), block, 0, st>>>(g, f, s, dq0, dq_in, dq_out);
 }
 
 void launch_flux32(const Geom &g, const Consts &c, const Sched &s, const StageBufs32 &b,
