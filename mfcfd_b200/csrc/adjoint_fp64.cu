@@ -199,24 +199,31 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
             const KState si = kstate(e_[0], e_[1], e_[2], e_[3], nx, ny, c.pi);
             const KState sk = kstate(e_[4], e_[5], e_[6], e_[7], nx, ny, c.pi);
             double *e = rec + r * BREC;
-            for (int L = 0; L < 4; ++L) {
-                const unsigned long long bits = (L < 2) ? mx : my;
-                if (!((bits >> (r + ((L & 1) ? 32 : 0))) & 1ull)) continue;
-                const double sg = (L & 1) ? -1.0 : 1.0;
-                double Gi[4], Gk[4];
-                if (L < 2) {
-                    if (kind == KIND_INTERIOR) {
-                        flux_gx(si, sg, Gi);
-                        flux_gx(sk, sg, Gk);
+            // one converged evaluation per direction and list holding the
+            // neighbour (two only at a zero projection), lists in ascending
+            // order, as in the forward kb_flux
+            for (int d = 0; d < 2; ++d) {
+                const unsigned long long bits = d == 0 ? mx : my;
+                const bool in0 = (bits >> r) & 1ull, in1 = (bits >> (r + 32)) & 1ull;
+                for (int pass = 0; pass < 2; ++pass) {
+                    if (pass == 0 ? !(in0 || in1) : !(in0 && in1)) continue;
+                    const int L = 2 * d + ((pass == 1 || !in0) ? 1 : 0);
+                    const double sg = (L & 1) ? -1.0 : 1.0;
+                    double Gi[4], Gk[4];
+                    if (d == 0) {
+                        if (kind == KIND_INTERIOR) {
+                            flux_gx(si, sg, Gi);
+                            flux_gx(sk, sg, Gk);
+                        } else {
+                            flux_quad(si, sg, s2q, Gi);
+                            flux_quad(sk, sg, s2q, Gk);
+                        }
                     } else {
-                        flux_quad(si, sg, s2q, Gi);
-                        flux_quad(sk, sg, s2q, Gk);
+                        flux_gy(si, sg, Gi);
+                        flux_gy(sk, sg, Gk);
                     }
-                } else {
-                    flux_gy(si, sg, Gi);
-                    flux_gy(sk, sg, Gk);
+                    for (int m = 0; m < 4; ++m) e[4 * L + m] = Gk[m] - Gi[m];
                 }
-                for (int m = 0; m < 4; ++m) e[4 * L + m] = Gk[m] - Gi[m];
             }
             e[16] = delx * ny - dely * nx;
             e[17] = delx * nx + dely * ny;
@@ -336,9 +343,14 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
             KStateB sib, skb;
             kzero(sib);
             kzero(skb);
-            for (int LL = 0; LL < 4; ++LL) {
-                const unsigned long long bits = (LL < 2) ? mx : my;
-                if (!((bits >> (r + ((LL & 1) ? 32 : 0))) & 1ull)) continue;
+            for (int slot = 0; slot < 4; ++slot) {
+                // (direction, pass) as in phase A: the lists holding the
+                // neighbour in ascending order, one converged pass each
+                const int d = slot >> 1, pass = slot & 1;
+                const unsigned long long bits = d == 0 ? mx : my;
+                const bool in0 = (bits >> r) & 1ull, in1 = (bits >> (r + 32)) & 1ull;
+                if (pass == 0 ? !(in0 || in1) : !(in0 && in1)) continue;
+                const int LL = 2 * d + ((pass == 1 || !in0) ? 1 : 0);
                 if ((kind == KIND_WALL && LL == 2) || (kind == KIND_OUTER && LL == 3)) continue;
                 const double sg = (LL & 1) ? -1.0 : 1.0;
                 double dGb[4], mdGb[4];
@@ -352,7 +364,7 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
                 const double s2b = lb[grp][LL][8], n2b = lb[grp][LL][9], snb = lb[grp][LL][10];
                 delsb += 2.0 * dels * s2b + deln * snb;
                 delnb += 2.0 * deln * n2b + dels * snb;
-                if (LL < 2) {
+                if (d == 0) {
                     if (kind == KIND_INTERIOR) {
                         flux_gx_b(sk, sg, dGb, skb);
                         flux_gx_b(si, sg, mdGb, sib);
