@@ -21,6 +21,15 @@ struct AdjShape {
     const double *nx, *ny;
 };
 
+// Source lists of the gather forms of the force and normal reverses (one
+// thread per boundary point; see k_forces_b_gather).  Null pointers select
+// the single-thread kernels.
+struct AdjGather {
+    int nbnd;
+    const int *fptr, *fsrc;  // forces: 3 j + role, per boundary point
+    const int *nptr, *nsrc;  // normals: 2 j + role, per boundary point
+};
+
 cudaError_t init_adjoint_kernels();
 void launch_update_b(const Geom &g, const Consts &c, const AdjConsts &a, const R4 *prim_in,
                      const R4 *prim_old, const R4 *fr, const double *pb_out, double *pb_in,
@@ -42,11 +51,11 @@ void launch_gather(int n, int kp, const int *tptr, const int *tlist, const doubl
                    int mode, double *a4, double *a8, double *b8, double *xb, double *yb,
                    cudaStream_t s);
 void launch_qvar_b(int n, const R4 *prim, const double *qb, double *pb, cudaStream_t s);
-void launch_forces_b(const AdjShape &t, const R4 *prim, const double2 *xy, double mach,
-                     double cos_t, double sin_t, int objective, double *pb, double *xb,
-                     double *yb, double *nxb, double *nyb, cudaStream_t s);
-void launch_normals_b(int nbnd, const int *left, const int *right, const double2 *xy,
-                      const double *nxb, const double *nyb, double *xb, double *yb,
-                      cudaStream_t s);
+void launch_forces_b(const AdjShape &t, const AdjGather &gth, const R4 *prim, const double2 *xy,
+                     double mach, double cos_t, double sin_t, int objective, double *pb,
+                     double *xb, double *yb, double *nxb, double *nyb, cudaStream_t s);
+void launch_normals_b(int nbnd, const AdjGather &gth, const int *left, const int *right,
+                      const double2 *xy, const double *nxb, const double *nyb, double *xb,
+                      double *yb, cudaStream_t s);
 
 }  // namespace lskum

@@ -36,6 +36,9 @@ struct AdjointState {
     double *d_snx = nullptr, *d_sny = nullptr;
     int nbnd = 0;
     int *d_bleft = nullptr, *d_bright = nullptr;
+    // source lists of the gather forms of the force / normal reverses
+    // (null: the single-thread kernels run)
+    int *d_fptr = nullptr, *d_fsrc = nullptr, *d_nptr = nullptr, *d_nsrc = nullptr;
     R4 *tprim[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     R4 *tq[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     R4 *tfr[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -127,6 +130,45 @@ int adj_setup(mfcfd_t *h) {
         CK(cudaMemcpy(a->d_sright, sr.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(a->d_snx, snx.data(), ns * sizeof(double), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(a->d_sny, sny.data(), ns * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    // per boundary point q, the entries j of the force and normal reverses
+    // that add to xb[q] / yb[q], in the serial loops' order (ascending j, and
+    // within one j the order of its statements)
+    {
+        const int nb = a->nbnd;
+        std::vector<std::vector<int>> nl(std::max(nb, 1)), fl(std::max(nb, 1));
+        bool n_ok = nb > 0, f_ok = nb > 0;
+        for (int j = 0; j < nb && n_ok; ++j) {
+            if (br[j] < 0 || br[j] >= nb || bl[j] < 0 || bl[j] >= nb) n_ok = false;
+            else {
+                nl[br[j]].push_back(2 * j);
+                nl[bl[j]].push_back(2 * j + 1);
+            }
+        }
+        for (int j = 0; j < a->nshape && f_ok; ++j) {
+            const int tgt[3] = {si[j], sl[j], sr[j]};
+            for (int role = 0; role < 3; ++role) {
+                if (tgt[role] < 0 || tgt[role] >= nb) { f_ok = false; break; }
+                fl[tgt[role]].push_back(3 * j + role);
+            }
+        }
+        auto upload_csr = [&](const std::vector<std::vector<int>> &lists, int **d_ptr,
+                              int **d_src) -> int {
+            std::vector<int> ptr(nb + 1, 0), src;
+            for (int q = 0; q < nb; ++q) {
+                ptr[q + 1] = ptr[q] + (int)lists[q].size();
+                src.insert(src.end(), lists[q].begin(), lists[q].end());
+            }
+            if (src.empty()) src.push_back(0);
+            CK(dmalloc(d_ptr, ptr.size()));
+            CK(dmalloc(d_src, src.size()));
+            CK(cudaMemcpy(*d_ptr, ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(*d_src, src.data(), src.size() * sizeof(int), cudaMemcpyHostToDevice));
+            return MFCFD_OK;
+        };
+        int st = MFCFD_OK;
+        if (n_ok && (st = upload_csr(nl, &a->d_nptr, &a->d_nsrc))) return st;
+        if (f_ok && (st = upload_csr(fl, &a->d_fptr, &a->d_fsrc))) return st;
     }
     // tape of one iteration and the adjoint arrays
     for (int s = 0; s <= rks; ++s) {
@@ -268,7 +310,8 @@ int reverse_iteration(mfcfd_t *h, AdjointState *a, int k, const R4 *state) {
         CK(cudaMemsetAsync(a->pb[0], 0, sizeof(double) * 4 * n, s));
         if (a->objective == MFCFD_OBJ_CL || a->objective == MFCFD_OBJ_CD) {
             AdjShape t{a->nshape, a->d_sidx, a->d_sleft, a->d_sright, a->d_snx, a->d_sny};
-            launch_forces_b(t, a->tprim[a->rks], h->d_xy, h->p.mach, h->cos_t, h->sin_t,
+            const AdjGather gth{a->nbnd, a->d_fptr, a->d_fsrc, a->d_nptr, a->d_nsrc};
+            launch_forces_b(t, gth, a->tprim[a->rks], h->d_xy, h->p.mach, h->cos_t, h->sin_t,
                             a->objective, a->pb[0], a->xb, a->yb, a->nxb, a->nyb, s);
         } else {
             lskum_host::launch_objective_b(h, a->objective, a->tprim[a->rks], a->pb[0], a->xb,
@@ -330,7 +373,8 @@ void lskum_host::free_adjoint(mfcfd_t *h) {
     AdjointState *a = h->adj;
     if (!a) return;
     void *bufs[] = {a->d_tptr, a->d_tlist, a->d_sidx, a->d_sleft, a->d_sright, a->d_snx,
-                    a->d_sny, a->d_bleft, a->d_bright, a->tdq, a->tqm, a->tdelta, a->tspd,
+                    a->d_sny, a->d_bleft, a->d_bright, a->d_fptr, a->d_fsrc, a->d_nptr,
+                    a->d_nsrc, a->tdq, a->tqm, a->tdelta, a->tspd,
                     a->pb[0], a->pb[1], a->pbA, a->qb, a->dqb[0], a->dqb[1], a->qmb,
                     a->deltab, a->frb, a->xb, a->yb, a->nxb, a->nyb, a->contrib, a->hist,
                     a->snap0, a->fin};
@@ -359,7 +403,8 @@ bool adjoint_args_ok(const mfcfd_t *h, int objective, int n_iters) {
 int adjoint_prepare(mfcfd_t *h, int objective, int n_iters, size_t ckpt_bytes, int *nsnap) {
     if (h->fp32) return fail(h, MFCFD_ERR_ARG, "mfcfd_adjoint: FP64 handles only");
     if (h->p.power != 0.0)
-        return fail(h, MFCFD_ERR_ARG, "mfcfd_adjoint: LSQ weights with power != 0 are not differentiated");
+        return fail(h, MFCFD_ERR_ARG,
+                    "mfcfd_adjoint: LSQ weights with power != 0 are not differentiated");
     int st = adj_setup(h);
     if (st) return st;
     AdjointState *a = h->adj;
@@ -400,8 +445,9 @@ int adjoint_execute(mfcfd_t *h, int nsnap, double *J, double *dJdx, double *dJdy
     CK(cudaMemsetAsync(a->nyb, 0, sizeof(double) * n, h->stream));
     int st = reverse_range(h, a, 0, a->n_iters, a->snap0, free_slots, scratch);
     if (st) return st;
-    launch_normals_b(a->nbnd, a->d_bleft, a->d_bright, h->d_xy, a->nxb, a->nyb, a->xb, a->yb,
-                     h->stream);
+    const AdjGather gth{a->nbnd, a->d_fptr, a->d_fsrc, a->d_nptr, a->d_nsrc};
+    launch_normals_b(a->nbnd, gth, a->d_bleft, a->d_bright, h->d_xy, a->nxb, a->nyb, a->xb,
+                     a->yb, h->stream);
     h->launches += 1;
     CK(cudaGetLastError());
     // leave the final state current, as mfcfd_run would

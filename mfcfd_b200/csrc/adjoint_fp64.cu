@@ -15,6 +15,8 @@
 // fixed (i, r) order of the transposed stencil: results are deterministic.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "adjoint.h"
 #include "lskum_adjoint.cuh"
 
@@ -769,6 +771,89 @@ __global__ void k_normals_b(int nbnd, const int *__restrict__ left, const int *_
     }
 }
 
+// The same two reverses with a thread per boundary point q.  src[ptr[q] ..
+// ptr[q+1]) lists the entries j whose loop body above adds to xb[q] / yb[q],
+// in the loop's order (ascending j; within one j the order of its
+// statements), so that each sum is formed in the serial kernel's order and
+// the results are the same bit for bit.  Normals: src = 2j + (0: q is
+// right[j], 1: q is left[j]).  Forces: src = 3j + (0: q is idx[j], 1: q is
+// left[j], 2: q is right[j]).
+__global__ void k_normals_b_gather(int nbnd, const int *__restrict__ left,
+                                   const int *__restrict__ right, const double2 *__restrict__ xy,
+                                   const double *__restrict__ nxb, const double *__restrict__ nyb,
+                                   const int *__restrict__ ptr, const int *__restrict__ src,
+                                   double *__restrict__ xb, double *__restrict__ yb) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nbnd) return;
+    double xq = xb[q], yq = yb[q];
+    for (int e = ptr[q]; e < ptr[q + 1]; ++e) {
+        const int m = src[e] >> 1, role = src[e] & 1;
+        const int l = left[m], r = right[m];
+        const double2 L = xy[l], M = xy[m], R = xy[r];
+        const double vx = 0.5 * ((M.y - L.y) + (R.y - M.y));
+        const double vy = 0.5 * ((M.x - L.x) + (R.x - M.x));
+        const double det = sqrt(vx * vx + vy * vy);
+        double vxb = -nxb[m] / det;
+        double vyb = nyb[m] / det;
+        const double detb = nxb[m] * vx / (det * det) - nyb[m] * vy / (det * det);
+        vxb += detb * vx / det;
+        vyb += detb * vy / det;
+        if (role == 0) {
+            yq += 0.5 * vxb;
+            xq += 0.5 * vyb;
+        } else {
+            yq -= 0.5 * vxb;
+            xq -= 0.5 * vyb;
+        }
+    }
+    xb[q] = xq;
+    yb[q] = yq;
+}
+
+__global__ void k_forces_b_gather(AdjShape t, int nbnd, const R4 *__restrict__ prim,
+                                  const double2 *__restrict__ xy, double mach, double cos_t,
+                                  double sin_t, int objective, const int *__restrict__ ptr,
+                                  const int *__restrict__ src, double *__restrict__ pb,
+                                  double *__restrict__ xb, double *__restrict__ yb,
+                                  double *__restrict__ nxb, double *__restrict__ nyb) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nbnd) return;
+    const double pr_inf = 1.0 / 1.4;
+    const double temp = 0.5 * 1.0 * mach * mach;
+    const double Hb = objective == 1 ? cos_t : -sin_t;
+    const double Vb = objective == 1 ? sin_t : cos_t;
+    double xq = xb[q], yq = yb[q];
+    for (int e = ptr[q]; e < ptr[q + 1]; ++e) {
+        const int j = src[e] / 3, role = src[e] % 3;
+        const int m = t.idx[j], l = t.left[j], r = t.right[j];
+        const double nx = t.nx[j], ny = t.ny[j];
+        const double2 L = xy[l], M = xy[m], R = xy[r];
+        const double ds1 = sqrt((M.x - L.x) * (M.x - L.x) + (M.y - L.y) * (M.y - L.y));
+        const double ds2 = sqrt((R.x - M.x) * (R.x - M.x) + (R.y - M.y) * (R.y - M.y));
+        const double ds = 0.5 * (ds1 + ds2);
+        double cp = prim[m].d - pr_inf;
+        cp = -cp / temp;
+        const double dsb = Hb * cp * nx + Vb * cp * ny;
+        const double d1 = 0.5 * dsb / ds1, d2 = 0.5 * dsb / ds2;
+        if (role == 0) {
+            const double cpb = Hb * nx * ds + Vb * ny * ds;
+            nxb[m] += Hb * cp * ds;
+            nyb[m] += Vb * cp * ds;
+            pb[4 * (size_t)m + 3] += -cpb / temp;
+            xq += d1 * (M.x - L.x) - d2 * (R.x - M.x);
+            yq += d1 * (M.y - L.y) - d2 * (R.y - M.y);
+        } else if (role == 1) {
+            xq -= d1 * (M.x - L.x);
+            yq -= d1 * (M.y - L.y);
+        } else {
+            xq += d2 * (R.x - M.x);
+            yq += d2 * (R.y - M.y);
+        }
+    }
+    xb[q] = xq;
+    yb[q] = yq;
+}
+
 inline int nblk(int n, int b) { return (n + b - 1) / b; }
 
 }  // namespace
@@ -828,16 +913,26 @@ void launch_qvar_b(int n, const R4 *prim, const double *qb, double *pb, cudaStre
     k_qvar_b<<<nblk(n, 256), 256, 0, s>>>(n, prim, qb, pb);
 }
 
-void launch_forces_b(const AdjShape &t, const R4 *prim, const double2 *xy, double mach,
-                     double cos_t, double sin_t, int objective, double *pb, double *xb,
-                     double *yb, double *nxb, double *nyb, cudaStream_t s) {
-    k_forces_b<<<1, 32, 0, s>>>(t, prim, xy, mach, cos_t, sin_t, objective, pb, xb, yb, nxb, nyb);
+void launch_forces_b(const AdjShape &t, const AdjGather &gth, const R4 *prim, const double2 *xy,
+                     double mach, double cos_t, double sin_t, int objective, double *pb,
+                     double *xb, double *yb, double *nxb, double *nyb, cudaStream_t s) {
+    if (gth.fptr)
+        k_forces_b_gather<<<nblk(std::max(gth.nbnd, 1), 128), 128, 0, s>>>(
+            t, gth.nbnd, prim, xy, mach, cos_t, sin_t, objective, gth.fptr, gth.fsrc, pb, xb, yb,
+            nxb, nyb);
+    else
+        k_forces_b<<<1, 32, 0, s>>>(t, prim, xy, mach, cos_t, sin_t, objective, pb, xb, yb, nxb,
+                                    nyb);
 }
 
-void launch_normals_b(int nbnd, const int *left, const int *right, const double2 *xy,
-                      const double *nxb, const double *nyb, double *xb, double *yb,
-                      cudaStream_t s) {
-    k_normals_b<<<1, 32, 0, s>>>(nbnd, left, right, xy, nxb, nyb, xb, yb);
+void launch_normals_b(int nbnd, const AdjGather &gth, const int *left, const int *right,
+                      const double2 *xy, const double *nxb, const double *nyb, double *xb,
+                      double *yb, cudaStream_t s) {
+    if (gth.nptr)
+        k_normals_b_gather<<<nblk(std::max(nbnd, 1), 128), 128, 0, s>>>(
+            nbnd, left, right, xy, nxb, nyb, gth.nptr, gth.nsrc, xb, yb);
+    else
+        k_normals_b<<<1, 32, 0, s>>>(nbnd, left, right, xy, nxb, nyb, xb, yb);
 }
 
 }  // namespace lskum
