@@ -555,30 +555,55 @@ __global__ void k_init_state(Geom g, const R4 *__restrict__ prim, R4 *__restrict
 }
 
 // compute_force_coeffs.F90:11-102, one thread, shape points in grid order.
-__global__ void k_forces(ShapeTab t, const R4 *__restrict__ prim, double mach, double cos_t,
-                         double sin_t, double *out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// One block of FORCE_BLOCK threads: per chunk of FORCE_BLOCK shape points the
+// threads form cp and the point's three terms in parallel, then thread 0
+// adds them to its shape's sums in point order (the reference's loop order),
+// so the sums do not depend on the launch.
+constexpr int FORCE_BLOCK = 1024;
+
+__global__ void __launch_bounds__(FORCE_BLOCK)
+k_forces(ShapeTab t, const R4 *__restrict__ prim, double mach, double cos_t, double sin_t,
+         double *out) {
+    __shared__ double th[FORCE_BLOCK], tv[FORCE_BLOCK], tm[FORCE_BLOCK];
+    __shared__ int ts[FORCE_BLOCK];
     const double rho_inf = 1.0, pr_inf = 1.0 / 1.4;
     double *H = out, *V = out + t.shapes, *PM = out + 2 * t.shapes;
     double *cp_out = out + 3 * t.shapes;
-    for (int s = 0; s < t.shapes; ++s) H[s] = V[s] = PM[s] = 0.0;
-    double temp = 0.5 * rho_inf * mach * mach;
-    for (int j = 0; j < t.npts; ++j) {
-        int m = t.idx[j], s = t.shape[j];
-        double nx = t.geo[4 * j], ny = t.geo[4 * j + 1], ds = t.geo[4 * j + 2];
-        double mx = t.geo[4 * j + 3], my = t.my[j];
-        double cp = prim[m].d - pr_inf;
-        cp = -cp / temp;
-        cp_out[j] = cp;
-        H[s] = H[s] + cp * nx * ds;
-        V[s] = V[s] + cp * ny * ds;
-        PM[s] = PM[s] + (-cp * ny * ds * (mx - 0.25) + cp * nx * ds * (my));
+    if (threadIdx.x == 0)
+        for (int s = 0; s < t.shapes; ++s) H[s] = V[s] = PM[s] = 0.0;
+    const double temp = 0.5 * rho_inf * mach * mach;
+    for (int j0 = 0; j0 < t.npts; j0 += FORCE_BLOCK) {
+        const int j = j0 + threadIdx.x;
+        if (j < t.npts) {
+            const int m = t.idx[j];
+            const double nx = t.geo[4 * j], ny = t.geo[4 * j + 1], ds = t.geo[4 * j + 2];
+            const double mx = t.geo[4 * j + 3], my = t.my[j];
+            double cp = prim[m].d - pr_inf;
+            cp = -cp / temp;
+            cp_out[j] = cp;
+            th[threadIdx.x] = cp * nx * ds;
+            tv[threadIdx.x] = cp * ny * ds;
+            tm[threadIdx.x] = -cp * ny * ds * (mx - 0.25) + cp * nx * ds * (my);
+            ts[threadIdx.x] = t.shape[j];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int nj = min(FORCE_BLOCK, t.npts - j0);
+            for (int q = 0; q < nj; ++q) {
+                const int s = ts[q];
+                H[s] = H[s] + th[q];
+                V[s] = V[s] + tv[q];
+                PM[s] = PM[s] + tm[q];
+            }
+        }
+        __syncthreads();
     }
-    for (int s = 0; s < t.shapes; ++s) {
-        double h = H[s], v = V[s];
-        H[s] = v * cos_t - h * sin_t;  // Cl
-        V[s] = h * cos_t + v * sin_t;  // Cd
-    }
+    if (threadIdx.x == 0)
+        for (int s = 0; s < t.shapes; ++s) {
+            double h = H[s], v = V[s];
+            H[s] = v * cos_t - h * sin_t;  // Cl
+            V[s] = h * cos_t + v * sin_t;  // Cd
+        }
 }
 
 inline int nblk(int n, int b) { return (n + b - 1) / b; }
@@ -651,7 +676,7 @@ void launch_init_state(const Geom &g, const R4 *prim, R4 *q, double *spd, cudaSt
 
 void launch_forces(const ShapeTab &t, const R4 *prim, double mach, double cos_t, double sin_t,
                    double *out, cudaStream_t s) {
-    k_forces<<<1, 32, 0, s>>>(t, prim, mach, cos_t, sin_t, out);
+    k_forces<<<1, FORCE_BLOCK, 0, s>>>(t, prim, mach, cos_t, sin_t, out);
 }
 
 }  // namespace lskum
