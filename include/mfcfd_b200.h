@@ -131,8 +131,9 @@ int mfcfd_adjoint(mfcfd_t *h, int objective, int n_iters, size_t ckpt_bytes, dou
  * per handle are those of mfcfd_adjoint on it (bit for bit): J[i] (J may be
  * NULL), dJdx[i], dJdy[i] (caller order), n_forward[i] (may be NULL),
  * status[i] (may be NULL; MFCFD_OK or that handle's error).  Handles must be
- * distinct and on distinct streams.  Returns MFCFD_OK or the first
- * handle's error. */
+ * distinct and on distinct streams; handles may live on different devices
+ * (each handle's work runs with its device current; the caller's current
+ * device is restored).  Returns MFCFD_OK or the first handle's error. */
 #define MFCFD_ADJOINT_MANY_MAX 256
 int mfcfd_adjoint_many(int n_handles, mfcfd_t *const *handles, int objective, int n_iters,
                        size_t ckpt_bytes, double *J, double *const *dJdx, double *const *dJdy,
@@ -143,9 +144,10 @@ int mfcfd_adjoint_many(int n_handles, mfcfd_t *const *handles, int objective, in
  * pointd%x(1) = 1).  From the handle's current state (held fixed) it runs
  * n_iters iterations with the grid moved along the direction (dx, dy) per
  * point (caller order; NULL = 0) and writes J = an MFCFD_OBJ_* objective of
- * the final state and dJ/de along the direction.  For the gradient of mfcfd_adjoint over the same iterations,
- * dJ/de = sum_i dJdx_i dx_i + dJdy_i dy_i.  The handle's state is left
- * unchanged.  FP64 handles with power == 0 only (else MFCFD_ERR_ARG). */
+ * the final state and dJ/de along the direction.  For the gradient of
+ * mfcfd_adjoint over the same iterations, dJ/de = sum_i dJdx_i dx_i +
+ * dJdy_i dy_i.  The handle's state is left unchanged.  FP64 handles with
+ * power == 0 only (else MFCFD_ERR_ARG). */
 int mfcfd_tangent(mfcfd_t *h, int objective, int n_iters, const double *dx, const double *dy,
                   double *J, double *dJ);
 

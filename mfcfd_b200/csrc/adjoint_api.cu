@@ -496,12 +496,22 @@ extern "C" int mfcfd_adjoint_many(int n_handles, mfcfd_t *const *handles, int ob
                             "mfcfd_adjoint_many: handles must be distinct, on distinct streams");
     }
     std::vector<int> st(n_handles, MFCFD_OK), nsnap(n_handles, 0);
+    // the CUDA device is per host thread: each handle's work runs with the
+    // handle's device current, and the caller's device is restored at the end
+    int caller_dev = 0;
+    if (cudaGetDevice(&caller_dev) != cudaSuccess) caller_dev = handles[0]->dev;
+    auto use_dev = [&](int i) -> int {
+        const cudaError_t e = cudaSetDevice(handles[i]->dev);
+        return e == cudaSuccess ? MFCFD_OK : cuda_fail(handles[i], e, "cudaSetDevice");
+    };
     // every allocation first, one handle after the other
     for (int i = 0; i < n_handles; ++i) {
-        st[i] = adjoint_prepare(handles[i], objective, n_iters, ckpt_bytes, &nsnap[i]);
+        st[i] = use_dev(i);
+        if (!st[i]) st[i] = adjoint_prepare(handles[i], objective, n_iters, ckpt_bytes, &nsnap[i]);
         if (st[i]) {
             if (status)
                 for (int k = 0; k < n_handles; ++k) status[k] = k == i ? st[i] : MFCFD_OK;
+            cudaSetDevice(caller_dev);
             return st[i];
         }
     }
@@ -511,21 +521,43 @@ extern "C" int mfcfd_adjoint_many(int n_handles, mfcfd_t *const *handles, int ob
     // of its own, and its latency-bound sweep overlaps that chain on its own
     // stream.  Running all large sweeps at once only made them contend.
     auto run = [&](int i) {
+        st[i] = use_dev(i);
+        if (st[i]) return;
         st[i] = adjoint_execute(handles[i], nsnap[i], J ? J + i : nullptr, dJdx[i], dJdy[i],
                                 n_forward ? n_forward + i : nullptr);
     };
-    std::vector<int> large;
+    std::vector<int> large, small;
+    for (int i = 0; i < n_handles; ++i)
+        (handles[i]->n >= ADJ_OVERLAP_POINTS ? large : small).push_back(i);
+    auto run_large = [&] {
+        for (int i : large) run(i);
+    };
+    // a thread that cannot be created runs its work on the calling thread
     std::vector<std::thread> pool;
-    pool.reserve(n_handles);
-    for (int i = 0; i < n_handles; ++i) {
-        if (handles[i]->n >= ADJ_OVERLAP_POINTS) large.push_back(i);
-        else pool.emplace_back(run, i);
+    std::vector<int> inline_small;
+    bool large_inline = false;
+    try {
+        pool.reserve(n_handles + 1);
+    } catch (...) {
     }
-    if (!large.empty())
-        pool.emplace_back([&] {
-            for (int i : large) run(i);
-        });
+    for (int i : small) {
+        try {
+            pool.emplace_back(run, i);
+        } catch (...) {
+            inline_small.push_back(i);
+        }
+    }
+    if (!large.empty()) {
+        try {
+            pool.emplace_back(run_large);
+        } catch (...) {
+            large_inline = true;
+        }
+    }
+    for (int i : inline_small) run(i);
+    if (large_inline) run_large();
     for (auto &t : pool) t.join();
+    cudaSetDevice(caller_dev);
     int first = MFCFD_OK;
     for (int i = 0; i < n_handles; ++i) {
         if (status) status[i] = st[i];
