@@ -329,7 +329,8 @@ def adjoint_batch_leg(args, world, rank, dist):
 
 def batch_leg(args, stream, world, rank, dist):
     """The batched workload: 64 seeded instances (4k-256k points, M, aoa and
-    thickness drawn per instance), sharded across ranks with no exchange,
+    thickness drawn per instance; FP32-mixed unless --batch-precision says
+    otherwise), sharded across ranks with no exchange,
     advanced together by one Batch for a bounded number of iterations (tol
     -8 retires an instance early), device-timed on the stream; beside it the
     same instances run one Solver at a time for the same iterations."""
@@ -339,7 +340,8 @@ def batch_leg(args, stream, world, rank, dist):
     from mfcfd_b200.solver import Solver
     grids, flows, specs = batch_instances(args.batch_instances)
     mine = shard(len(grids), rank, world)
-    grids, flows = [grids[i] for i in mine], [flows[i] for i in mine]
+    grids = [grids[i] for i in mine]
+    flows = [dict(flows[i], precision=args.batch_precision) for i in mine]
     n = args.batch_iters
     with Batch(grids, flows) as b:
         b.set_stream(stream.cuda_stream)
@@ -372,7 +374,7 @@ def batch_leg(args, stream, world, rank, dist):
     states = {k: r.state.count(k) for k in sorted(set(r.state))}
     return {"config": (f"{args.batch_instances} NACA 00tt O-grids, N log-uniform in [4k, 256k] "
                        f"(seeded draws), M in [0.5, 0.8], aoa in [-2, 4] deg, t in [0.08, 0.16], "
-                       f"FP64, retire at residue <= -8 or {n} iterations"),
+                       f"{args.batch_precision}, retire at residue <= -8 or {n} iterations"),
             "instances_per_rank": len(grids), "points_per_rank": int(sum(g.n for g in grids)),
             "iterations": n, "value": work / (batch_ms / 1e3) / 1e6, "unit": UNIT,
             "ms": batch_ms, "one_handle_at_a_time_ms": seq_ms,
@@ -397,6 +399,8 @@ def main():
     ap.add_argument("--batch-iters", type=int, default=100,
                     help="iterations of the batched-workload leg (0 = skip)")
     ap.add_argument("--batch-instances", type=int, default=64)
+    ap.add_argument("--batch-precision", choices=("fp32_mixed", "fp64"), default="fp32_mixed",
+                    help="precision of the batched leg (the batched workload is FP32-mixed)")
     ap.add_argument("--adjoint-batch-iters", type=int, default=20,
                     help="iterations reversed by the batched-adjoint leg (0 = skip)")
     ap.add_argument("--adjoint-batch-instances", type=int, default=16)
