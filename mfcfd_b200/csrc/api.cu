@@ -20,6 +20,7 @@
 #include <deque>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "handle.h"
@@ -790,25 +791,67 @@ int mfcfd_set_stream(mfcfd_t *h, void *stream) {
     return MFCFD_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Runs fn(begin, end) over [0, n) split into contiguous ranges on up to 8
+// host threads (the state copies between the caller's order and the
+// renumbered staging buffer are host-memory bound); each range is written by
+// one thread only, so the result does not depend on the split.  A thread
+// that cannot be created runs its range on the calling thread.
+template <class F>
+void host_parallel_for(int n, F fn) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nt = (int)std::min<long long>({8LL, (long long)hw, (long long)n / 65536 + 1});
+    if (nt <= 1) {
+        fn(0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    std::vector<int> inline_ranges;
+    const int chunk = (n + nt - 1) / nt;
+    for (int t = 1; t < nt; ++t) {
+        const int b = t * chunk, e = std::min(n, b + chunk);
+        if (b >= e) break;
+        try {
+            pool.emplace_back(fn, b, e);
+        } catch (...) {
+            inline_ranges.push_back(t);
+        }
+    }
+    fn(0, std::min(n, chunk));
+    for (int t : inline_ranges) fn(t * chunk, std::min(n, t * chunk + chunk));
+    for (auto &th : pool) th.join();
+}
+
+}  // namespace
+
+extern "C" {
+
 int mfcfd_set_state(mfcfd_t *h, const double *prim) {
     if (!h || !prim) return MFCFD_ERR_ARG;
     CK(cudaStreamSynchronize(h->stream));
     if (h->fp32) {
         float *fs = reinterpret_cast<float *>(h->h_stage);
-        for (int p = 0; p < h->n; ++p) {
-            const double *src = prim + 4 * (size_t)h->perm[p];
-            float *dst = fs + 4 * (size_t)p;
-            dst[0] = (float)src[0]; dst[1] = (float)src[1]; dst[2] = (float)src[2];
-            dst[3] = (float)src[3];
-        }
+        host_parallel_for(h->n, [&](int b, int e) {
+            for (int p = b; p < e; ++p) {
+                const double *src = prim + 4 * (size_t)h->perm[p];
+                float *dst = fs + 4 * (size_t)p;
+                dst[0] = (float)src[0]; dst[1] = (float)src[1]; dst[2] = (float)src[2];
+                dst[3] = (float)src[3];
+            }
+        });
         CK(cudaMemcpyAsync(h->f_prim[h->cur], fs, sizeof(float) * 4 * (size_t)h->n,
                            cudaMemcpyHostToDevice, h->stream));
     } else {
-        for (int p = 0; p < h->n; ++p) {
-            const double *src = prim + 4 * (size_t)h->perm[p];
-            double *dst = h->h_stage + 4 * (size_t)p;
-            dst[0] = src[0]; dst[1] = src[1]; dst[2] = src[2]; dst[3] = src[3];
-        }
+        host_parallel_for(h->n, [&](int b, int e) {
+            for (int p = b; p < e; ++p) {
+                const double *src = prim + 4 * (size_t)h->perm[p];
+                double *dst = h->h_stage + 4 * (size_t)p;
+                dst[0] = src[0]; dst[1] = src[1]; dst[2] = src[2]; dst[3] = src[3];
+            }
+        });
         CK(cudaMemcpyAsync(h->d_prim[h->cur], h->h_stage, sizeof(double) * 4 * (size_t)h->n,
                            cudaMemcpyHostToDevice, h->stream));
     }
@@ -825,21 +868,25 @@ int mfcfd_get_state(mfcfd_t *h, double *prim) {
         CK(cudaMemcpyAsync(fs, h->f_prim[h->cur], sizeof(float) * 4 * (size_t)h->n,
                            cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
-        for (int p = 0; p < h->n; ++p) {
-            const float *src = fs + 4 * (size_t)p;
-            double *dst = prim + 4 * (size_t)h->perm[p];
-            dst[0] = src[0]; dst[1] = src[1]; dst[2] = src[2]; dst[3] = src[3];
-        }
+        host_parallel_for(h->n, [&](int b, int e) {
+            for (int p = b; p < e; ++p) {
+                const float *src = fs + 4 * (size_t)p;
+                double *dst = prim + 4 * (size_t)h->perm[p];
+                dst[0] = src[0]; dst[1] = src[1]; dst[2] = src[2]; dst[3] = src[3];
+            }
+        });
         return MFCFD_OK;
     }
     CK(cudaMemcpyAsync(h->h_stage, h->d_prim[h->cur], sizeof(double) * 4 * (size_t)h->n,
                        cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    for (int p = 0; p < h->n; ++p) {
-        const double *src = h->h_stage + 4 * (size_t)p;
-        double *dst = prim + 4 * (size_t)h->perm[p];
-        dst[0] = src[0]; dst[1] = src[1]; dst[2] = src[2]; dst[3] = src[3];
-    }
+    host_parallel_for(h->n, [&](int b, int e) {
+        for (int p = b; p < e; ++p) {
+            const double *src = h->h_stage + 4 * (size_t)p;
+            double *dst = prim + 4 * (size_t)h->perm[p];
+            dst[0] = src[0]; dst[1] = src[1]; dst[2] = src[2]; dst[3] = src[3];
+        }
+    });
     return MFCFD_OK;
 }
 
