@@ -63,6 +63,9 @@ void free_all(mfcfd_t *h) {
     for (auto &row : h->pair_exec)
         for (auto &g : row)
             if (g) cudaGraphExecDestroy(g);
+    for (auto &row : h->one_exec)
+        for (auto &g : row)
+            if (g) cudaGraphExecDestroy(g);
     void *bufs[] = {h->d_xy, h->d_nrm, h->d_eps2, h->d_obc, h->d_conn, h->d_nbhs, h->d_mx,
                     h->d_my, h->d_prim[0], h->d_prim[1], h->d_q[0], h->d_q[1], h->d_dq[0],
                     h->d_dq[1], h->d_qm, h->d_delta, h->d_spd, h->d_res_part, h->d_flux_dbg,
@@ -195,12 +198,40 @@ int enqueue_iteration(mfcfd_t *h, cudaStream_t s) { return enqueue_iteration_to(
 // Captures two consecutive iterations into one graph.  After two iterations
 // both the prim and the q buffer parity are back where they started.
 void drop_graphs(mfcfd_t *h) {
-    for (auto &row : h->pair_exec)
-        for (auto &g : row)
-            if (g) {
-                cudaGraphExecDestroy(g);
-                g = nullptr;
-            }
+    for (auto *tab : {&h->pair_exec, &h->one_exec})
+        for (auto &row : *tab)
+            for (auto &g : row)
+                if (g) {
+                    cudaGraphExecDestroy(g);
+                    g = nullptr;
+                }
+}
+
+// Captures one iteration (the odd one of an odd count) into a graph and
+// records the (cur, qcur) it leaves current.
+int build_one_graph(mfcfd_t *h) {
+    const int cur0 = h->cur, q0 = h->qcur;
+    cudaGraphExec_t &slot = h->one_exec[cur0][q0];
+    if (slot) {
+        cudaGraphExecDestroy(slot);
+        slot = nullptr;
+    }
+    const long long l0 = h->launches;
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(h->own, cudaStreamCaptureModeThreadLocal));
+    const int st = enqueue_iteration(h, h->own);
+    cudaError_t e = cudaStreamEndCapture(h->own, &graph);
+    h->one_next[cur0][q0][0] = h->cur;
+    h->one_next[cur0][q0][1] = h->qcur;
+    h->cur = cur0;
+    h->qcur = q0;
+    h->launches = l0;
+    if (st != MFCFD_OK) return st;
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&slot, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
+    return MFCFD_OK;
 }
 
 int build_pair_graph(mfcfd_t *h) {
@@ -907,8 +938,16 @@ int mfcfd_run(mfcfd_t *h, int it_first, int n_iters, double *residue, int *n_don
     if (int st = lskum_host::reset_run(h, it_first)) return st;
     int rem = n_iters;
     if (rem & 1) {
-        int st = enqueue_iteration(h, h->stream);
-        if (st) return st;
+        if (!h->one_exec[h->cur][h->qcur]) {
+            CK(cudaStreamSynchronize(h->stream));
+            int st = build_one_graph(h);
+            if (st) return st;
+        }
+        CK(cudaGraphLaunch(h->one_exec[h->cur][h->qcur], h->stream));
+        const int c0 = h->cur, q0 = h->qcur;
+        h->cur = h->one_next[c0][q0][0];
+        h->qcur = h->one_next[c0][q0][1];
+        h->launches += (long long)h->p.rks * (2 + h->p.inner_iterations) + 1;
         --rem;
     }
     if (rem > 0) {

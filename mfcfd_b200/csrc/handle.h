@@ -64,6 +64,10 @@ struct mfcfd {
     int iters_done_total = 0;
     cudaStream_t own = nullptr, stream = nullptr;
     cudaGraphExec_t pair_exec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [cur][qcur]
+    // one iteration as a graph (for odd iteration counts), and the (cur, qcur)
+    // it leaves current
+    cudaGraphExec_t one_exec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    int one_next[2][2][2] = {};
     bool keep_diag = false;
     long long launches = 0;
     std::string err;
