@@ -25,6 +25,8 @@
  * renumbered internally; all inputs and outputs use the caller's order.
  *
  * Threading: one host thread per handle at a time; handles are independent.
+ * Some calls use host threads of their own inside the call (state
+ * reordering, mfcfd_adjoint_many) and join them before returning.
  */
 #ifndef MFCFD_B200_H
 #define MFCFD_B200_H
@@ -164,10 +166,12 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
 /* Frees every device and host resource of the handle.  NULL is a no-op. */
 int mfcfd_destroy(mfcfd_t *h);
 
-/* Loads prim(4,N) (restart_sol, initial_conditions.F90:44-70). */
+/* Loads prim(4,N) (restart_sol, initial_conditions.F90:44-70).  The
+ * reordering into the handle's point order runs on up to 8 host threads of
+ * the library's own, joined before the call returns. */
 int mfcfd_set_state(mfcfd_t *h, const double *prim);
 
-/* Copies prim(4,N) out. */
+/* Copies prim(4,N) out (reordered as mfcfd_set_state does). */
 int mfcfd_get_state(mfcfd_t *h, double *prim);
 
 /* Runs iterations it_first .. it_first+n_iters-1 of the q_lskum loop
