@@ -50,6 +50,14 @@ __device__ __forceinline__ KState kst_load(const double *e) {
 }
 
 // state_update_b (state_update.F90:10-141, reverse)
+// Stores n (even) doubles as 16-byte pairs; dst is 16-byte aligned (records
+// are ADJ_CW = 22 doubles = 176 bytes from an aligned base).
+__device__ __forceinline__ void st_pairs(double *dst, const double *v, int n) {
+    double2 *d2 = reinterpret_cast<double2 *>(dst);
+#pragma unroll
+    for (int h = 0; h < n / 2; ++h) d2[h] = make_double2(v[2 * h], v[2 * h + 1]);
+}
+
 #ifndef ADJ_MIN_BLOCKS
 #define ADJ_MIN_BLOCKS 3
 #endif
@@ -401,12 +409,16 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
             reconstruct_b(qk, dxk, dyk, qmaxk, qmink, g.eps2[k], delx, dely, c.gm1, pr_[6], pku1b,
                           pku2b, pkrb, pkpb, qkb, dxkb, dykb, qmaxkb, qminkb, delxb, delyb);
             double *cb = contrib + ((size_t)i * g.kp + r) * ADJ_CW;
-            for (int m = 0; m < 4; ++m) {
-                cb[m] = qkb[m];
-                cb[4 + m] = dxkb[m];
-                cb[8 + m] = dykb[m];
-                cb[12 + m] = qmaxkb[m];
-                cb[16 + m] = qminkb[m];
+            {
+                double v[20];
+                for (int m = 0; m < 4; ++m) {
+                    v[m] = qkb[m];
+                    v[4 + m] = dxkb[m];
+                    v[8 + m] = dykb[m];
+                    v[12 + m] = qmaxkb[m];
+                    v[16 + m] = qminkb[m];
+                }
+                st_pairs(cb, v, 20);
             }
             const R4 qv = ld4(q_in + i);
             const double qi[4] = {qv.a, qv.b, qv.c, qv.d};
@@ -417,8 +429,7 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
                    qmaxib[4] = {0, 0, 0, 0}, qminib[4] = {0, 0, 0, 0};
             reconstruct_b(qi, dxi, dyi, qmaxi, qmini, g.eps2[i], delx, dely, c.gm1, pr_[2], piu1b,
                           piu2b, pirb, pipb, qib, dxib, dyib, qmaxib, qminib, delxb, delyb);
-            cb[20] = delxb;
-            cb[21] = delyb;
+            reinterpret_cast<double2 *>(cb + 20)[0] = make_double2(delxb, delyb);
             // self contribution of this slot, summed in slot order below
             for (int m = 0; m < 4; ++m) {
                 e[m] = qib[m];
@@ -510,6 +521,7 @@ k_inner_b(Geom g, const R4 *__restrict__ q, const double *__restrict__ dq_in,
         double delxb = 2.0 * delx * s0b + dely * s2b;
         double delyb = 2.0 * dely * s1b + delx * s2b;
         double *cb = contrib + ((size_t)i * g.kp + r) * ADJ_CW;
+        double v[14];  // the record, stored as 16-byte pairs at the end
         for (int m = 0; m < 4; ++m) {
             const double t1 = qi[m] - 0.5 * (delx * dxi[m] + dely * dyi[m]);
             const double t2 = qk[m] - 0.5 * (delx * dxk[m] + dely * dyk[m]);
@@ -517,17 +529,18 @@ k_inner_b(Geom g, const R4 *__restrict__ q, const double *__restrict__ dq_in,
             const double db = sxb[m] * delx + syb[m] * dely;
             delxb += sxb[m] * d;
             delyb += syb[m] * d;
-            cb[m] = db;
-            cb[4 + m] = -0.5 * delx * db;
-            cb[8 + m] = -0.5 * dely * db;
+            v[m] = db;
+            v[4 + m] = -0.5 * delx * db;
+            v[8 + m] = -0.5 * dely * db;
             delxb += -0.5 * dxk[m] * db + 0.5 * dxi[m] * db;
             delyb += -0.5 * dyk[m] * db + 0.5 * dyi[m] * db;
             qib[m] -= db;
             dxib[m] += 0.5 * delx * db;
             dyib[m] += 0.5 * dely * db;
         }
-        cb[12] = delxb;
-        cb[13] = delyb;
+        v[12] = delxb;
+        v[13] = delyb;
+        st_pairs(cb, v, 14);
         xib -= delxb;
         yib -= delyb;
     }
@@ -615,6 +628,7 @@ k_grad_b(Geom g, Consts c, const R4 *__restrict__ q, const R4 *__restrict__ prim
         double delxb = 2.0 * delx * s0b + dely * s2b;
         double delyb = 2.0 * dely * s1b + delx * s2b;
         double *cb = contrib + ((size_t)i * g.kp + r) * ADJ_CW;
+        double v[10];  // the record, stored as 16-byte pairs at the end
         for (int m = 0; m < 4; ++m) {
             const double t = sxb[m] * delx + syb[m] * dely;
             double qkb = t;
@@ -623,8 +637,8 @@ k_grad_b(Geom g, Consts c, const R4 *__restrict__ q, const R4 *__restrict__ prim
             if (amin[m] == r) qkb += qmnb[m];
             delxb += sxb[m] * (qk[m] - qi[m]);
             delyb += syb[m] * (qk[m] - qi[m]);
-            cb[m] = qkb;
-            cb[4 + m] = 0.0;
+            v[m] = qkb;
+            v[4 + m] = 0.0;
         }
         if (with_delta && r == amd && dlb != 0.0) {
             const R4 P = ld4(primA + k);
@@ -637,15 +651,16 @@ k_grad_b(Geom g, Consts c, const R4 *__restrict__ q, const R4 *__restrict__ prim
             delxb += distb * delx / dist;
             delyb += distb * dely / dist;
             if (modu > 0.0) {
-                cb[5] = spdb * P.b / modu;
-                cb[6] = spdb * P.c / modu;
+                v[5] = spdb * P.b / modu;
+                v[6] = spdb * P.c / modu;
             }
             const double csb = 3.0 * spdb;
-            cb[7] = csb * 0.5 / (cs * P.a);
-            cb[4] = -csb * 0.5 * P.d / (cs * P.a * P.a);
+            v[7] = csb * 0.5 / (cs * P.a);
+            v[4] = -csb * 0.5 * P.d / (cs * P.a * P.a);
         }
-        cb[8] = delxb;
-        cb[9] = delyb;
+        v[8] = delxb;
+        v[9] = delyb;
+        st_pairs(cb, v, 10);
         xib -= delxb;
         yib -= delyb;
     }
