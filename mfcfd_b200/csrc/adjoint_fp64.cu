@@ -58,6 +58,18 @@ __device__ __forceinline__ void st_pairs(double *dst, const double *v, int n) {
     for (int h = 0; h < n / 2; ++h) d2[h] = make_double2(v[2 * h], v[2 * h + 1]);
 }
 
+// dst[j] += v[j] for n (even) doubles, as 16-byte pairs (dst 16-byte aligned)
+__device__ __forceinline__ void add_pairs(double *dst, const double *v, int n) {
+    double2 *d2 = reinterpret_cast<double2 *>(dst);
+#pragma unroll
+    for (int h = 0; h < n / 2; ++h) {
+        double2 t = d2[h];
+        t.x = t.x + v[2 * h];
+        t.y = t.y + v[2 * h + 1];
+        d2[h] = t;
+    }
+}
+
 #ifndef ADJ_MIN_BLOCKS
 #define ADJ_MIN_BLOCKS 3
 #endif
@@ -544,11 +556,9 @@ k_inner_b(Geom g, const R4 *__restrict__ q, const double *__restrict__ dq_in,
         xib -= delxb;
         yib -= delyb;
     }
-    for (int m = 0; m < 4; ++m) {
-        qb[4 * (size_t)i + m] += qib[m];
-        dqb_in[8 * (size_t)i + m] = dxib[m];
-        dqb_in[8 * (size_t)i + 4 + m] = dyib[m];
-    }
+    add_pairs(qb + 4 * (size_t)i, qib, 4);
+    st_pairs(dqb_in + 8 * (size_t)i, dxib, 4);
+    st_pairs(dqb_in + 8 * (size_t)i + 4, dyib, 4);
     xb[i] += xib;
     yb[i] += yib;
 }
@@ -693,26 +703,17 @@ k_gather(int n, const int *__restrict__ tptr, const int *__restrict__ tlist,
             acc[2 * f + 1] = acc[2 * f + 1] + v.y;
         }
     }
-#pragma unroll
-    for (int m = 0; m < 4; ++m) a4[4 * (size_t)k + m] += acc[m];
+    add_pairs(a4 + 4 * (size_t)k, acc, 4);
     if (MODE == ADJ_GATHER_FLUX) {
-#pragma unroll
-        for (int m = 0; m < 8; ++m) a8[8 * (size_t)k + m] += acc[4 + m];
-#pragma unroll
-        for (int m = 0; m < 8; ++m) b8[8 * (size_t)k + m] += acc[12 + m];
-        xb[k] += acc[NF - 2];
-        yb[k] += acc[NF - 1];
+        add_pairs(a8 + 8 * (size_t)k, acc + 4, 8);
+        add_pairs(b8 + 8 * (size_t)k, acc + 12, 8);
     } else if (MODE == ADJ_GATHER_INNER) {
-#pragma unroll
-        for (int m = 0; m < 8; ++m) a8[8 * (size_t)k + m] += acc[4 + m];
-        xb[k] += acc[NF - 2];
-        yb[k] += acc[NF - 1];
+        add_pairs(a8 + 8 * (size_t)k, acc + 4, 8);
     } else {
-#pragma unroll
-        for (int m = 0; m < 4; ++m) b8[4 * (size_t)k + m] += acc[4 + m];
-        xb[k] += acc[NF - 2];
-        yb[k] += acc[NF - 1];
+        add_pairs(b8 + 4 * (size_t)k, acc + 4, 4);
     }
+    xb[k] += acc[NF - 2];
+    yb[k] += acc[NF - 1];
 }
 
 // eval_q_variables_b: pb += (dq/dprim)^T qb
