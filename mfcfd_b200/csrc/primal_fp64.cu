@@ -53,6 +53,26 @@ __device__ __forceinline__ void ld8(const double *p, double a[4], double b[4]) {
     b[0] = t2.x; b[1] = t2.y; b[2] = t3.x; b[3] = t3.y;
 }
 
+// Rows in 256-bit read-only loads (ld.global.nc.v4.f64, sm_100) for the
+// thread-per-point gathers of the D and I passes: a 32-byte q row in one
+// load, a 64-byte dq row in two.  R4 rows and dq rows are 32-byte aligned.
+// (The flux pass keeps 128-bit loads: the wide form's register quads made
+// it spill at its 96-register cap.)
+__device__ __forceinline__ R4 ld4w(const R4 *p) {
+    R4 r;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(r.a), "=d"(r.b), "=d"(r.c), "=d"(r.d)
+        : "l"(p));
+    return r;
+}
+
+__device__ __forceinline__ void ld8w(const double *p, double a[4], double b[4]) {
+    const R4 u = ld4w(reinterpret_cast<const R4 *>(p));
+    const R4 v = ld4w(reinterpret_cast<const R4 *>(p + 4));
+    a[0] = u.a; a[1] = u.b; a[2] = u.c; a[3] = u.d;
+    b[0] = v.a; b[1] = v.b; b[2] = v.c; b[3] = v.d;
+}
+
 // q_variables.F90:41-112 eval_q_derivatives, and state_update.F90:190-236
 // func_delta (spd[k] = |u_k| + 3 sqrt(p_k/rho_k) of the neighbour's state).
 __device__ __forceinline__ void
@@ -60,7 +80,7 @@ grad_point(const Geom &g, const Consts &c, const R4 *__restrict__ q, const doubl
            double *__restrict__ dq, double *__restrict__ qm, double *__restrict__ delta,
            int with_delta, int i) {
     double2 pi_ = g.xy[i];
-    R4 qv = ld4(q + i);
+    R4 qv = ld4w(q + i);
     double qi[4] = {qv.a, qv.b, qv.c, qv.d};
     double qmax[4] = {qi[0], qi[1], qi[2], qi[3]};
     double qmin[4] = {qi[0], qi[1], qi[2], qi[3]};
@@ -70,7 +90,7 @@ grad_point(const Geom &g, const Consts &c, const R4 *__restrict__ q, const doubl
     int nb = g.nbhs[i];
     for (int r = 0; r < nb; ++r) {
         int k = g.conn[r * g.n + i];
-        R4 kv = ld4(q + k);
+        R4 kv = ld4w(q + k);
         double qk[4] = {kv.a, kv.b, kv.c, kv.d};
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
@@ -130,19 +150,19 @@ __device__ __forceinline__ void
 inner_point(const Geom &g, const Consts &c, const R4 *__restrict__ q,
             const double *__restrict__ dq_in, double *__restrict__ dq_out, int i) {
     double2 pi_ = g.xy[i];
-    R4 qv = ld4(q + i);
+    R4 qv = ld4w(q + i);
     double qi[4] = {qv.a, qv.b, qv.c, qv.d};
     double dxi[4], dyi[4];
-    ld8(dq_in + 8 * (size_t)i, dxi, dyi);
+    ld8w(dq_in + 8 * (size_t)i, dxi, dyi);
     double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
     double sdxq[4] = {0.0, 0.0, 0.0, 0.0}, sdyq[4] = {0.0, 0.0, 0.0, 0.0};
     int nb = g.nbhs[i];
     for (int r = 0; r < nb; ++r) {
         int k = g.conn[r * g.n + i];
-        R4 kv = ld4(q + k);
+        R4 kv = ld4w(q + k);
         double qk[4] = {kv.a, kv.b, kv.c, kv.d};
         double dxk[4], dyk[4];
-        ld8(dq_in + 8 * (size_t)k, dxk, dyk);
+        ld8w(dq_in + 8 * (size_t)k, dxk, dyk);
         double2 pk = g.xy[k];
         double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
         double w = 1.0;
