@@ -38,6 +38,15 @@ __device__ __forceinline__ void ldf8(const float *p, float a[4], float b[4]) {
     b[0] = y.x; b[1] = y.y; b[2] = y.z; b[3] = y.w;
 }
 
+// A 32-byte row (dq or qm of one point) in one 256-bit read-only load
+// (ld.global.nc.v8.f32, sm_100); the rows are 32-byte aligned.
+__device__ __forceinline__ void ldf8w(const float *p, float a[4], float b[4]) {
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(a[0]), "=f"(a[1]), "=f"(a[2]), "=f"(a[3]), "=f"(b[0]), "=f"(b[1]), "=f"(b[2]),
+          "=f"(b[3])
+        : "l"(p));
+}
+
 __device__ __forceinline__ void stf8(float *p, const float a[4], const float b[4]) {
     float4 *v = reinterpret_cast<float4 *>(p);
     v[0] = make_float4(a[0], a[1], a[2], a[3]);
@@ -130,7 +139,7 @@ inner32_point(const Geom &g, const Geom32 &f, const float *__restrict__ dq0,
         const float2 d = __ldg(f.dxy + r * g.n + i);
         const float w = f.w ? __ldg(f.w + r * g.n + i) : 1.0f;
         float dxk[4], dyk[4];
-        ldf8(dq_in + 8 * (size_t)k, dxk, dyk);
+        ldf8w(dq_in + 8 * (size_t)k, dxk, dyk);
         const float wdx = w * d.x, wdy = w * d.y;
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
@@ -206,8 +215,8 @@ flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool va
                 const float4 kv = __ldg(b.q_in + k);
                 const float qk[4] = {kv.x, kv.y, kv.z, kv.w};
                 float dxk[4], dyk[4], qmaxk[4], qmink[4];
-                ldf8(b.dq + 8 * (size_t)k, dxk, dyk);
-                ldf8(b.qm + 8 * (size_t)k, qmaxk, qmink);
+                ldf8w(b.dq + 8 * (size_t)k, dxk, dyk);
+                ldf8w(b.qm + 8 * (size_t)k, qmaxk, qmink);
                 sk = reconstruct_kstate<float>(qk, dxk, dyk, qmaxk, qmink, b.eps2f[k], dxf, dyf,
                                                inv_gm1, nxf, nyf, inv_sqrt_pi);
             }
@@ -215,8 +224,8 @@ flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool va
                 const float4 qv = __ldg(b.q_in + i);
                 const float qi[4] = {qv.x, qv.y, qv.z, qv.w};
                 float dxi[4], dyi[4], qmaxi[4], qmini[4];
-                ldf8(b.dq + 8 * (size_t)i, dxi, dyi);
-                ldf8(b.qm + 8 * (size_t)i, qmaxi, qmini);
+                ldf8w(b.dq + 8 * (size_t)i, dxi, dyi);
+                ldf8w(b.qm + 8 * (size_t)i, qmaxi, qmini);
                 si = reconstruct_kstate<float>(qi, dxi, dyi, qmaxi, qmini, b.eps2f[i], dxf, dyf,
                                                inv_gm1, nxf, nyf, inv_sqrt_pi);
             }
