@@ -56,8 +56,8 @@ __device__ __forceinline__ void ld8(const double *p, double a[4], double b[4]) {
 // Rows in 256-bit read-only loads (ld.global.nc.v4.f64, sm_100) for the
 // thread-per-point gathers of the D and I passes: a 32-byte q row in one
 // load, a 64-byte dq row in two.  R4 rows and dq rows are 32-byte aligned.
-// (The flux pass keeps 128-bit loads: the wide form's register quads made
-// it spill at its 96-register cap.)
+// The flux pass uses them for its 64-byte dq and qm rows only: its 32-byte
+// q rows in the wide form made it spill at its 96-register cap.
 __device__ __forceinline__ R4 ld4w(const R4 *p) {
     R4 r;
     asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
@@ -252,8 +252,8 @@ flux_tile(const Geom &g, const Consts &c, const StageBufs &b, int i, bool valid,
                 const R4 kv = ld4(b.q_in + k);
                 const double qk[4] = {kv.a, kv.b, kv.c, kv.d};
                 double dxk[4], dyk[4], qmaxk[4], qmink[4];
-                ld8(b.dq + 8 * (size_t)k, dxk, dyk);
-                ld8(b.qm + 8 * (size_t)k, qmaxk, qmink);
+                ld8w(b.dq + 8 * (size_t)k, dxk, dyk);
+                ld8w(b.qm + 8 * (size_t)k, qmaxk, qmink);
                 sk = reconstruct_kstate(qk, dxk, dyk, qmaxk, qmink, g.eps2[k], delx, dely,
                                         inv_gm1, nx, ny, inv_sqrt_pi);
             }
@@ -261,8 +261,8 @@ flux_tile(const Geom &g, const Consts &c, const StageBufs &b, int i, bool valid,
                 const R4 qv = ld4(b.q_in + i);
                 const double qi[4] = {qv.a, qv.b, qv.c, qv.d};
                 double dxi[4], dyi[4], qmaxi[4], qmini[4];
-                ld8(b.dq + 8 * (size_t)i, dxi, dyi);
-                ld8(b.qm + 8 * (size_t)i, qmaxi, qmini);
+                ld8w(b.dq + 8 * (size_t)i, dxi, dyi);
+                ld8w(b.qm + 8 * (size_t)i, qmaxi, qmini);
                 si = reconstruct_kstate(qi, dxi, dyi, qmaxi, qmini, g.eps2[i], delx, dely,
                                         inv_gm1, nx, ny, inv_sqrt_pi);
             }
