@@ -63,3 +63,16 @@ def test_config_c1_size():
     g = config_grid("C1")
     assert g.n == 16000
     assert 7.9 < g.mean_nbhs() < 8.0
+
+
+def test_repair_leaves_well_posed_grids_unchanged():
+    # the repair pass only rebuilds points the first pass left singular: a
+    # grid without such points (the 160x100 C1 wall) is the same with and
+    # without it
+    from mfcfd_b200 import grid as G
+    full = config_grid("C1")
+    ni, nj = 160, 100
+    first = naca_ogrid(ni, nj, seed=1000, first_spacing=5e-3, augment=False)
+    G._augment_stencils(first, ni, nj, 1e-4)
+    assert G._repair_stencils(first, ni, nj, 1e-4) == 0
+    assert np.array_equal(first.conn, full.conn) and np.array_equal(first.nbhs, full.nbhs)
