@@ -229,8 +229,8 @@ long long mfcfd_launch_count(mfcfd_t *h);
 
 /* mfcfd_run without any device allocation.  No counterpart in the
  * reference.  For callers that cannot allocate device memory while they run
- * (a host whose device memory belongs to its own pool, a loop being
- * captured into a CUDA graph, a service that allocates only at start-up):
+ * (a host whose device memory belongs to its own pool, a service that
+ * allocates only at start-up):
  * mfcfd_run may grow its residue-history buffer with cudaMalloc and
  * instantiates CUDA graphs; this call keeps the history in a fixed
  * per-device array of MFCFD_NOALLOC_MAX_ITERS doubles (512 KiB, held by every

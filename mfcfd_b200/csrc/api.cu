@@ -1145,8 +1145,7 @@ const char *mfcfd_last_error(mfcfd_t *h) {
 // grows with cudaMalloc when a call asks for more iterations than any call
 // before, and it instantiates CUDA graphs.  Callers that must not allocate
 // device memory once they are running -- a Fortran/OpenACC host whose device
-// memory belongs to its own pool, a loop that is being captured into a CUDA
-// graph (cudaMalloc cannot be captured), a time-critical service that
+// memory belongs to its own pool, a time-critical service that
 // allocates only at start-up -- use this entry point instead.  It keeps the
 // history in the fixed array below, launches the same kernels directly, and
 // calls no cudaMalloc, cudaFree or graph instantiation.

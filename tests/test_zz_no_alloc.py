@@ -1,7 +1,7 @@
 """mfcfd_run_noalloc: the pseudo-time loop for callers that cannot allocate.
 
-A caller whose device memory belongs to its own pool, or whose loop is being
-captured into a CUDA graph, cannot let the library call cudaMalloc while it
+A caller whose device memory belongs to its own pool, or a service that
+allocates only at start-up, cannot let the library call cudaMalloc while it
 runs; mfcfd_run_noalloc keeps its scratch (the residue history) in a fixed
 per-device array instead.  These checks call it through the C ABI and compare
 it with mfcfd_run on an identical solver, on two calls in a row.  The file is
