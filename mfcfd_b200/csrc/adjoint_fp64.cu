@@ -111,7 +111,7 @@ k_update_b(Geom g, Consts c, AdjConsts a, const R4 *__restrict__ prim_in,
     if (kind == KIND_WALL) Up[2] = 0.0;
     const double V1 = Up[1] * ny + Up[2] * nx;
     const double V2 = Up[2] * ny - Up[1] * nx;
-    const double V0 = Up[0], V3 = Up[3];
+    const double V0 = Up[0];
     const double tmp = 1.0 / V0;
     // reverse of prim_out = (V0, V1 tmp, V2 tmp, 0.4 (V3 - 0.5 tmp (V1^2 + V2^2)))
     const double *po = pb_out + 4 * (size_t)i;
@@ -704,10 +704,10 @@ k_gather(int n, const int *__restrict__ tptr, const int *__restrict__ tlist,
         }
     }
     add_pairs(a4 + 4 * (size_t)k, acc, 4);
-    if (MODE == ADJ_GATHER_FLUX) {
+    if constexpr (MODE == ADJ_GATHER_FLUX) {
         add_pairs(a8 + 8 * (size_t)k, acc + 4, 8);
         add_pairs(b8 + 8 * (size_t)k, acc + 12, 8);
-    } else if (MODE == ADJ_GATHER_INNER) {
+    } else if constexpr (MODE == ADJ_GATHER_INNER) {
         add_pairs(a8 + 8 * (size_t)k, acc + 4, 8);
     } else {
         add_pairs(b8 + 4 * (size_t)k, acc + 4, 4);

@@ -46,13 +46,6 @@ __device__ __forceinline__ void st8(double *p, const double a[4], const double b
     v[3] = make_double2(b[2], b[3]);
 }
 
-__device__ __forceinline__ void ld8(const double *p, double a[4], double b[4]) {
-    const double2 *v = reinterpret_cast<const double2 *>(p);
-    double2 t0 = __ldg(v), t1 = __ldg(v + 1), t2 = __ldg(v + 2), t3 = __ldg(v + 3);
-    a[0] = t0.x; a[1] = t0.y; a[2] = t1.x; a[3] = t1.y;
-    b[0] = t2.x; b[1] = t2.y; b[2] = t3.x; b[3] = t3.y;
-}
-
 // Rows in 256-bit read-only loads (ld.global.nc.v4.f64, sm_100) for the
 // thread-per-point gathers of the D and I passes: a 32-byte q row in one
 // load, a 64-byte dq row in two.  R4 rows and dq rows are 32-byte aligned.
