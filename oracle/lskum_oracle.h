@@ -2,9 +2,9 @@
  * CPU oracle for the meshfree LSKUM 2-D Euler pseudo-time loop.
  *
  * TEST INFRASTRUCTURE ONLY.  This is a plain-C, FP64 restatement of the
- * reference primal solver (src_mpi_primal/*.F90 of Nischay-Pro/mfcfd), one
- * function per reference routine, same loop order and same expression
- * association.  Only tests/, __graft_entry__.smoke() and the CPU-baseline leg
+ * reference primal solver (the .F90 files of src_mpi_primal in
+ * Nischay-Pro/mfcfd), one function per reference routine, same loop order
+ * and same expression association.  Only tests/, __graft_entry__.smoke() and the CPU-baseline leg
  * of bench.py may call it, and only as the checker or the timed CPU baseline.
  * The product library never links or calls it.
  *
