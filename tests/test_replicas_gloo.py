@@ -44,7 +44,8 @@ def _rank(rank, world, port, out):
 
 def test_two_gloo_ranks_shard_and_reduce():
     world = 2
-    with mp.Manager() as mgr:
+    # spawn, not fork: the test process may already hold CUDA or other threads
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.spawn(_rank, args=(world, _free_port(), out), nprocs=world, join=True)
         r0, r1 = dict(out[0]), dict(out[1])
