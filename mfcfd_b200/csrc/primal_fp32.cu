@@ -55,7 +55,8 @@ __device__ __forceinline__ void stf8(float *p, const float a[4], const float b[4
 
 // eval_q_derivatives (q_variables.F90:41-112) with FP32 sums and the
 // precomputed inverse normal matrix, and func_delta (state_update.F90:190-236)
-// in FP64 from the coordinates.
+// with each neighbour's distance from the slot's FP32 offset (FP32 geometry,
+// read anyway) and the division and minimum in FP64.
 __device__ __forceinline__ void
 grad32_point(const Geom &g, const Consts &c, const Geom32 &f, const float4 *__restrict__ q,
              const double *__restrict__ spd, float *__restrict__ dq, float *__restrict__ qm,
@@ -65,8 +66,6 @@ grad32_point(const Geom &g, const Consts &c, const Geom32 &f, const float4 *__re
     float qmax[4] = {qi[0], qi[1], qi[2], qi[3]};
     float qmin[4] = {qi[0], qi[1], qi[2], qi[3]};
     float sx[4] = {0.f, 0.f, 0.f, 0.f}, sy[4] = {0.f, 0.f, 0.f, 0.f};
-    double2 pi_ = make_double2(0.0, 0.0);
-    if (with_delta) pi_ = g.xy[i];
     double min_delt = 1.0;
     const int nb = g.nbhs[i];
     for (int r = 0; r < nb; ++r) {
@@ -88,9 +87,8 @@ grad32_point(const Geom &g, const Consts &c, const Geom32 &f, const float4 *__re
             sy[m] = sy[m] + wdy * dqm;
         }
         if (with_delta) {
-            const double2 pk = g.xy[k];
-            const double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
-            double delta_t = sqrt(delx * delx + dely * dely) / spd[k];
+            const double dist = (double)sqrtf(d.x * d.x + d.y * d.y);
+            double delta_t = dist / spd[k];
             delta_t = c.cfl * delta_t;
             if (min_delt > delta_t) min_delt = delta_t;
         }
