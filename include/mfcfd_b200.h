@@ -236,10 +236,13 @@ long long mfcfd_launch_count(mfcfd_t *h);
  * per-device array of MFCFD_NOALLOC_MAX_ITERS doubles (512 KiB, held by every
  * GPU that loads the library until exit), launches the kernels directly and
  * allocates nothing.  Same arguments, results and status codes as mfcfd_run;
- * n_iters above MFCFD_NOALLOC_MAX_ITERS gives MFCFD_ERR_ARG.  The first call
- * on a device looks up the array's device address: make it before any
- * stream capture.  All calls on a device share the array, so calls that
- * overlap on the GPU (handles on concurrent streams) race on it. */
+ * n_iters above MFCFD_NOALLOC_MAX_ITERS gives MFCFD_ERR_ARG.  The array's
+ * device address is looked up by mfcfd_create, with the handle's device
+ * current (the first create on a device loads the library's module there,
+ * which places the array); the call itself runs on the handle's device
+ * whatever device the caller has current.  All calls on a device share the
+ * array, so calls that overlap on the GPU (handles on concurrent streams)
+ * race on it. */
 int mfcfd_run_noalloc(mfcfd_t *h, int it_first, int n_iters, double *residue, int *n_done);
 
 /* Runs iteration `it` with a CUDA event after every kernel on the handle's

@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <deque>
+#include <mutex>
 #include <new>
 #include <string>
 #include <thread>
@@ -580,6 +581,56 @@ int lskum_host::prepare_grid(const mfcfd_grid &G, const mfcfd_params &P, HostGri
     return MFCFD_OK;
 }
 
+// ---------------------------------------------------------------------------
+// The fixed residue-history array of mfcfd_run_noalloc.
+//
+// mfcfd_run keeps each call's residue history in a device buffer that it
+// grows with cudaMalloc when a call asks for more iterations than any call
+// before, and it instantiates CUDA graphs.  Callers that must not allocate
+// device memory once they are running -- a Fortran/OpenACC host whose device
+// memory belongs to its own pool, a time-critical service that allocates
+// only at start-up -- use mfcfd_run_noalloc instead, which keeps the history
+// in this array.
+//
+// In host code the array's name is a host-side stand-in, not a device
+// address.  Its address on a device is taken with cudaGetSymbolAddress, with
+// that device current, once per device: by the first mfcfd_create on the
+// device (set-up time, when the caller allows allocation; the lookup also
+// loads this file's module on the device, which places the array).  The
+// address is kept in every handle made on the device.
+namespace {
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+__device__ __align__(256) double g_noalloc_hist[MFCFD_NOALLOC_MAX_ITERS];
+
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+
+// Called by mfcfd_create with h->dev current.  A failed lookup does not fail
+// the create (mfcfd_run does not need the array); mfcfd_run_noalloc reports
+// it instead.
+void noalloc_resolve(mfcfd_t *h) {
+    h->noalloc_hist = nullptr;
+    if (h->dev < 0 || h->dev >= NOALLOC_MAX_DEVICES) {
+        h->noalloc_err = "mfcfd_run_noalloc: device index out of range";
+        return;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[h->dev]) {
+        double *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&p), g_noalloc_hist);
+        if (e != cudaSuccess) {
+            h->noalloc_err = std::string("cudaGetSymbolAddress(g_noalloc_hist): ") +
+                             cudaGetErrorString(e);
+            return;
+        }
+        g_noalloc_ptr[h->dev] = p;
+    }
+    h->noalloc_hist = g_noalloc_ptr[h->dev];
+}
+
+}  // namespace
+
 extern "C" {
 
 int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **out) {
@@ -626,6 +677,7 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
     h->right0.assign(G.right, G.right + n);
     h->flag2_0.assign(G.flag_2, G.flag_2 + n);
     cudaGetDevice(&h->dev);
+    noalloc_resolve(h);
     h->pi = hg.pi;
     h->theta = hg.theta;
     h->cos_t = hg.cos_t;
@@ -925,6 +977,9 @@ int mfcfd_run(mfcfd_t *h, int it_first, int n_iters, double *residue, int *n_don
     if (n_done) *n_done = 0;
     if (!h || n_iters < 0) return MFCFD_ERR_ARG;
     if (n_iters == 0) return MFCFD_OK;
+    // the history buffer and the graphs belong on the handle's device
+    DevGuard dg(h->dev);
+    CK(dg.err);
     if (n_iters > h->hist_cap) {
         if (h->d_hist) cudaFree(h->d_hist);
         h->d_hist = nullptr;
@@ -1140,51 +1195,12 @@ const char *mfcfd_last_error(mfcfd_t *h) {
 
 // ---------------------------------------------------------------------------
 // mfcfd_run_noalloc: the pseudo-time loop without any device allocation.
-//
-// mfcfd_run keeps each call's residue history in a device buffer that it
-// grows with cudaMalloc when a call asks for more iterations than any call
-// before, and it instantiates CUDA graphs.  Callers that must not allocate
-// device memory once they are running -- a Fortran/OpenACC host whose device
-// memory belongs to its own pool, a time-critical service that
-// allocates only at start-up -- use this entry point instead.  It keeps the
-// history in the fixed array below, launches the same kernels directly, and
-// calls no cudaMalloc, cudaFree or graph instantiation.
-//
-// The array is a host-side stand-in in host code: its device address is
-// taken with cudaGetSymbolAddress once per device, with that device current,
-// on the first call made on that device.  Make that first call before any
-// stream capture.  Every call on a device shares the array: each iteration
-// writes its history entry before anything reads it, and calls that overlap
-// on the GPU (two handles on concurrent streams) race on it.
-namespace {
-
-constexpr int NOALLOC_MAX_DEVICES = 64;
-__device__ __align__(256) double g_noalloc_hist[MFCFD_NOALLOC_MAX_ITERS];
-double *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
-
-int noalloc_setup(mfcfd_t *h, double **out) {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGetDevice");
-    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
-        return fail(h, MFCFD_ERR_NODEV, "mfcfd_run_noalloc: device index out of range");
-    if (!g_noalloc_ptr[dev]) {
-        double *p = nullptr;
-        e = cudaGetSymbolAddress(reinterpret_cast<void **>(&p), g_noalloc_hist);
-        if (e != cudaSuccess) return cuda_fail(h, e, "cudaGetSymbolAddress(g_noalloc_hist)");
-        g_noalloc_ptr[dev] = p;
-    }
-    *out = g_noalloc_ptr[dev];
-    return MFCFD_OK;
-}
-
-// One iteration, as mfcfd_run enqueues it, with the history written to `hist`.
-int noalloc_iteration(mfcfd_t *h, cudaStream_t s, double *hist) {
-    return enqueue_iteration_to(h, s, hist);
-}
-
-}  // namespace
-
+// It launches the same kernels as mfcfd_run, one iteration after another
+// (no graph instantiation), with the history written to the array above,
+// whose address mfcfd_create resolved.  Every call on a device shares the
+// array: each iteration writes its history entry before anything reads it,
+// and calls that overlap on the GPU (two handles on concurrent streams) race
+// on it.
 extern "C" int mfcfd_run_noalloc(mfcfd_t *h, int it_first, int n_iters, double *residue,
                                  int *n_done) {
     if (n_done) *n_done = 0;
@@ -1194,15 +1210,14 @@ extern "C" int mfcfd_run_noalloc(mfcfd_t *h, int it_first, int n_iters, double *
                     "mfcfd_run_noalloc: n_iters exceeds MFCFD_NOALLOC_MAX_ITERS (65536); "
                     "split the run into several calls");
     if (n_iters == 0) return MFCFD_OK;
-    double *hist = nullptr;
-    int st = noalloc_setup(h, &hist);
-    if (st) return st;
+    double *hist = h->noalloc_hist;
+    if (!hist) return fail(h, MFCFD_ERR_CUDA, h->noalloc_err);
+    DevGuard dg(h->dev);
+    CK(dg.err);
     CK(cudaStreamSynchronize(h->stream));
-    if ((st = lskum_host::reset_run(h, it_first))) return st;
-    for (int k = 0; k < n_iters; ++k) {
-        st = noalloc_iteration(h, h->stream, hist);
-        if (st) return st;
-    }
+    if (int st = lskum_host::reset_run(h, it_first)) return st;
+    for (int k = 0; k < n_iters; ++k)
+        if (int st = enqueue_iteration_to(h, h->stream, hist)) return st;
     CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     const int done = h->h_ctl->done;

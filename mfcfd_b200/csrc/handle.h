@@ -73,6 +73,11 @@ struct mfcfd {
     std::string err;
     std::vector<double> shape_cp;
     AdjointState *adj = nullptr;
+    // device address of the fixed residue-history array of mfcfd_run_noalloc
+    // on this handle's device, resolved by mfcfd_create (nullptr if that
+    // lookup failed; noalloc_err then says why)
+    double *noalloc_hist = nullptr;
+    std::string noalloc_err;
     // caller-order ring neighbours of every point (for the adjoint set-up)
     std::vector<int> left0, right0, flag2_0;
 };
@@ -111,6 +116,25 @@ inline cudaError_t dmalloc(T **p, size_t count) {
     return cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T) + (count == 0 ? 16 : 0));
 }
 }  // namespace lskum_host
+
+// Makes `dev` the calling thread's current device for the scope of a call
+// and gives the caller's device back afterwards, so that a handle's work
+// (allocations, launches, symbol lookups) lands on the handle's own GPU
+// whatever device the caller has current.
+struct DevGuard {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DevGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) err = cudaSetDevice(dev);
+    }
+    ~DevGuard() {
+        int now = -1;
+        if (prev >= 0 && cudaGetDevice(&now) == cudaSuccess && now != prev) cudaSetDevice(prev);
+    }
+    DevGuard(const DevGuard &) = delete;
+    DevGuard &operator=(const DevGuard &) = delete;
+};
 
 #define CK(call)                                                                   \
     do {                                                                           \

@@ -3,10 +3,11 @@
 A caller whose device memory belongs to its own pool, or a service that
 allocates only at start-up, cannot let the library call cudaMalloc while it
 runs; mfcfd_run_noalloc keeps its scratch (the residue history) in a fixed
-per-device array instead.  These checks call it through the C ABI and compare
-it with mfcfd_run on an identical solver, on two calls in a row.  The file is
-collected last so that a run stopping at the first failure has already run
-every other test.
+per-device array instead, whose address mfcfd_create looks up.  These checks
+call it through the C ABI and compare it with mfcfd_run on an identical
+solver, on two calls in a row, and check that the two calls leave the
+device's free memory unchanged.  The file is collected last so that a run
+stopping at the first failure has already run every other test.
 """
 import ctypes as C
 
@@ -16,7 +17,6 @@ import pytest
 from mfcfd_b200 import _lib
 from mfcfd_b200.grid import naca_ogrid
 from mfcfd_b200.solver import Solver
-from tests.helpers import max_rel
 
 pytestmark = pytest.mark.gpu
 
@@ -29,20 +29,30 @@ def _run_noalloc(s, it_first, n):
     return st, res[:done.value]
 
 
+def _free_bytes():
+    import torch
+    torch.cuda.synchronize()
+    return torch.cuda.mem_get_info(0)[0]
+
+
 def test_run_noalloc_matches_run_on_two_calls(gpu):
     g = naca_ogrid(48, 20, seed=41, first_spacing=5e-3)
     flow = dict(cfl=0.2, vl_const=5.0, mach=0.7, aoa=1.5, inner_iterations=2)
+    calls = ((1, 7), (8, 5))  # two calls in a row; the shared array keeps the first's history
     with Solver(g, **flow) as a, Solver(g, **flow) as b:
-        it = 1
-        for n in (7, 5):  # two calls in a row; the shared array keeps the first call's history
+        ref = []
+        for it, n in calls:
             ra = a.run(n, it_first=it)
+            ref.append((ra, a.get_state()))
+        free0 = _free_bytes()
+        for (it, n), (ra, pa) in zip(calls, ref):
             st, rb = _run_noalloc(b, it, n)
             assert st == _lib.MFCFD_OK, b.lib.mfcfd_last_error(b.h)
+            # same kernels in the same order on the same inputs: identical bits
             assert len(rb) == len(ra) == n
-            # same kernels in the same order: results agree to the parity tolerance
-            assert np.allclose(rb, ra, rtol=0, atol=1e-12)
-            assert max_rel(b.get_state(), a.get_state()) < 1e-12
-            it += n
+            assert np.array_equal(rb, ra)
+            assert np.array_equal(b.get_state(), pa)
+            assert _free_bytes() == free0, "mfcfd_run_noalloc changed the device's free memory"
 
 
 def test_run_noalloc_rejects_oversized_runs(gpu):
