@@ -3,7 +3,9 @@
 
     python -m mfcfd_b200.driver CASE_DIR
 
-reads CASE_DIR/case.in (or input.nml), the grid CASE_DIR/point/partGrid,
+reads CASE_DIR/case.in (or input.nml), the grid CASE_DIR/point/point.h5
+(group /1, the reference's reader: point_preprocessor.F90:177-546; the legacy
+text CASE_DIR/point/partGrid when there is no point.h5),
 optionally CASE_DIR/restart/sol.dat, runs max_iters iterations on the GPU and
 writes CASE_DIR/residue, CASE_DIR/cp/cp-file, every nsave iterations
 CASE_DIR/solution/sol.dat, and at the end the CUDA tree's CASE_DIR/output.dat
@@ -17,8 +19,17 @@ import os
 import sys
 import time
 
-from . import io
+from . import io, pointh5
 from .solver import Solver
+
+
+def read_case_grid(case_dir: str, shapes: int = 1):
+    """The case's grid: point/point.h5 as the reference reads it, else the
+    legacy point/partGrid."""
+    h5 = os.path.join(case_dir, "point", "point.h5")
+    if os.path.exists(h5):
+        return pointh5.read_grid_h5(h5, shapes=shapes)
+    return io.read_partgrid(os.path.join(case_dir, "point", "partGrid"), shapes=shapes)
 
 
 def run_case(case_dir: str, grid=None, quiet: bool = False, chunk: int = 100) -> dict:
@@ -27,8 +38,7 @@ def run_case(case_dir: str, grid=None, quiet: bool = False, chunk: int = 100) ->
         os.path.join(case_dir, "input.nml"))
     params = io.solver_params(opts)
     if grid is None:
-        grid = io.read_partgrid(os.path.join(case_dir, "point", "partGrid"),
-                                shapes=int(opts["shapes"]))
+        grid = read_case_grid(case_dir, shapes=int(opts["shapes"]))
     itr, res_old = 0, 0.0
     prim0 = None
     if params["restart"]:
