@@ -38,11 +38,20 @@ _INT_KEYS = {"max_iters", "inner_iterations", "interior_points_normal_flag", "sh
 _REAL_KEYS = {"cfl", "mach", "aoa", "tfinal", "power", "vl_const"}
 
 
-def _convert(key, value):
-    if key in _INT_KEYS:
-        return int(float(value))
-    if key in _REAL_KEYS:
-        return float(value.replace("d", "e").replace("D", "e"))
+class FormatError(ValueError):
+    """An input file (case.in, input.nml, partGrid, restart sol.dat) that does
+    not parse: the message names the file, the line or option, and what was
+    wrong.  The reference's Fortran reads stop the run on the same inputs."""
+
+
+def _convert(key, value, where=""):
+    try:
+        if key in _INT_KEYS:
+            return int(float(value.replace("d", "e").replace("D", "e")))
+        if key in _REAL_KEYS:
+            return float(value.replace("d", "e").replace("D", "e"))
+    except ValueError:
+        raise FormatError(f"{where}option -{key}: {value!r} is not a number") from None
     return value.strip().strip("'\"")
 
 
@@ -60,11 +69,11 @@ def read_case(path: str) -> dict:
     while i < len(tokens):
         t = tokens[i]
         if not t.startswith("-"):
-            raise ValueError(f"{path}: expected an option, got {t!r}")
+            raise FormatError(f"{path}: expected an option, got {t!r}")
         key = t.lstrip("-")
         nxt = tokens[i + 1] if i + 1 < len(tokens) else None
         if nxt is not None and (not nxt.startswith("-") or re.match(r"^-[\d.]", nxt)):
-            opts[key] = _convert(key, nxt)
+            opts[key] = _convert(key, nxt, f"{path}: ")
             i += 2
         else:
             opts[key] = True
@@ -80,9 +89,9 @@ def read_nml(path: str) -> dict:
         text = fh.read()
     m = re.search(r"&\s*input_parameters(.*?)/", text, re.S | re.I)
     if not m:
-        raise ValueError(f"{path}: no &input_parameters group")
+        raise FormatError(f"{path}: no &input_parameters group")
     for key, value in re.findall(r"(\w+)\s*=\s*('[^']*'|\"[^\"]*\"|[^,\n]+)", m.group(1)):
-        opts[key.lower()] = _convert(key.lower(), value.strip().rstrip(","))
+        opts[key.lower()] = _convert(key.lower(), value.strip().rstrip(","), f"{path}: ")
     return opts
 
 
@@ -159,32 +168,57 @@ def write_partgrid(grid: Grid, path: str) -> None:
                      f"{int(grid.flag_2[k])} {float(grid.min_dist[k])!r} {nb} {conn}\n")
 
 
+def _numbers(path, lineno, tokens, kinds):
+    """Converts the leading tokens of a line to the given kinds (int/float)."""
+    if len(tokens) < len(kinds):
+        raise FormatError(f"{path}: line {lineno}: {len(tokens)} values, expected at least "
+                          f"{len(kinds)}")
+    out = []
+    for tok, kind in zip(tokens, kinds):
+        try:
+            out.append(kind(tok.replace("D", "E").replace("d", "e")) if kind is float
+                       else int(tok))
+        except ValueError:
+            raise FormatError(f"{path}: line {lineno}: {tok!r} is not "
+                              f"{'a number' if kind is float else 'an integer'}") from None
+    return out
+
+
 def read_partgrid(path: str, shapes: int = 1) -> Grid:
     with open(path) as fh:
         head = fh.readline().split()
-        nproc, max_points, local_points, ghost_points = (int(x) for x in head[:4])
+        nproc, max_points, local_points, ghost_points = _numbers(path, 1, head, (int,) * 4)
         if nproc != 1:
-            raise ValueError("check number of partitions and proc (single-rank reader)")
+            raise FormatError(f"{path}: check number of partitions and proc (single-rank "
+                              f"reader, file has {nproc})")
+        if local_points < 0 or ghost_points < 0 or max_points < local_points:
+            raise FormatError(f"{path}: line 1: inconsistent point counts {head[:4]}")
         n = local_points
         x = np.zeros(n); y = np.zeros(n); md = np.zeros(n)
         left = np.zeros(n, np.int32); right = np.zeros(n, np.int32)
         f1 = np.zeros(n, np.int32); f2 = np.zeros(n, np.int32)
         nbhs = np.zeros(n, np.int32); oid = np.zeros(n, np.int32)
         conn = np.zeros((MAX_NBHS, n), np.int32)
+        kinds = (int, float, float, int, int, int, int, float, int)
         for k in range(n):
-            t = fh.readline().split()
-            if len(t) < 9:
-                raise ValueError(f"{path}: short row {k + 1}")
-            oid[k] = int(t[0]); x[k] = float(t[1]); y[k] = float(t[2])
-            left[k] = int(t[3]); right[k] = int(t[4]); f1[k] = int(t[5]); f2[k] = int(t[6])
-            md[k] = float(t[7]); nb = int(t[8]); nbhs[k] = nb
-            if nb > MAX_NBHS or len(t) < 9 + nb:
-                raise ValueError(f"{path}: bad stencil on row {k + 1}")
-            conn[:nb, k] = [int(v) for v in t[9:9 + nb]]
+            line = fh.readline()
+            if not line:
+                raise FormatError(f"{path}: truncated after {k} of {n} point rows")
+            t = line.split()
+            v = _numbers(path, k + 2, t, kinds)
+            oid[k], x[k], y[k], left[k], right[k], f1[k], f2[k], md[k], nb = v
+            nbhs[k] = nb
+            if nb < 0 or nb > MAX_NBHS or len(t) < 9 + nb:
+                raise FormatError(f"{path}: line {k + 2}: bad stencil (nbhs {nb}, "
+                                  f"{len(t) - 9} indices)")
+            conn[:nb, k] = _numbers(path, k + 2, t[9:9 + nb], (int,) * nb)
     g = Grid(x=x, y=y, nx=np.zeros(n), ny=np.ones(n), min_dist=md, flag_1=f1, flag_2=f2,
              left=left, right=right, nbhs=nbhs, conn=conn, original_id=oid,
              qtdepth=np.zeros(n, np.int32), shapes=shapes, name=os.path.basename(path))
-    g.validate()
+    try:
+        g.validate()
+    except ValueError as e:
+        raise FormatError(f"{path}: {e}") from None
     return g
 
 
@@ -248,15 +282,17 @@ def read_restart(path: str, n: int):
     output.dat (prim in columns 5-8)."""
     with open(path) as fh:
         head = fh.readline().split()
-        itr = int(float(head[1]))
-        res_old = float(head[2].replace("D", "E").replace("d", "e"))
+        _, itr, res_old = _numbers(path, 1, head, (int, float, float))
         prim = np.zeros((n, 4))
         for i in range(n):
-            t = fh.readline().split()
+            line = fh.readline()
+            if not line:
+                raise FormatError(f"{path}: truncated after {i} of {n} point rows")
+            t = line.split()
             if len(t) == 9:
-                prim[i] = [float(v) for v in t[5:9]]
+                prim[i] = _numbers(path, i + 2, t[5:9], (float,) * 4)
             elif len(t) == 11:
-                prim[i] = [float(v) for v in t[4:8]]
+                prim[i] = _numbers(path, i + 2, t[4:8], (float,) * 4)
             else:
-                raise ValueError(f"{path}: row {i + 2} has {len(t)} values (want 9 or 11)")
-    return itr, res_old, prim
+                raise FormatError(f"{path}: line {i + 2} has {len(t)} values (want 9 or 11)")
+    return int(itr), res_old, prim

@@ -79,3 +79,73 @@ def test_residue_and_cp_files(tmp_path):
     rows = [r.split() for r in (tmp_path / "cp" / "cp-file").read_text().splitlines()]
     assert len(rows) == cp.size and int(rows[0][0]) == 1
     assert np.allclose([float(r[2]) for r in rows], cp, rtol=0, atol=1e-15)
+
+
+# --- garbled and truncated inputs: each reader stops with io.FormatError ---
+
+def test_garbled_partgrid_is_rejected(tmp_path):
+    import pytest
+    g = naca_ogrid(16, 6, seed=4)
+    path = tmp_path / "partGrid"
+    io.write_partgrid(g, str(path))
+    lines = path.read_text().splitlines(keepends=True)
+    cases = {
+        "header_short": ["1 96 96\n"] + lines[1:],
+        "header_text": ["one 96 96 0\n"] + lines[1:],
+        "two_ranks": ["2 96 96 0\n"] + lines[1:],
+        "counts": ["1 10 96 0\n"] + lines[1:],
+        "truncated": lines[:40],
+        "row_text": lines[:5] + [lines[5].replace(lines[5].split()[1], "x.y", 1)] + lines[6:],
+        "row_short": lines[:7] + ["7 0.1 0.2 0 0\n"] + lines[8:],
+        "stencil": lines[:9] + [" ".join(lines[9].split()[:8] + ["25"]) + "\n"] + lines[10:],
+        "conn_range": lines[:3] + [" ".join(lines[3].split()[:9] + ["999"] * int(lines[3].split()[8]))
+                                   + "\n"] + lines[4:],
+    }
+    for name, text in cases.items():
+        p = tmp_path / f"pg_{name}"
+        p.write_text("".join(text))
+        with pytest.raises(io.FormatError, match=str(p)):
+            io.read_partgrid(str(p))
+
+
+def test_garbled_restart_is_rejected(tmp_path):
+    import pytest
+    g = naca_ogrid(16, 6, seed=4)
+    prim = np.tile([1.0, 0.5, 0.0, 1 / 1.4], (g.n, 1))
+    path = tmp_path / "sol.dat"
+    io.write_solution(str(path), g, prim, 11, 1e-3)
+    it, res_old, back = io.read_restart(str(path), g.n)
+    assert it == 10 and res_old == 1e-3 and np.array_equal(back, prim)
+    lines = path.read_text().splitlines(keepends=True)
+    cases = {
+        "header_text": ["96 ten 1e-3\n"] + lines[1:],
+        "truncated": lines[:50],
+        "row_width": lines[:4] + [" ".join(lines[4].split()[:7]) + "\n"] + lines[5:],
+        "row_text": lines[:4] + [lines[4].replace(lines[4].split()[6], "nanx", 1)] + lines[5:],
+    }
+    for name, text in cases.items():
+        p = tmp_path / f"sol_{name}.dat"
+        p.write_text("".join(text))
+        with pytest.raises(io.FormatError, match=str(p)):
+            io.read_restart(str(p), g.n)
+
+
+def test_garbled_case_files_are_rejected(tmp_path):
+    import pytest
+    bad = {
+        "value": "-cfl fast\n-max_iters 10\n",
+        "int": "-inner_iterations three\n",
+        "token": "cfl 0.2\n",
+    }
+    for name, text in bad.items():
+        p = tmp_path / f"case_{name}.in"
+        p.write_text(text)
+        with pytest.raises(io.FormatError, match=str(p)):
+            io.read_case(str(p))
+    p = tmp_path / "input.nml"
+    p.write_text("&other_group\n cfl = 0.2\n/\n")
+    with pytest.raises(io.FormatError, match="no &input_parameters"):
+        io.read_nml(str(p))
+    p.write_text("&input_parameters\n cfl = abc\n/\n")
+    with pytest.raises(io.FormatError, match="-cfl"):
+        io.read_nml(str(p))
