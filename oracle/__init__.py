@@ -47,7 +47,12 @@ def _lib(variant: str = "") -> C.CDLL:
     lib.orc_create.restype = P
     lib.orc_create.argtypes = [C.c_int, D, D, D, D, D, I, I, I, I, I, I, C.c_int,
                                C.POINTER(OrcParams)]
+    lib.orc_create_part.restype = P
+    lib.orc_create_part.argtypes = [C.c_int, C.c_int, C.c_int, D, D, D, D, D, I, I, I, I, I,
+                                    I, C.c_int, C.POINTER(OrcParams)]
     lib.orc_destroy.argtypes = [P]
+    lib.orc_set.argtypes = [P, C.c_char_p, D]
+    lib.orc_set.restype = C.c_int
     for fn in ("orc_init_freestream", "orc_func_delta", "orc_eval_q_variables",
                "orc_eval_q_derivatives", "orc_eval_q_inner_loop",
                "orc_eval_update_innerloop", "orc_cal_flux_residual", "orc_save_prim_old"):
@@ -89,7 +94,10 @@ class Oracle:
 
     def __init__(self, grid, cfl=0.2, power=0.0, vl_const=5.0, mach=0.63, aoa=2.0,
                  tscheme="ssprk43", inner_iterations=0, interior_points_normal_flag=0,
-                 format=1, restart=0, res_old=0.0, variant=""):
+                 format=1, restart=0, res_old=0.0, variant="", n_local=None, plen=None):
+        """n_local / plen: one rank's part of a partitioned grid -- points
+        beyond n_local are ghosts (refreshed by the caller with ``put``), and
+        the residual norm divides by plen, the global point count."""
         self.lib = _lib(variant)
         self.grid = grid
         self.n = grid.n
@@ -102,9 +110,12 @@ class Oracle:
                       (g.x, g.y, g.nx, g.ny, g.min_dist, g.flag_1, g.flag_2, g.left,
                        g.right, g.nbhs, g.conn)]
         k = self._keep
-        self.h = self.lib.orc_create(self.n, _d(k[0]), _d(k[1]), _d(k[2]), _d(k[3]),
-                                     _d(k[4]), _i(k[5]), _i(k[6]), _i(k[7]), _i(k[8]),
-                                     _i(k[9]), _i(k[10]), self.n, C.byref(self.params))
+        self.n_local = self.n if n_local is None else int(n_local)
+        self.h = self.lib.orc_create_part(self.n, self.n_local,
+                                          self.n if plen is None else int(plen),
+                                          _d(k[0]), _d(k[1]), _d(k[2]), _d(k[3]),
+                                          _d(k[4]), _i(k[5]), _i(k[6]), _i(k[7]), _i(k[8]),
+                                          _i(k[9]), _i(k[10]), self.n, C.byref(self.params))
 
     def close(self):
         if getattr(self, "h", None):
@@ -128,6 +139,12 @@ class Oracle:
         if self.lib.orc_get(self.h, name.encode(), _d(out)) != 0:
             raise KeyError(name)
         return out.reshape(self.n, -1) if _SIZES[name] > 1 else out
+
+    def put(self, name, values):
+        """Copies a whole array in ("prim" (n,4), "dq" / "qm" (n,8))."""
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        if self.lib.orc_set(self.h, name.encode(), _d(a)) != 0:
+            raise KeyError(name)
 
     def split_counts(self):
         out = np.empty((self.n, 4), dtype=np.int32)

@@ -35,6 +35,8 @@ static const double GAMMA = 1.4;
 
 struct orc {
     int n, ldconn;
+    int n_local;  /* owned points (local_points); points n_local+1..n are ghosts */
+    int plen;     /* points in the residual norm (all ranks' owned points) */
     orc_params p;
     double pi, theta, q_inf[4];
     double *x, *y, *nx, *ny, *min_dist;
@@ -157,8 +159,23 @@ orc_t *orc_create(int n, const double *x, const double *y, const double *nx,
                   const int *flag_2, const int *left, const int *right,
                   const int *nbhs, const int *conn, int ldconn,
                   const orc_params *p) {
+    return orc_create_part(n, n, n, x, y, nx, ny, min_dist, flag_1, flag_2, left, right, nbhs,
+                           conn, ldconn, p);
+}
+
+/* One rank's part of a partitioned point set (point_preprocessor.F90:177-546,
+ * petsc_data_structure.F90:21-54): points 1..n_local are owned, the rest are
+ * ghosts whose prim, dq and qm the caller refreshes between phases; plen is
+ * the global point count of the residual norm. */
+orc_t *orc_create_part(int n, int n_local, int plen, const double *x, const double *y,
+                       const double *nx, const double *ny, const double *min_dist,
+                       const int *flag_1, const int *flag_2, const int *left,
+                       const int *right, const int *nbhs, const int *conn, int ldconn,
+                       const orc_params *p) {
     orc_t *h = (orc_t *)calloc(1, sizeof(orc_t));
     h->n = n;
+    h->n_local = n_local;
+    h->plen = plen;
     h->ldconn = ldconn;
     h->p = *p;
     size_t nd = (size_t)n * sizeof(double), ni = (size_t)n * sizeof(int);
@@ -177,7 +194,7 @@ orc_t *orc_create(int n, const double *x, const double *y, const double *nx,
     /* point_preprocessor.F90:374-435: type counts and index lists */
     h->wall_idx = malloc(ni); h->outer_idx = malloc(ni);
     h->interior_idx = malloc(ni); h->shape_idx = malloc(ni);
-    for (int k = 1; k <= n; ++k) {
+    for (int k = 1; k <= n_local; ++k) {
         int f = flag_1[k - 1];
         if (f == 0) h->wall_idx[h->wall_points++] = k;
         else if (f == 1) h->interior_idx[h->interior_points++] = k;
@@ -231,7 +248,7 @@ void orc_get_prim(const orc_t *h, double *prim) {
 }
 
 void orc_save_prim_old(orc_t *h) {
-    memcpy(h->prim_old, h->prim, (size_t)4 * h->n * sizeof(double));
+    memcpy(h->prim_old, h->prim, (size_t)4 * h->n_local * sizeof(double));
 }
 
 /* ------------------------------------------------------------------------ */
@@ -253,7 +270,7 @@ void orc_eval_q_variables(orc_t *h) {
 void orc_eval_q_derivatives(orc_t *h) {
     const double power = h->p.power;
 #pragma omp parallel for schedule(static)
-    for (int i = 1; i <= h->n; ++i) {
+    for (int i = 1; i <= h->n_local; ++i) {
         double x_i = X(i), y_i = Y(i);
         double sum_delx_sqr = 0.0, sum_dely_sqr = 0.0, sum_delx_dely = 0.0;
         double sum_delx_delq[4] = {0, 0, 0, 0}, sum_dely_delq[4] = {0, 0, 0, 0};
@@ -288,7 +305,7 @@ void orc_eval_q_derivatives(orc_t *h) {
 void orc_eval_q_inner_loop(orc_t *h) {
     const double power = h->p.power;
 #pragma omp parallel for schedule(static)
-    for (int i = 1; i <= h->n; ++i) {
+    for (int i = 1; i <= h->n_local; ++i) {
         double x_i = X(i), y_i = Y(i);
         double sum_delx_sqr = 0.0, sum_dely_sqr = 0.0, sum_delx_dely = 0.0;
         double sdx[4] = {0, 0, 0, 0}, sdy[4] = {0, 0, 0, 0};
@@ -320,7 +337,7 @@ void orc_eval_q_inner_loop(orc_t *h) {
 /* q_variables.F90:215-227 eval_update_innerloop */
 void orc_eval_update_innerloop(orc_t *h) {
 #pragma omp parallel for schedule(static)
-    for (int i = 1; i <= h->n; ++i)
+    for (int i = 1; i <= h->n_local; ++i)
         for (int r = 1; r <= 4; ++r) {
             DQ(1, r, i) = TMP(1, r, i);
             DQ(2, r, i) = TMP(2, r, i);
@@ -734,7 +751,7 @@ double orc_sum_res_sqr(const orc_t *h) { return h->sum_res_sqr; }
 void orc_func_delta(orc_t *h) {
     const double cfl = h->p.cfl;
 #pragma omp parallel for schedule(static)
-    for (int i = 1; i <= h->n; ++i) {
+    for (int i = 1; i <= h->n_local; ++i) {
         double min_delt = 1.0;
         for (int r = 1; r <= NBHS(i); ++r) {
             int k = CONN(i, r);
@@ -765,7 +782,7 @@ static void fpi_solver(orc_t *h, int t) {
         orc_cal_flux_residual(h);
         orc_state_update(h, rk);
     }
-    h->res_new = sqrt(h->sum_res_sqr) / h->n;
+    h->res_new = sqrt(h->sum_res_sqr) / h->plen;
     if (t <= 2 && h->p.restart == 0) {
         h->res_old = h->res_new;
         h->residue = 0.0;
@@ -942,6 +959,18 @@ int orc_get(const orc_t *h, const char *name, double *out) {
     else if (!strcmp(name, "temp")) { src = h->temp; cnt = 12 * n; }
     else return -1;
     memcpy(out, src, cnt * sizeof(double));
+    return 0;
+}
+
+int orc_set(orc_t *h, const char *name, const double *in) {
+    size_t n = (size_t)h->n;
+    double *dst = NULL;
+    size_t cnt = 0;
+    if (!strcmp(name, "prim")) { dst = h->prim; cnt = 4 * n; }
+    else if (!strcmp(name, "dq")) { dst = h->dq; cnt = 8 * n; }
+    else if (!strcmp(name, "qm")) { dst = h->qm; cnt = 8 * n; }
+    else return -1;
+    memcpy(dst, in, cnt * sizeof(double));
     return 0;
 }
 

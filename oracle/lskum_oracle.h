@@ -47,6 +47,15 @@ orc_t *orc_create(int n, const double *x, const double *y, const double *nx,
                   const int *flag_2, const int *left, const int *right,
                   const int *nbhs, const int *conn, int ldconn,
                   const orc_params *p);
+/* One rank's part of a partitioned point set: points 1..n_local are owned
+ * (local_points), n_local+1..n ghosts; loops the reference runs over
+ * local_points, and the point classification, skip the ghosts; plen is the
+ * global point count of the residual norm (fpi_solver.F90:57-63). */
+orc_t *orc_create_part(int n, int n_local, int plen, const double *x, const double *y,
+                       const double *nx, const double *ny, const double *min_dist,
+                       const int *flag_1, const int *flag_2, const int *left,
+                       const int *right, const int *nbhs, const int *conn, int ldconn,
+                       const orc_params *p);
 void orc_destroy(orc_t *h);
 
 /* freestream initial condition (initial_conditions.F90:9-42) */
@@ -90,6 +99,8 @@ double orc_objective(const orc_t *h, int kind);
 /* copies an internal array out: name is one of
  * "prim","prim_old","q","dq","qm","flux_res","delta","nx","ny","temp" */
 int orc_get(const orc_t *h, const char *name, double *out);
+/* copies an array in: "prim", "dq" or "qm" (ghost refresh of a partition) */
+int orc_set(orc_t *h, const char *name, const double *in);
 /* split-connectivity counts: out[4*(i-1)+d] for d = xpos,xneg,ypos,yneg */
 void orc_get_split_counts(const orc_t *h, int *out);
 int orc_num_threads(void);
