@@ -309,9 +309,11 @@ int mfcfd_batch_forces(mfcfd_batch_t *b, int inst, double *cl, double *cd, doubl
                        double *cp);
 
 /* Autotuner: times iters iterations (>= 2) of each candidate launch shape
- * (block size of the point passes; blocks of every grid-stride pass as 1, 2
- * or 4 waves of resident blocks, or one block per tile) on a copy of the
- * current state, keeps the fastest and restores the state.  Results do not
+ * (block size 256 or 128 of the point passes; blocks of every grid-stride
+ * pass as 1, 2 or 4 waves of resident blocks, or sized for 1, 2 or 4 points
+ * per thread of the point passes and 1, 2 or 4 two-tile chunks per warp of
+ * the flux pass) on a copy of the current state, keeps the fastest and
+ * restores the state.  Results do not
  * depend on the launch shape.  *ms_per_iter (may be NULL) gets the best time
  * per iteration. */
 int mfcfd_batch_tune(mfcfd_batch_t *b, int iters, double *ms_per_iter);

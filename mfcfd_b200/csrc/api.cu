@@ -790,9 +790,10 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
     // block per tile, which reloads the schedule in every block)
     h->inst_h = InstInfo{0, n, nw, no, 0, 0, flux_blocks(n), 0};
     h->sched = sched_view(h->d_inst, h->d_sched);
-    h->point_block = 256;
-    h->point_grid = std::min((n + 255) / 256, wave_blocks(h->dev, 0, 256, 0, h->fp32));
-    h->flux_grid = std::min(flux_blocks(n),
+    h->point_block = default_point_block(h->fp32);
+    h->point_grid = std::min((n + h->point_block - 1) / h->point_block,
+                             point_wave_blocks(h->dev, h->point_block, h->fp32));
+    h->flux_grid = std::min(flux_grid_blocks(n),
                             wave_blocks(h->dev, 2, 128,
                                         h->fp32 ? flux32_smem_bytes(kp) : flux_smem_bytes(kp),
                                         h->fp32));

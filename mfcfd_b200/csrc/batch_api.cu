@@ -151,24 +151,29 @@ void free_batch(mfcfd_batch_t *b) {
 
 // blocks in one wave of resident blocks of a batched pass
 int batch_wave(const mfcfd_batch_t *b, int kind, int block) {
+    if (kind == 0) return point_wave_blocks(b->dev, block, b->fp32);
     size_t smem = 0;
     if (kind == 2) smem = b->fp32 ? flux32_smem_bytes(b->kp) : flux_smem_bytes(b->kp);
     return wave_blocks(b->dev, kind, block, smem, b->fp32);
 }
 
-// Launch shape from (block, waves): waves 0 = one block per tile (flux) and
-// one thread per point (D/I passes).
-void set_shape(mfcfd_batch_t *b, int block, int waves) {
+// Launch shape from (block, waves) or (block, points per thread): waves > 0
+// sizes every pass to that many waves of resident blocks; otherwise ppt
+// (1, 2, 4) gives each thread of the point passes ppt points and each warp
+// of the flux pass ppt chunks of two tiles (ppt 1: every point its thread).
+void set_shape(mfcfd_batch_t *b, int block, int waves, int ppt = 1) {
     b->point_block = block;
+    const int fmax = flux_grid_blocks(b->ntiles * TILE);
     if (waves > 0) {
         b->point_grid = waves * batch_wave(b, 0, block);
         b->flux_grid = waves * batch_wave(b, 2, 128);
     } else {
-        b->point_grid = (b->ntot + block - 1) / block;
-        b->flux_grid = b->ntiles;
+        ppt = std::max(1, ppt);
+        b->point_grid = (b->ntot + block * ppt - 1) / (block * ppt);
+        b->flux_grid = (fmax + ppt - 1) / ppt;
     }
     b->point_grid = std::max(1, std::min(b->point_grid, (b->ntot + block - 1) / block));
-    b->flux_grid = std::max(1, std::min(b->flux_grid, b->ntiles));
+    b->flux_grid = std::max(1, std::min(b->flux_grid, fmax));
 }
 
 // One pseudo-time stage over all active instances (launch_stage of the
@@ -640,7 +645,7 @@ int mfcfd_batch_create(int n_inst, const mfcfd_grid *const *grids, const mfcfd_p
     // initial_conditions.F90:9-20: freestream everywhere
     for (int i = 0; i < n_inst; ++i)
         if ((st = upload_instance_state(b, i, nullptr))) goto fail_create;
-    set_shape(b, 256, 1);
+    set_shape(b, default_point_block(b->fp32), 1);
     *out = b;
     return MFCFD_OK;
 fail_create:
@@ -780,7 +785,7 @@ int mfcfd_batch_set_launch(mfcfd_batch_t *b, int point_block, int point_grid, in
     BK(cudaStreamSynchronize(b->stream));
     set_shape(b, point_block, 1);
     if (point_grid > 0) b->point_grid = std::min(point_grid, (b->ntot + point_block - 1) / point_block);
-    if (flux_grid > 0) b->flux_grid = std::min(flux_grid, b->ntiles);
+    if (flux_grid > 0) b->flux_grid = std::min(flux_grid, flux_grid_blocks(b->ntiles * TILE));
     drop_graphs(b);
     return MFCFD_OK;
 }
@@ -832,10 +837,13 @@ int mfcfd_batch_tune(mfcfd_batch_t *b, int iters, double *ms_per_iter) {
         if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
         if (e != cudaSuccess) st = bcuda(b, e, "tune set-up");
     }
-    const int blocks[2] = {256, 128}, waves[4] = {1, 2, 4, 0};
+    // candidates: 1, 2, 4 waves of resident blocks, and 1, 2, 4 points per
+    // thread (chunks per flux warp), for blocks of 256 and 128 threads
+    const int blocks[2] = {256, 128};
+    const int waves[6] = {1, 2, 4, 0, 0, 0}, ppts[6] = {0, 0, 0, 1, 2, 4};
     for (int bi = 0; bi < 2 && st == MFCFD_OK; ++bi)
-        for (int wi = 0; wi < 4 && st == MFCFD_OK; ++wi) {
-            set_shape(b, blocks[bi], waves[wi]);
+        for (int wi = 0; wi < 6 && st == MFCFD_OK; ++wi) {
+            set_shape(b, blocks[bi], waves[wi], ppts[wi]);
             drop_graphs(b);
             if ((st = restore())) break;
             for (int i = 0; i < b->n_inst; ++i) {

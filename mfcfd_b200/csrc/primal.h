@@ -115,17 +115,34 @@ void launch_residual(const InstInfo *inst, int n_inst, const double *res_part, C
                      cudaStream_t st);
 // One-time kernel attributes (before any stream capture).
 cudaError_t init_kernels();
-// tiles (flux blocks) of n points
+// tiles (TILE-point schedule units) of n points
 int flux_blocks(int n);
+// flux-pass blocks beyond which some warps would find no chunk of two tiles
+int flux_grid_blocks(int n);
 // resident blocks per SM (kind: 0 D pass, 1 I pass, 2 F pass; fp32 selects
 // the FP32-mixed kernels)
 int batch_occupancy(int kind, bool fp32, int block, size_t smem);
 int batch_occupancy32(int kind, int block, size_t smem);
+// dynamic shared memory of the D and I passes (their staging buffers) for
+// blocks of `block` threads
+size_t grad_smem_bytes(int block);
+size_t inner_smem_bytes(int block);
+size_t grad32_smem_bytes(int block);
+size_t inner32_smem_bytes(int block);
 // dynamic shared memory of the flux passes for stencils of kp slots
 size_t flux_smem_bytes(int kp);
 size_t flux32_smem_bytes(int kp);
-// blocks of one wave of resident blocks of a pass on device dev
+// blocks of one wave of resident blocks of a pass on device dev (for the
+// point passes the staging memory of `block` replaces `smem`)
 int wave_blocks(int dev, int kind, int block, size_t smem, bool fp32);
+// blocks of one wave of both point passes (D and I share their launch shape)
+inline int point_wave_blocks(int dev, int block, bool fp32) {
+    const int a = wave_blocks(dev, 0, block, 0, fp32), b = wave_blocks(dev, 1, block, 0, fp32);
+    return a < b ? a : b;
+}
+// threads per block of the point passes (their staging buffers take up to
+// 512 B of shared memory a thread)
+inline int default_point_block(bool) { return 128; }
 // q and spd from prim (set_state)
 void launch_init_state(const Geom &g, const R4 *prim, R4 *q, double *spd, cudaStream_t s);
 

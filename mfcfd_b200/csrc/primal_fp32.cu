@@ -22,11 +22,10 @@ namespace {
 
 constexpr int GRAD_BLOCK = 256;
 constexpr int LPP = 8;
-constexpr int FLUX_BLOCK = 128;
-constexpr int GROUPS = FLUX_BLOCK / LPP;
+constexpr int FLUX_BLOCK = 128;  // four independent warps
 constexpr int FREC = 9;   // dGxp..dGyn as 16 floats, then dels*w, deln*w (18 floats)
 #ifndef FLUX32_MIN_BLOCKS
-#define FLUX32_MIN_BLOCKS 8              // 64 registers: 32 warps per SM
+#define FLUX32_MIN_BLOCKS 6              // <= 80 registers; shared memory allows 6 blocks
 #endif
 constexpr double OBT = 1.0 / 3.0;
 constexpr double TBT = 2.0 / 3.0;
@@ -53,6 +52,34 @@ __device__ __forceinline__ void stf8(float *p, const float a[4], const float b[4
     v[1] = make_float4(b[0], b[1], b[2], b[3]);
 }
 
+// Staged neighbour gathers, as in the FP64 D and I passes: a thread copies
+// the rows of a round of stencil slots into its own shared-memory slots with
+// cp.async (no registers held while the copies fly), waits once, and sums in
+// slot order from shared memory.  16-byte units, thread-minor
+// (sb[unit * blockDim + thread]).  D pass units: the neighbour's q row, then
+// (slot offset dx dy, neighbour spd); I pass: the two halves of the
+// neighbour's dq row, then (slot offset, -).
+#ifndef STAGE32
+#define STAGE32 8    // slots per round, D pass
+#endif
+#ifndef STAGE32_I
+#define STAGE32_I 4  // slots per round, I pass
+#endif
+constexpr int UNITS32_D = 2;
+constexpr int UNITS32_I = 3;
+
+__device__ __forceinline__ void cp16(void *dst, const void *src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp8(void *dst, const void *src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // eval_q_derivatives (q_variables.F90:41-112) with FP32 sums and the
 // precomputed inverse normal matrix, and func_delta (state_update.F90:190-236)
 // with each neighbour's distance from the slot's FP32 offset (FP32 geometry,
@@ -60,7 +87,8 @@ __device__ __forceinline__ void stf8(float *p, const float a[4], const float b[4
 __device__ __forceinline__ void
 grad32_point(const Geom &g, const Consts &c, const Geom32 &f, const float4 *__restrict__ q,
              const double *__restrict__ spd, float *__restrict__ dq, float *__restrict__ qm,
-             double *__restrict__ delta, int with_delta, int i) {
+             double *__restrict__ delta, int with_delta, int i, float4 *sb) {
+    const int T = blockDim.x;
     const float4 qv = __ldg(q + i);
     const float qi[4] = {qv.x, qv.y, qv.z, qv.w};
     float qmax[4] = {qi[0], qi[1], qi[2], qi[3]};
@@ -68,29 +96,46 @@ grad32_point(const Geom &g, const Consts &c, const Geom32 &f, const float4 *__re
     float sx[4] = {0.f, 0.f, 0.f, 0.f}, sy[4] = {0.f, 0.f, 0.f, 0.f};
     double min_delt = 1.0;
     const int nb = g.nbhs[i];
-    for (int r = 0; r < nb; ++r) {
-        const int k = g.conn[r * g.n + i];
-        const float2 d = __ldg(f.dxy + r * g.n + i);
-        const float w = f.w ? __ldg(f.w + r * g.n + i) : 1.0f;
-        const float4 kv = __ldg(q + k);
-        const float qk[4] = {kv.x, kv.y, kv.z, kv.w};
+    for (int r0 = 0; r0 < nb; r0 += STAGE32) {
+        const int m = min(STAGE32, nb - r0);
+        int kk[STAGE32];
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            if (qk[m] > qmax[m]) qmax[m] = qk[m];
-            if (qk[m] < qmin[m]) qmin[m] = qk[m];
-        }
-        const float wdx = w * d.x, wdy = w * d.y;
+        for (int t = 0; t < STAGE32; ++t) kk[t] = t < m ? __ldg(g.conn + (r0 + t) * g.n + i) : 0;
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            const float dqm = qk[m] - qi[m];
-            sx[m] = sx[m] + wdx * dqm;
-            sy[m] = sy[m] + wdy * dqm;
+        for (int t = 0; t < STAGE32; ++t) {
+            if (t < m) {
+                float4 *d = sb + t * UNITS32_D * T;
+                cp16(d, q + kk[t]);
+                cp8(d + T, f.dxy + (r0 + t) * g.n + i);
+                if (with_delta) cp8(reinterpret_cast<char *>(d + T) + 8, spd + kk[t]);
+            }
         }
-        if (with_delta) {
-            const double dist = (double)sqrtf(d.x * d.x + d.y * d.y);
-            double delta_t = dist / spd[k];
-            delta_t = c.cfl * delta_t;
-            if (min_delt > delta_t) min_delt = delta_t;
+        cp_wait_all();
+        for (int t = 0; t < m; ++t) {
+            const float4 *d = sb + t * UNITS32_D * T;
+            const float4 kv = d[0], gs = d[T];
+            const float qk[4] = {kv.x, kv.y, kv.z, kv.w};
+            const int r = r0 + t;
+            const float w = f.w ? __ldg(f.w + r * g.n + i) : 1.0f;
+#pragma unroll
+            for (int mm = 0; mm < 4; ++mm) {
+                if (qk[mm] > qmax[mm]) qmax[mm] = qk[mm];
+                if (qk[mm] < qmin[mm]) qmin[mm] = qk[mm];
+            }
+            const float wdx = w * gs.x, wdy = w * gs.y;
+#pragma unroll
+            for (int mm = 0; mm < 4; ++mm) {
+                const float dqm = qk[mm] - qi[mm];
+                sx[mm] = sx[mm] + wdx * dqm;
+                sy[mm] = sy[mm] + wdy * dqm;
+            }
+            if (with_delta) {
+                const double sk = __hiloint2double(__float_as_int(gs.w), __float_as_int(gs.z));
+                const double dist = (double)sqrtf(gs.x * gs.x + gs.y * gs.y);
+                double delta_t = dist / sk;
+                delta_t = c.cfl * delta_t;
+                if (min_delt > delta_t) min_delt = delta_t;
+            }
         }
     }
     const float4 L = __ldg(f.lsq + i);
@@ -109,13 +154,15 @@ __global__ void __launch_bounds__(GRAD_BLOCK)
 kb_grad32(Geom g, Consts c, Geom32 f, Sched s, const float4 *__restrict__ q,
           const double *__restrict__ spd, float *__restrict__ dq, float *__restrict__ qm,
           double *__restrict__ delta, int with_delta) {
+    extern __shared__ float4 sbd32[];
     __shared__ SchedSmem ss;
     load_sched(s, ss);
     const int total = ss.pre[ss.nact] * TILE;
     for (int vp = blockIdx.x * blockDim.x + threadIdx.x; vp < total;
          vp += gridDim.x * blockDim.x) {
         const int i = sched_point(s, ss, vp);
-        if (i >= 0) grad32_point(g, c, f, q, spd, dq, qm, delta, with_delta, i);
+        if (i >= 0)
+            grad32_point(g, c, f, q, spd, dq, qm, delta, with_delta, i, sbd32 + threadIdx.x);
     }
 }
 
@@ -129,21 +176,40 @@ kb_grad32(Geom g, Consts c, Geom32 f, Sched s, const float4 *__restrict__ q,
 // arithmetic; only the neighbours' derivatives are gathered (no q).
 __device__ __forceinline__ void
 inner32_point(const Geom &g, const Geom32 &f, const float *__restrict__ dq0,
-              const float *__restrict__ dq_in, float *__restrict__ dq_out, int i) {
+              const float *__restrict__ dq_in, float *__restrict__ dq_out, int i, float4 *sb) {
+    const int T = blockDim.x;
     float tx[4] = {0.f, 0.f, 0.f, 0.f}, ty[4] = {0.f, 0.f, 0.f, 0.f};
     const int nb = g.nbhs[i];
-    for (int r = 0; r < nb; ++r) {
-        const int k = g.conn[r * g.n + i];
-        const float2 d = __ldg(f.dxy + r * g.n + i);
-        const float w = f.w ? __ldg(f.w + r * g.n + i) : 1.0f;
-        float dxk[4], dyk[4];
-        ldf8w(dq_in + 8 * (size_t)k, dxk, dyk);
-        const float wdx = w * d.x, wdy = w * d.y;
+    for (int r0 = 0; r0 < nb; r0 += STAGE32_I) {
+        const int m = min(STAGE32_I, nb - r0);
+        int kk[STAGE32_I];
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            const float pk = d.x * dxk[m] + d.y * dyk[m];
-            tx[m] = tx[m] + wdx * pk;
-            ty[m] = ty[m] + wdy * pk;
+        for (int t = 0; t < STAGE32_I; ++t)
+            kk[t] = t < m ? __ldg(g.conn + (r0 + t) * g.n + i) : 0;
+#pragma unroll
+        for (int t = 0; t < STAGE32_I; ++t) {
+            if (t < m) {
+                float4 *d = sb + t * UNITS32_I * T;
+                const float4 *row = reinterpret_cast<const float4 *>(dq_in + 8 * (size_t)kk[t]);
+                cp16(d, row);
+                cp16(d + T, row + 1);
+                cp8(d + 2 * T, f.dxy + (r0 + t) * g.n + i);
+            }
+        }
+        cp_wait_all();
+        for (int t = 0; t < m; ++t) {
+            const float4 *d = sb + t * UNITS32_I * T;
+            const float4 a = d[0], b = d[T], gs = d[2 * T];
+            const float dxk[4] = {a.x, a.y, a.z, a.w}, dyk[4] = {b.x, b.y, b.z, b.w};
+            const int r = r0 + t;
+            const float w = f.w ? __ldg(f.w + r * g.n + i) : 1.0f;
+            const float wdx = w * gs.x, wdy = w * gs.y;
+#pragma unroll
+            for (int mm = 0; mm < 4; ++mm) {
+                const float pk = gs.x * dxk[mm] + gs.y * dyk[mm];
+                tx[mm] = tx[mm] + wdx * pk;
+                ty[mm] = ty[mm] + wdy * pk;
+            }
         }
     }
     float dxi[4], dyi[4], dx0[4], dy0[4];
@@ -162,13 +228,14 @@ inner32_point(const Geom &g, const Geom32 &f, const float *__restrict__ dq0,
 __global__ void __launch_bounds__(GRAD_BLOCK)
 kb_inner32(Geom g, Geom32 f, Sched s, const float *__restrict__ dq0,
            const float *__restrict__ dq_in, float *__restrict__ dq_out) {
+    extern __shared__ float4 sbi32[];
     __shared__ SchedSmem ss;
     load_sched(s, ss);
     const int total = ss.pre[ss.nact] * TILE;
     for (int vp = blockIdx.x * blockDim.x + threadIdx.x; vp < total;
          vp += gridDim.x * blockDim.x) {
         const int i = sched_point(s, ss, vp);
-        if (i >= 0) inner32_point(g, f, dq0, dq_in, dq_out, i);
+        if (i >= 0) inner32_point(g, f, dq0, dq_in, dq_out, i, sbi32 + threadIdx.x);
     }
 }
 
@@ -181,30 +248,50 @@ __device__ __forceinline__ void kahan_add(float &s, float &cmp, float v) {
 }
 
 // cal_flux_residual + state_update + eval_q_variables of the new state, with
-// the per-neighbour work in FP32 (same lane layout as the FP64 kernel; the
-// list derivatives go to sG and update32_point runs on one warp per tile).
-// One call handles one tile of GROUPS points (arguments as in the FP64 pass).
-__device__ __forceinline__ void
-flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool valid,
-            int kind0, double *sm, double *sG) {
-    const int grp = threadIdx.x / LPP, lane = threadIdx.x % LPP;
-    double *rec = sm + (size_t)grp * g.kp * FREC;
+// the per-neighbour work in FP32.  Work split as in the FP64 pass: a warp
+// owns two tiles (32 points) end to end with no block barrier, computes
+// their list derivatives in rounds of four points (eight lanes each, slots
+// taken eight at a time with the lane pairs' Kahan sums parked in shared
+// memory between slot rounds), then updates the 32 points one per lane.
+constexpr int PPW = 32 / LPP;
+constexpr int CHUNK = 2 * TILE;
+constexpr int GST = 17;                                  // odd: no bank conflicts
+constexpr int FLUX_WARPS = FLUX_BLOCK / 32;
+constexpr int GROUP_SMEM = LPP * FREC + 4 * LPP;         // records + parked sums (doubles)
+constexpr int WARP_SMEM = PPW * GROUP_SMEM + CHUNK * GST + CHUNK;
 
+__device__ __forceinline__ void
+flux32_group(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool valid,
+             int kind0, double *rec, double *Gout) {
+    const int lane = threadIdx.x % LPP;
     int nb = 0, kind = KIND_INTERIOR;
     unsigned long long mx = 0, my = 0;
-    double nx = 0.0, ny = 1.0;
+    float nxf = 0.f, nyf = 1.f;
     if (valid) {
         nb = g.nbhs[i];
         kind = kind0;
         mx = g.mx[i];
         my = g.my[i];
         const double2 nn = g.nrm[i];
-        nx = nn.x;
-        ny = nn.y;
-        const float nxf = (float)nx, nyf = (float)ny;
-        const float inv_gm1 = (float)(1.0 / c.gm1), inv_sqrt_pi = (float)(1.0 / sqrt(c.pi));
-        const float s2q = kind == KIND_WALL ? -1.0f : 1.0f;
-        for (int r = lane; r < nb; r += LPP) {
+        nxf = (float)nn.x;
+        nyf = (float)nn.y;
+    }
+    const float inv_gm1 = (float)(1.0 / c.gm1), inv_sqrt_pi = (float)(1.0 / sqrt(c.pi));
+    const float s2q = kind == KIND_WALL ? -1.0f : 1.0f;
+    const int nbw = __reduce_max_sync(0xffffffffu, nb);
+    const int L = lane >> 1, c0 = (lane & 1) * 2;
+    const bool used =
+        valid && !((kind == KIND_WALL && L == 2) || (kind == KIND_OUTER && L == 3));
+    float fx0 = 0.f, fx1 = 0.f, fy0 = 0.f, fy1 = 0.f;
+    float cx0 = 0.f, cx1 = 0.f, cy0 = 0.f, cy1 = 0.f;
+    float *park = reinterpret_cast<float *>(rec + LPP * FREC) + 8 * lane;
+    for (int r0 = 0; r0 < nbw; r0 += LPP) {
+        if (r0 > 0) {
+            park[0] = fx0; park[1] = fx1; park[2] = fy0; park[3] = fy1;
+            park[4] = cx0; park[5] = cx1; park[6] = cy0; park[7] = cy1;
+        }
+        const int r = r0 + lane;
+        if (r < nb) {
             const int k = g.conn[r * g.n + i];
             const float2 d = __ldg(b.f.dxy + r * g.n + i);
             const float dxf = d.x, dyf = d.y;
@@ -230,20 +317,19 @@ flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool va
             const float dels = dxf * nyf - dyf * nxf;
             const float deln = dxf * nxf + dyf * nyf;
             const float w = b.f.w ? __ldg(b.f.w + r * g.n + i) : 1.0f;
-            double *e = rec + r * FREC;
-            float *ef = reinterpret_cast<float *>(e);
+            float *ef = reinterpret_cast<float *>(rec + lane * FREC);
             float Gi[4], Gk[4];
 #pragma unroll
-            for (int d = 0; d < 2; ++d) {
+            for (int dd = 0; dd < 2; ++dd) {
                 // one converged evaluation per direction, as in the FP64 pass
-                const unsigned long long bits = d == 0 ? mx : my;
+                const unsigned long long bits = dd == 0 ? mx : my;
                 const bool in0 = (bits >> r) & 1ull, in1 = (bits >> (r + 32)) & 1ull;
 #pragma unroll
                 for (int pass = 0; pass < 2; ++pass) {
                     if (pass == 0 ? !(in0 || in1) : !(in0 && in1)) continue;
-                    const int L = 2 * d + ((pass == 1 || !in0) ? 1 : 0);
-                    const float sg = (L & 1) ? -1.0f : 1.0f;
-                    if (d == 0) {
+                    const int Lx = 2 * dd + ((pass == 1 || !in0) ? 1 : 0);
+                    const float sg = (Lx & 1) ? -1.0f : 1.0f;
+                    if (dd == 0) {
                         if (kind == KIND_INTERIOR) {
                             flux_gx<float>(si, sg, Gi);
                             flux_gx<float>(sk, sg, Gk);
@@ -256,26 +342,23 @@ flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool va
                         flux_gy<float>(sk, sg, Gk);
                     }
 #pragma unroll
-                    for (int m = 0; m < 4; ++m) ef[4 * L + m] = Gk[m] - Gi[m];
+                    for (int m = 0; m < 4; ++m) ef[4 * Lx + m] = Gk[m] - Gi[m];
                 }
             }
             ef[16] = dels * w;
             ef[17] = deln * w;
         }
-    }
-    __syncwarp();
-
-    double Gv0 = 0.0, Gv1 = 0.0;
-    if (valid) {
-        const int L = lane >> 1, c0 = (lane & 1) * 2;
-        const bool used = !((kind == KIND_WALL && L == 2) || (kind == KIND_OUTER && L == 3));
-        const unsigned long long bits = ((L < 2) ? mx : my) >> ((L & 1) ? 32 : 0);
+        __syncwarp();
+        if (r0 > 0) {
+            fx0 = park[0]; fx1 = park[1]; fy0 = park[2]; fy1 = park[3];
+            cx0 = park[4]; cx1 = park[5]; cy0 = park[6]; cy1 = park[7];
+        }
         if (used) {
-            float fx0 = 0.f, fx1 = 0.f, fy0 = 0.f, fy1 = 0.f;
-            float cx0 = 0.f, cx1 = 0.f, cy0 = 0.f, cy1 = 0.f;
-            for (int r = 0; r < nb; ++r) {
-                if (!((bits >> r) & 1ull)) continue;
-                const float *ef = reinterpret_cast<const float *>(rec + r * FREC);
+            const unsigned long long lbits = ((L < 2) ? mx : my) >> ((L & 1) ? 32 : 0);
+            const int rend = min(nb, r0 + LPP);
+            for (int rr = r0; rr < rend; ++rr) {
+                if (!((lbits >> rr) & 1ull)) continue;
+                const float *ef = reinterpret_cast<const float *>(rec + (rr - r0) * FREC);
                 const float d0 = ef[4 * L + c0], d1 = ef[4 * L + c0 + 1];
                 const float sw = ef[16], nw = ef[17];
                 kahan_add(fx0, cx0, d0 * sw);
@@ -283,23 +366,27 @@ flux32_tile(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool va
                 kahan_add(fx1, cx1, d1 * sw);
                 kahan_add(fy1, cy1, d1 * nw);
             }
-            // the list's precomputed solve: x lists a Sx + b Sy, y lists a Sy + b Sx
-            const float4 co = __ldg(b.f.flsq + 2 * (size_t)i + (L >> 1));
-            const double a = (L & 1) ? co.z : co.x, bb = (L & 1) ? co.w : co.y;
-            const double X0 = (double)fx0 - cx0, X1 = (double)fx1 - cx1;
-            const double Y0 = (double)fy0 - cy0, Y1 = (double)fy1 - cy1;
-            if (L < 2) {
-                Gv0 = a * X0 + bb * Y0;
-                Gv1 = a * X1 + bb * Y1;
-            } else {
-                Gv0 = a * Y0 + bb * X0;
-                Gv1 = a * Y1 + bb * X1;
-            }
+        }
+        __syncwarp();  // the next round overwrites the records
+    }
+    double Gv0 = 0.0, Gv1 = 0.0;
+    if (used) {
+        // the list's precomputed solve: x lists a Sx + b Sy, y lists a Sy + b Sx
+        const float4 co = __ldg(b.f.flsq + 2 * (size_t)i + (L >> 1));
+        const double a = (L & 1) ? co.z : co.x, bb = (L & 1) ? co.w : co.y;
+        const double X0 = (double)fx0 - cx0, X1 = (double)fx1 - cx1;
+        const double Y0 = (double)fy0 - cy0, Y1 = (double)fy1 - cy1;
+        if (L < 2) {
+            Gv0 = a * X0 + bb * Y0;
+            Gv1 = a * X1 + bb * Y1;
+        } else {
+            Gv0 = a * Y0 + bb * X0;
+            Gv1 = a * Y1 + bb * X1;
         }
     }
     // lane 2L+h holds G[L][2h], G[L][2h+1]
-    sG[grp * 16 + 2 * lane] = Gv0;
-    sG[grp * 16 + 2 * lane + 1] = Gv1;
+    Gout[2 * lane] = Gv0;
+    Gout[2 * lane + 1] = Gv1;
 }
 
 // state_update.F90:10-141 of one point from its four list derivatives
@@ -373,40 +460,56 @@ update32_point(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, int
     return res_sqr;
 }
 
+// Each warp walks chunks of two scheduled tiles with a stride of all warps of
+// the grid; tile partials as in the FP64 pass.
 __global__ void __launch_bounds__(FLUX_BLOCK, FLUX32_MIN_BLOCKS)
 kb_flux32(Geom g, Consts c, Sched s, StageBufs32 b, int rk, int last) {
-    extern __shared__ double sm[];
-    __shared__ double sres[GROUPS];
-    __shared__ double sG[GROUPS * 16];
+    __shared__ double sm[FLUX_WARPS * WARP_SMEM];
     __shared__ SchedSmem ss;
-    load_sched(s, ss);
-    const int total = ss.pre[ss.nact];
-    for (int v = blockIdx.x; v < total; v += gridDim.x) {
-        const TileRef t = sched_tile(s, ss, v);
-        const int j = t.j0 + threadIdx.x / LPP;
-        const int kind = j < t.nw ? KIND_WALL : (j < t.nw + t.no ? KIND_OUTER : KIND_INTERIOR);
-        flux32_tile(g, c, b, t.base + j, j < t.n, kind, sm, sG);
-        __syncthreads();
-        if (threadIdx.x < GROUPS) {
-            const int jj = t.j0 + threadIdx.x;
-            double rs = 0.0;
-            if (jj < t.n) {
-                const int kk =
-                    jj < t.nw ? KIND_WALL : (jj < t.nw + t.no ? KIND_OUTER : KIND_INTERIOR);
-                rs = update32_point(g, c, b, rk, last, t.base + jj, kk, t.obc_off + jj - t.nw,
-                                    sG + 16 * threadIdx.x);
+    load_sched(s, ss);  // the kernel's only block barrier
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    double *rec = sm + warp * WARP_SMEM;
+    double *wG = rec + PPW * GROUP_SMEM;
+    double *wres = wG + CHUNK * GST;
+    const int ntiles = ss.pre[ss.nact];
+    const int nchunks = (ntiles + 1) / 2;
+    for (int ch = blockIdx.x * FLUX_WARPS + warp; ch < nchunks; ch += gridDim.x * FLUX_WARPS) {
+        const bool has1 = 2 * ch + 1 < ntiles;
+        for (int rnd = 0; rnd < CHUNK / PPW; ++rnd) {
+            const int pj = rnd * PPW + lane / LPP;
+            const int v = 2 * ch + (pj < TILE ? 0 : 1);
+            bool valid = false;
+            int i = 0, kind = KIND_INTERIOR;
+            if (v < ntiles) {
+                const TileRef t = sched_tile(s, ss, v);
+                const int j = t.j0 + (pj % TILE);
+                valid = j < t.n;
+                i = t.base + j;
+                kind = j < t.nw ? KIND_WALL : (j < t.nw + t.no ? KIND_OUTER : KIND_INTERIOR);
             }
-            if (last) {
-                sres[threadIdx.x] = rs;
-                __syncwarp(0xffffu);
-                if (threadIdx.x == 0) {
-                    double acc = 0.0;
-                    for (int q = 0; q < GROUPS; ++q) acc = acc + sres[q];
-                    b.res_part[t.tile] = acc;
-                }
+            flux32_group(g, c, b, i, valid, kind, rec + (lane / LPP) * GROUP_SMEM, wG + GST * pj);
+        }
+        __syncwarp();
+        const int v = 2 * ch + (lane < TILE ? 0 : 1);
+        const TileRef t = sched_tile(s, ss, v < ntiles ? v : 2 * ch);
+        const int j = t.j0 + (lane % TILE);
+        const bool valid = v < ntiles && j < t.n;
+        double rs = 0.0;
+        if (valid) {
+            const int kind = j < t.nw ? KIND_WALL : (j < t.nw + t.no ? KIND_OUTER : KIND_INTERIOR);
+            rs = update32_point(g, c, b, rk, last, t.base + j, kind, t.obc_off + j - t.nw,
+                                wG + GST * lane);
+        }
+        if (last) {
+            wres[lane] = rs;
+            __syncwarp();
+            if ((lane % TILE) == 0 && (lane < TILE || has1)) {
+                double acc = 0.0;
+                for (int q = 0; q < TILE; ++q) acc = acc + wres[lane + q];
+                b.res_part[t.tile] = acc;
             }
         }
-        __syncthreads();  // the next tile reuses sm, sG and sres
+        __syncwarp();  // the next chunk reuses wG and wres
     }
 }
 
@@ -433,12 +536,20 @@ inline int nblk(int n, int b) { return (n + b - 1) / b; }
 
 }  // namespace
 
+size_t grad32_smem_bytes(int block) { return (size_t)block * STAGE32 * UNITS32_D * 16; }
+size_t inner32_smem_bytes(int block) { return (size_t)block * STAGE32_I * UNITS32_I * 16; }
+
 cudaError_t init_kernels32() {
-    return cudaFuncSetAttribute(kb_flux32, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                GROUPS * 20 * FREC * (int)sizeof(double));
+    cudaError_t e = cudaFuncSetAttribute(kb_grad32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)grad32_smem_bytes(GRAD_BLOCK));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kb_inner32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)inner32_smem_bytes(GRAD_BLOCK));
+    return e;
 }
 
-size_t flux32_smem_bytes(int kp) { return (size_t)GROUPS * kp * FREC * sizeof(double); }
+// the flux pass's shared memory is static (independent of the stencil size)
+size_t flux32_smem_bytes(int) { return 0; }
 
 int batch_occupancy32(int kind, int block, size_t smem) {
     int nb = 0;
@@ -462,22 +573,23 @@ int wave32(int kind, int block, size_t smem, int grid) {
 void launch_grad32(const Geom &g, const Consts &c, const Geom32 &f, const Sched &s,
                    const float4 *q, const double *spd, float *dq, float *qm, double *delta,
                    bool with_delta, int block, int grid, cudaStream_t st) {
-    kb_grad32<<<wave32(0, block, 0, grid), block, 0, st>>>(g, c, f, s, q, spd, dq, qm, delta,
-                                                           with_delta ? 1 : 0);
+    const size_t smem = grad32_smem_bytes(block);
+    kb_grad32<<<wave32(0, block, smem, grid), block, smem, st>>>(g, c, f, s, q, spd, dq, qm,
+                                                                 delta, with_delta ? 1 : 0);
 }
 
 void launch_inner32(const Geom &g, const Consts &c, const Geom32 &f, const Sched &s,
                     const float *dq0, const float *dq_in, float *dq_out, int block, int grid,
                     cudaStream_t st) {
     (void)c;
-    kb_inner32<<<wave32(1, block, 0, grid), block, 0, st>>>(g, f, s, dq0, dq_in, dq_out);
+    const size_t smem = inner32_smem_bytes(block);
+    kb_inner32<<<wave32(1, block, smem, grid), block, smem, st>>>(g, f, s, dq0, dq_in, dq_out);
 }
 
 void launch_flux32(const Geom &g, const Consts &c, const Sched &s, const StageBufs32 &b,
                          int rk, bool last, int grid, cudaStream_t st) {
-    size_t smem = (size_t)GROUPS * g.kp * FREC * sizeof(double);
-    kb_flux32<<<wave32(2, FLUX_BLOCK, smem, grid), FLUX_BLOCK, smem, st>>>(g, c, s, b, rk,
-                                                                           last ? 1 : 0);
+    kb_flux32<<<wave32(2, FLUX_BLOCK, 0, grid), FLUX_BLOCK, 0, st>>>(g, c, s, b, rk,
+                                                                     last ? 1 : 0);
 }
 
 void launch_init_state32(const Geom &g, const float4 *prim, float4 *q, double *spd,

@@ -29,11 +29,10 @@ namespace {
 
 constexpr int GRAD_BLOCK = 256;
 constexpr int LPP = 8;                   // lanes per point in the flux pass
-constexpr int FLUX_BLOCK = 128;          // 16 points per block
-constexpr int GROUPS = FLUX_BLOCK / LPP;
+constexpr int FLUX_BLOCK = 128;          // four independent warps
 constexpr int REC = 19;                  // dGxp[4] dGxn[4] dGyp[4] dGyn[4] dels deln w
 #ifndef FLUX_MIN_BLOCKS
-#define FLUX_MIN_BLOCKS 5                // <= 102 registers: 20 warps per SM
+#define FLUX_MIN_BLOCKS 4                // <= 128 registers; shared memory allows 4 blocks
 #endif
 constexpr double OBT = 1.0 / 3.0;        // state_update.F90:19-20
 constexpr double TBT = 2.0 / 3.0;
@@ -66,12 +65,51 @@ __device__ __forceinline__ void ld8w(const double *p, double a[4], double b[4]) 
     b[0] = v.a; b[1] = v.b; b[2] = v.c; b[3] = v.d;
 }
 
+// ---------------------------------------------------------------------------
+// Staged neighbour gathers of the D and I passes.
+//
+// A thread owns one point.  Its stencil is read in rounds of STAGE slots:
+// the round's conn entries are loaded first (independent, coalesced loads),
+// then every neighbour row the round needs is copied into the thread's own
+// shared-memory slots with cp.async (16-byte asynchronous copies that hold no
+// registers while in flight), and one wait covers them all.  The per-point
+// sums then run in slot order -- the reference's loop order -- from shared
+// memory.  The serial chain of the plain loop (conn -> row -> sums, once per
+// neighbour) becomes one chain per round, with every row of the round in
+// flight at once.  Shared memory is laid out thread-minor
+// (sb[pair * blockDim + thread], a pair = 16 bytes) so the copies and the
+// reads of a warp hit distinct banks.  Each thread reads only what it
+// copied, so no block barrier is needed.
+#ifndef STAGE_D
+#define STAGE_D 8  // slots per round, D pass
+#endif
+#ifndef STAGE_I
+#define STAGE_I 4  // slots per round, I pass
+#endif
+constexpr int PAIRS_D = 4;  // q[0..1], q[2..3], (x, y), (spd, -)
+constexpr int PAIRS_I = 7;  // q[0..1], q[2..3], dq[0..1], dq[2..3], dq[4..5], dq[6..7], (x, y)
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+// Waits for every cp.async this thread issued.
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // q_variables.F90:41-112 eval_q_derivatives, and state_update.F90:190-236
 // func_delta (spd[k] = |u_k| + 3 sqrt(p_k/rho_k) of the neighbour's state).
 __device__ __forceinline__ void
 grad_point(const Geom &g, const Consts &c, const R4 *__restrict__ q, const double *__restrict__ spd,
            double *__restrict__ dq, double *__restrict__ qm, double *__restrict__ delta,
-           int with_delta, int i) {
+           int with_delta, int i, double2 *sb) {
+    const int T = blockDim.x;
+    const int nb = g.nbhs[i];
     double2 pi_ = g.xy[i];
     R4 qv = ld4w(q + i);
     double qi[4] = {qv.a, qv.b, qv.c, qv.d};
@@ -80,32 +118,48 @@ grad_point(const Geom &g, const Consts &c, const R4 *__restrict__ q, const doubl
     double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
     double sdxq[4] = {0.0, 0.0, 0.0, 0.0}, sdyq[4] = {0.0, 0.0, 0.0, 0.0};
     double min_delt = 1.0;
-    int nb = g.nbhs[i];
-    for (int r = 0; r < nb; ++r) {
-        int k = g.conn[r * g.n + i];
-        R4 kv = ld4w(q + k);
-        double qk[4] = {kv.a, kv.b, kv.c, kv.d};
+    for (int r0 = 0; r0 < nb; r0 += STAGE_D) {
+        const int m = min(STAGE_D, nb - r0);
+        int kk[STAGE_D];
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            if (qk[m] > qmax[m]) qmax[m] = qk[m];
-            if (qk[m] < qmin[m]) qmin[m] = qk[m];
-        }
-        double2 pk = g.xy[k];
-        double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
-        double dist = sqrt(delx * delx + dely * dely);
-        double w = c.power_zero ? 1.0 : pow(dist, c.power);
-        sdx2 = sdx2 + delx * delx * w;
-        sdy2 = sdy2 + dely * dely * w;
-        sdxy = sdxy + delx * dely * w;
+        for (int t = 0; t < STAGE_D; ++t) kk[t] = t < m ? __ldg(g.conn + (r0 + t) * g.n + i) : 0;
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            sdxq[m] = sdxq[m] + w * delx * (qk[m] - qi[m]);
-            sdyq[m] = sdyq[m] + w * dely * (qk[m] - qi[m]);
+        for (int t = 0; t < STAGE_D; ++t) {
+            if (t < m) {
+                double2 *d = sb + t * PAIRS_D * T;
+                const double2 *row = reinterpret_cast<const double2 *>(q + kk[t]);
+                cp_async16(d, row);
+                cp_async16(d + T, row + 1);
+                cp_async16(d + 2 * T, g.xy + kk[t]);
+                if (with_delta) cp_async8(d + 3 * T, spd + kk[t]);
+            }
         }
-        if (with_delta) {
-            double delta_t = dist / spd[k];
-            delta_t = c.cfl * delta_t;
-            if (min_delt > delta_t) min_delt = delta_t;
+        cp_async_wait_all();
+        for (int t = 0; t < m; ++t) {
+            const double2 *d = sb + t * PAIRS_D * T;
+            const double2 a = d[0], b = d[T], pk = d[2 * T];
+            double qk[4] = {a.x, a.y, b.x, b.y};
+#pragma unroll
+            for (int mm = 0; mm < 4; ++mm) {
+                if (qk[mm] > qmax[mm]) qmax[mm] = qk[mm];
+                if (qk[mm] < qmin[mm]) qmin[mm] = qk[mm];
+            }
+            double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
+            double dist = sqrt(delx * delx + dely * dely);
+            double w = c.power_zero ? 1.0 : pow(dist, c.power);
+            sdx2 = sdx2 + delx * delx * w;
+            sdy2 = sdy2 + dely * dely * w;
+            sdxy = sdxy + delx * dely * w;
+#pragma unroll
+            for (int mm = 0; mm < 4; ++mm) {
+                sdxq[mm] = sdxq[mm] + w * delx * (qk[mm] - qi[mm]);
+                sdyq[mm] = sdyq[mm] + w * dely * (qk[mm] - qi[mm]);
+            }
+            if (with_delta) {
+                double delta_t = dist / d[3 * T].x;
+                delta_t = c.cfl * delta_t;
+                if (min_delt > delta_t) min_delt = delta_t;
+            }
         }
     }
     double det = sdx2 * sdy2 - sdxy * sdxy;
@@ -122,18 +176,19 @@ grad_point(const Geom &g, const Consts &c, const R4 *__restrict__ q, const doubl
 }
 
 // D pass: grid-stride over the points of the scheduled instances (a single
-// grid is the one-instance case).
+// grid is the one-instance case).  Dynamic shared memory: grad_smem_bytes.
 __global__ void __launch_bounds__(GRAD_BLOCK)
 kb_grad(Geom g, Consts c, Sched s, const R4 *__restrict__ q, const double *__restrict__ spd,
         double *__restrict__ dq, double *__restrict__ qm, double *__restrict__ delta,
         int with_delta) {
+    extern __shared__ double2 sbd[];
     __shared__ SchedSmem ss;
     load_sched(s, ss);
     const int total = ss.pre[ss.nact] * TILE;
     for (int vp = blockIdx.x * blockDim.x + threadIdx.x; vp < total;
          vp += gridDim.x * blockDim.x) {
         const int i = sched_point(s, ss, vp);
-        if (i >= 0) grad_point(g, c, q, spd, dq, qm, delta, with_delta, i);
+        if (i >= 0) grad_point(g, c, q, spd, dq, qm, delta, with_delta, i, sbd + threadIdx.x);
     }
 }
 
@@ -141,7 +196,9 @@ kb_grad(Geom g, Consts c, Sched s, const R4 *__restrict__ q, const double *__res
 // dq_in, writes dq_out (the buffers swap instead of copying temp into dq).
 __device__ __forceinline__ void
 inner_point(const Geom &g, const Consts &c, const R4 *__restrict__ q,
-            const double *__restrict__ dq_in, double *__restrict__ dq_out, int i) {
+            const double *__restrict__ dq_in, double *__restrict__ dq_out, int i, double2 *sb) {
+    const int T = blockDim.x;
+    const int nb = g.nbhs[i];
     double2 pi_ = g.xy[i];
     R4 qv = ld4w(q + i);
     double qi[4] = {qv.a, qv.b, qv.c, qv.d};
@@ -149,26 +206,48 @@ inner_point(const Geom &g, const Consts &c, const R4 *__restrict__ q,
     ld8w(dq_in + 8 * (size_t)i, dxi, dyi);
     double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
     double sdxq[4] = {0.0, 0.0, 0.0, 0.0}, sdyq[4] = {0.0, 0.0, 0.0, 0.0};
-    int nb = g.nbhs[i];
-    for (int r = 0; r < nb; ++r) {
-        int k = g.conn[r * g.n + i];
-        R4 kv = ld4w(q + k);
-        double qk[4] = {kv.a, kv.b, kv.c, kv.d};
-        double dxk[4], dyk[4];
-        ld8w(dq_in + 8 * (size_t)k, dxk, dyk);
-        double2 pk = g.xy[k];
-        double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
-        double w = 1.0;
-        if (!c.power_zero) w = pow(sqrt(delx * delx + dely * dely), c.power);
-        sdx2 = sdx2 + delx * delx * w;
-        sdy2 = sdy2 + dely * dely * w;
-        sdxy = sdxy + delx * dely * w;
+    for (int r0 = 0; r0 < nb; r0 += STAGE_I) {
+        const int m = min(STAGE_I, nb - r0);
+        int kk[STAGE_I];
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            double temp1 = qi[m] - 0.5 * (delx * dxi[m] + dely * dyi[m]);
-            double temp2 = qk[m] - 0.5 * (delx * dxk[m] + dely * dyk[m]);
-            sdxq[m] = sdxq[m] + (w * delx * (temp2 - temp1));
-            sdyq[m] = sdyq[m] + (w * dely * (temp2 - temp1));
+        for (int t = 0; t < STAGE_I; ++t) kk[t] = t < m ? __ldg(g.conn + (r0 + t) * g.n + i) : 0;
+#pragma unroll
+        for (int t = 0; t < STAGE_I; ++t) {
+            if (t < m) {
+                double2 *d = sb + t * PAIRS_I * T;
+                const double2 *row = reinterpret_cast<const double2 *>(q + kk[t]);
+                const double2 *drow = reinterpret_cast<const double2 *>(dq_in + 8 * (size_t)kk[t]);
+                cp_async16(d, row);
+                cp_async16(d + T, row + 1);
+                cp_async16(d + 2 * T, drow);
+                cp_async16(d + 3 * T, drow + 1);
+                cp_async16(d + 4 * T, drow + 2);
+                cp_async16(d + 5 * T, drow + 3);
+                cp_async16(d + 6 * T, g.xy + kk[t]);
+            }
+        }
+        cp_async_wait_all();
+        for (int t = 0; t < m; ++t) {
+            const double2 *d = sb + t * PAIRS_I * T;
+            const double2 a = d[0], b = d[T];
+            const double2 e0 = d[2 * T], e1 = d[3 * T], e2 = d[4 * T], e3 = d[5 * T];
+            const double2 pk = d[6 * T];
+            const double qk[4] = {a.x, a.y, b.x, b.y};
+            const double dxk[4] = {e0.x, e0.y, e1.x, e1.y};
+            const double dyk[4] = {e2.x, e2.y, e3.x, e3.y};
+            double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
+            double w = 1.0;
+            if (!c.power_zero) w = pow(sqrt(delx * delx + dely * dely), c.power);
+            sdx2 = sdx2 + delx * delx * w;
+            sdy2 = sdy2 + dely * dely * w;
+            sdxy = sdxy + delx * dely * w;
+#pragma unroll
+            for (int mm = 0; mm < 4; ++mm) {
+                double temp1 = qi[mm] - 0.5 * (delx * dxi[mm] + dely * dyi[mm]);
+                double temp2 = qk[mm] - 0.5 * (delx * dxk[mm] + dely * dyk[mm]);
+                sdxq[mm] = sdxq[mm] + (w * delx * (temp2 - temp1));
+                sdyq[mm] = sdyq[mm] + (w * dely * (temp2 - temp1));
+            }
         }
     }
     double det = sdx2 * sdy2 - sdxy * sdxy;
@@ -185,37 +264,50 @@ inner_point(const Geom &g, const Consts &c, const R4 *__restrict__ q,
 __global__ void __launch_bounds__(GRAD_BLOCK)
 kb_inner(Geom g, Consts c, Sched s, const R4 *__restrict__ q, const double *__restrict__ dq_in,
          double *__restrict__ dq_out) {
+    extern __shared__ double2 sbi[];
     __shared__ SchedSmem ss;
     load_sched(s, ss);
     const int total = ss.pre[ss.nact] * TILE;
     for (int vp = blockIdx.x * blockDim.x + threadIdx.x; vp < total;
          vp += gridDim.x * blockDim.x) {
         const int i = sched_point(s, ss, vp);
-        if (i >= 0) inner_point(g, c, q, dq_in, dq_out, i);
+        if (i >= 0) inner_point(g, c, q, dq_in, dq_out, i, sbi + threadIdx.x);
     }
 }
 
 // flux_residual.F90:14-73 cal_flux_residual + state_update.F90:10-141 +
 // q_variables.F90:8-37 on the new state.
 //
-// Eight lanes share one point; lane l takes stencil slots l, l+8, l+16.  For
-// its neighbour k a lane reconstructs both states once (limiter + qtilde ->
-// kinetic state, reconstruct_kstate; the reference repeats this per direction
-// list with identical inputs, so sharing it is exact), evaluates the split fluxes of every list
-// the neighbour belongs to, and stores G_k - G_i with the geometry in shared
-// memory.  Then lane pair (2L, 2L+1) sums list L in slot order -- the
-// reference's loop order -- for components (0,1) and (2,3) and leaves the
-// list derivatives in sG[16 grp + 4L + m]; update_point then runs once per
-// point on the first GROUPS threads of the block (one warp), so that the
-// update's serial chain does not hold four warps at one lane in eight.
+// Work split: a warp owns CHUNK = 32 consecutive points (two tiles) end to
+// end, with no block barrier.  It computes their list derivatives in rounds
+// of PPW = 4 points, eight lanes per point (flux_group), leaving each point's
+// sixteen list derivatives in the warp's shared memory, then updates the 32
+// points with one lane each (update_point) and writes the two tiles'
+// residual partials.
 //
-// One call handles one tile of GROUPS points; point i of this thread's group
-// is valid or padding and kind0 is its kind.
+// In flux_group lane l of a point takes stencil slots l, l+8, l+16.  For its
+// neighbour k it reconstructs both states once (limiter + qtilde -> kinetic
+// state, reconstruct_kstate; the reference repeats this per direction list
+// with identical inputs, so sharing it is exact), evaluates the split fluxes
+// of every list the neighbour belongs to, and stores G_k - G_i with the
+// geometry in a record.  Lane pair (2L, 2L+1) then sums list L in slot order
+// -- the reference's loop order -- for components (0,1) and (2,3).  Slots
+// are taken eight at a time: the records of one round of slots are summed
+// before the next round overwrites them, the running sums waiting in shared
+// memory between rounds, so shared memory does not grow with the stencil.
+constexpr int PPW = 32 / LPP;          // points per warp round
+constexpr int CHUNK = 2 * TILE;        // points a warp owns (two tiles)
+constexpr int GST = 17;                // stride of a point's list derivatives (odd: no bank conflicts)
+constexpr int FLUX_WARPS = FLUX_BLOCK / 32;
+// doubles per warp: per point of a round its records and its lanes' parked
+// sums, then the chunk's list derivatives and residual terms
+constexpr int GROUP_SMEM = LPP * REC + 7 * LPP;
+constexpr int WARP_SMEM = PPW * GROUP_SMEM + CHUNK * GST + CHUNK;
+
 __device__ __forceinline__ void
-flux_tile(const Geom &g, const Consts &c, const StageBufs &b, int i, bool valid, int kind0,
-          double *sm, double *sG) {
-    const int grp = threadIdx.x / LPP, lane = threadIdx.x % LPP;
-    double *rec = sm + (size_t)grp * g.kp * REC;
+flux_group(const Geom &g, const Consts &c, const StageBufs &b, int i, bool valid, int kind0,
+           double *rec, double *Gout) {
+    const int lane = threadIdx.x % LPP;
     const double inv_gm1 = 1.0 / c.gm1, inv_sqrt_pi = 1.0 / sqrt(c.pi);
 
     int nb = 0, kind = KIND_INTERIOR;
@@ -229,10 +321,27 @@ flux_tile(const Geom &g, const Consts &c, const StageBufs &b, int i, bool valid,
         const double2 nn = g.nrm[i];
         nx = nn.x;
         ny = nn.y;
-        // x-list flux signs: interior Gxp/Gxn; wall GxII/GxI (A2neg); outer
-        // GxIII/GxIV (A2pos).  y lists: Gyp (+1) / Gyn (-1).
-        const double s2q = kind == KIND_WALL ? -1.0 : 1.0;
-        for (int r = lane; r < nb; r += LPP) {
+    }
+    // x-list flux signs: interior Gxp/Gxn; wall GxII/GxI (A2neg); outer
+    // GxIII/GxIV (A2pos).  y lists: Gyp (+1) / Gyn (-1).
+    const double s2q = kind == KIND_WALL ? -1.0 : 1.0;
+    const int nbw = __reduce_max_sync(0xffffffffu, nb);  // slot rounds of the warp
+    // list-sum role of this lane: list L, components c0, c0+1
+    const int L = lane >> 1, c0 = (lane & 1) * 2;
+    const bool used =
+        valid && !((kind == KIND_WALL && L == 2) || (kind == KIND_OUTER && L == 3));
+    double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
+    double fx0 = 0.0, fx1 = 0.0, fy0 = 0.0, fy1 = 0.0;
+    double *park = rec + LPP * REC + 7 * lane;  // running sums across slot rounds
+    for (int r0 = 0; r0 < nbw; r0 += LPP) {
+        if (r0 > 0) {
+            // stencils of more than eight slots: the sums wait in shared
+            // memory while the next round's records are computed
+            park[0] = sdx2; park[1] = sdy2; park[2] = sdxy;
+            park[3] = fx0; park[4] = fx1; park[5] = fy0; park[6] = fy1;
+        }
+        const int r = r0 + lane;
+        if (r < nb) {
             const int k = g.conn[r * g.n + i];
             const double2 pi_ = g.xy[i];
             const double2 pk = g.xy[k];
@@ -264,7 +373,7 @@ flux_tile(const Geom &g, const Consts &c, const StageBufs &b, int i, bool valid,
             const double deln = delx * nx + dely * ny;
             double w = 1.0;
             if (!c.power_zero) w = pow(sqrt(dels * dels + deln * deln), c.power);
-            double *e = rec + r * REC;
+            double *e = rec + lane * REC;
             // Per direction the neighbour is in one list of the pair (in both
             // only when its projection is exactly 0): one evaluation with the
             // list's sign taken per lane keeps the warp converged where
@@ -279,8 +388,8 @@ flux_tile(const Geom &g, const Consts &c, const StageBufs &b, int i, bool valid,
                     // pass 0: the first list holding the neighbour; pass 1:
                     // the second list of a neighbour in both
                     if (pass == 0 ? !(in0 || in1) : !(in0 && in1)) continue;
-                    const int L = 2 * d + ((pass == 1 || !in0) ? 1 : 0);
-                    const double sg = (L & 1) ? -1.0 : 1.0;
+                    const int Lx = 2 * d + ((pass == 1 || !in0) ? 1 : 0);
+                    const double sg = (Lx & 1) ? -1.0 : 1.0;
                     if (d == 0) {
                         if (kind == KIND_INTERIOR) {
                             flux_gx(si, sg, Gi);
@@ -294,28 +403,25 @@ flux_tile(const Geom &g, const Consts &c, const StageBufs &b, int i, bool valid,
                         flux_gy(sk, sg, Gk);
                     }
 #pragma unroll
-                    for (int m = 0; m < 4; ++m) e[4 * L + m] = Gk[m] - Gi[m];
+                    for (int m = 0; m < 4; ++m) e[4 * Lx + m] = Gk[m] - Gi[m];
                 }
             }
             e[16] = dels;
             e[17] = deln;
             e[18] = w;
         }
-    }
-    __syncwarp();
-
-    // List sums in slot order: lane -> list L = lane/2, components c0, c0+1.
-    double Gv0 = 0.0, Gv1 = 0.0;
-    if (valid) {
-        const int L = lane >> 1, c0 = (lane & 1) * 2;
-        const bool used = !((kind == KIND_WALL && L == 2) || (kind == KIND_OUTER && L == 3));
-        const unsigned long long bits = ((L < 2) ? mx : my) >> ((L & 1) ? 32 : 0);
+        __syncwarp();
+        if (r0 > 0) {
+            sdx2 = park[0]; sdy2 = park[1]; sdxy = park[2];
+            fx0 = park[3]; fx1 = park[4]; fy0 = park[5]; fy1 = park[6];
+        }
+        // list sums of this round's slots, in slot order
         if (used) {
-            double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
-            double fx0 = 0.0, fx1 = 0.0, fy0 = 0.0, fy1 = 0.0;
-            for (int r = 0; r < nb; ++r) {
-                if (!((bits >> r) & 1ull)) continue;
-                const double *e = rec + r * REC;
+            const unsigned long long lbits = ((L < 2) ? mx : my) >> ((L & 1) ? 32 : 0);
+            const int rend = min(nb, r0 + LPP);
+            for (int rr = r0; rr < rend; ++rr) {
+                if (!((lbits >> rr) & 1ull)) continue;
+                const double *e = rec + (rr - r0) * REC;
                 double dels = e[16], deln = e[17], w = e[18];
                 double dels_w = dels * w, deln_w = deln * w;
                 sdx2 = sdx2 + dels * dels_w;
@@ -327,20 +433,24 @@ flux_tile(const Geom &g, const Consts &c, const StageBufs &b, int i, bool valid,
                 fx1 = fx1 + d1 * dels_w;
                 fy1 = fy1 + d1 * deln_w;
             }
-            double det = sdx2 * sdy2 - sdxy * sdxy;
-            double one_by_det = 1.0 / det;
-            if (L < 2) {
-                Gv0 = (fx0 * sdy2 - fy0 * sdxy) * one_by_det;
-                Gv1 = (fx1 * sdy2 - fy1 * sdxy) * one_by_det;
-            } else {
-                Gv0 = (fy0 * sdx2 - fx0 * sdxy) * one_by_det;
-                Gv1 = (fy1 * sdx2 - fx1 * sdxy) * one_by_det;
-            }
+        }
+        __syncwarp();  // the next round overwrites the records
+    }
+    double Gv0 = 0.0, Gv1 = 0.0;
+    if (used) {
+        double det = sdx2 * sdy2 - sdxy * sdxy;
+        double one_by_det = 1.0 / det;
+        if (L < 2) {
+            Gv0 = (fx0 * sdy2 - fy0 * sdxy) * one_by_det;
+            Gv1 = (fx1 * sdy2 - fy1 * sdxy) * one_by_det;
+        } else {
+            Gv0 = (fy0 * sdx2 - fx0 * sdxy) * one_by_det;
+            Gv1 = (fy1 * sdx2 - fx1 * sdxy) * one_by_det;
         }
     }
     // lane 2L+h holds G[L][2h], G[L][2h+1]
-    sG[grp * 16 + 2 * lane] = Gv0;
-    sG[grp * 16 + 2 * lane + 1] = Gv1;
+    Gout[2 * lane] = Gv0;
+    Gout[2 * lane + 1] = Gv1;
 }
 
 // state_update.F90:10-141 of one point from its four list derivatives
@@ -407,44 +517,60 @@ update_point(const Geom &g, const Consts &c, const StageBufs &b, int rk, int las
     return res_sqr;
 }
 
-// F pass: each block walks the scheduled tiles with a stride of the grid.  A
-// tile never straddles two instances and its partial lands in slot
-// (instance's first tile + tile number), so an instance's residual sums do
-// not depend on the other instances or on the launch shape.
+// F pass: each warp walks chunks of two scheduled tiles with a stride of all
+// warps of the grid.  A tile never straddles two instances and its partial
+// lands in slot (instance's first tile + tile number), summed over its 16
+// points in point order, so an instance's residual sums do not depend on the
+// other instances or on the launch shape.
 __global__ void __launch_bounds__(FLUX_BLOCK, FLUX_MIN_BLOCKS)
 kb_flux(Geom g, Consts c, Sched s, StageBufs b, int rk, int last) {
-    extern __shared__ double sm[];
-    __shared__ double sres[GROUPS];
-    __shared__ double sG[GROUPS * 16];
+    __shared__ double sm[FLUX_WARPS * WARP_SMEM];
     __shared__ SchedSmem ss;
-    load_sched(s, ss);
-    const int total = ss.pre[ss.nact];
-    for (int v = blockIdx.x; v < total; v += gridDim.x) {
-        const TileRef t = sched_tile(s, ss, v);
-        const int j = t.j0 + threadIdx.x / LPP;
-        const int kind = j < t.nw ? KIND_WALL : (j < t.nw + t.no ? KIND_OUTER : KIND_INTERIOR);
-        flux_tile(g, c, b, t.base + j, j < t.n, kind, sm, sG);
-        __syncthreads();
-        if (threadIdx.x < GROUPS) {
-            const int jj = t.j0 + threadIdx.x;
-            double rs = 0.0;
-            if (jj < t.n) {
-                const int kk =
-                    jj < t.nw ? KIND_WALL : (jj < t.nw + t.no ? KIND_OUTER : KIND_INTERIOR);
-                rs = update_point(g, c, b, rk, last, t.base + jj, kk, t.obc_off + jj - t.nw,
-                                  sG + 16 * threadIdx.x);
+    load_sched(s, ss);  // the kernel's only block barrier
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    double *rec = sm + warp * WARP_SMEM;       // PPW groups of GROUP_SMEM
+    double *wG = rec + PPW * GROUP_SMEM;       // CHUNK points x GST
+    double *wres = wG + CHUNK * GST;           // CHUNK residual terms
+    const int ntiles = ss.pre[ss.nact];
+    const int nchunks = (ntiles + 1) / 2;
+    for (int ch = blockIdx.x * FLUX_WARPS + warp; ch < nchunks; ch += gridDim.x * FLUX_WARPS) {
+        const bool has1 = 2 * ch + 1 < ntiles;
+        for (int rnd = 0; rnd < CHUNK / PPW; ++rnd) {
+            const int pj = rnd * PPW + lane / LPP;  // point of the chunk
+            const int v = 2 * ch + (pj < TILE ? 0 : 1);
+            bool valid = false;
+            int i = 0, kind = KIND_INTERIOR;
+            if (v < ntiles) {
+                const TileRef t = sched_tile(s, ss, v);
+                const int j = t.j0 + (pj % TILE);
+                valid = j < t.n;
+                i = t.base + j;
+                kind = j < t.nw ? KIND_WALL : (j < t.nw + t.no ? KIND_OUTER : KIND_INTERIOR);
             }
-            if (last) {
-                sres[threadIdx.x] = rs;
-                __syncwarp(0xffffu);
-                if (threadIdx.x == 0) {
-                    double acc = 0.0;
-                    for (int q = 0; q < GROUPS; ++q) acc = acc + sres[q];
-                    b.res_part[t.tile] = acc;
-                }
+            flux_group(g, c, b, i, valid, kind, rec + (lane / LPP) * GROUP_SMEM, wG + GST * pj);
+        }
+        __syncwarp();
+        // the chunk's state updates, one point per lane
+        const int v = 2 * ch + (lane < TILE ? 0 : 1);
+        const TileRef t = sched_tile(s, ss, v < ntiles ? v : 2 * ch);
+        const int j = t.j0 + (lane % TILE);
+        const bool valid = v < ntiles && j < t.n;
+        double rs = 0.0;
+        if (valid) {
+            const int kind = j < t.nw ? KIND_WALL : (j < t.nw + t.no ? KIND_OUTER : KIND_INTERIOR);
+            rs = update_point(g, c, b, rk, last, t.base + j, kind, t.obc_off + j - t.nw,
+                              wG + GST * lane);
+        }
+        if (last) {
+            wres[lane] = rs;
+            __syncwarp();
+            if ((lane % TILE) == 0 && (lane < TILE || has1)) {
+                double acc = 0.0;
+                for (int q = 0; q < TILE; ++q) acc = acc + wres[lane + q];
+                b.res_part[t.tile] = acc;
             }
         }
-        __syncthreads();  // the next tile reuses sm, sG and sres
+        __syncwarp();  // the next chunk reuses wG and wres
     }
 }
 
@@ -623,14 +749,26 @@ inline int nblk(int n, int b) { return (n + b - 1) / b; }
 
 }  // namespace
 
-int flux_blocks(int n) { return nblk(n, GROUPS); }
+int flux_blocks(int n) { return nblk(n, TILE); }
+// blocks that give every warp of the flux pass one chunk of two tiles
+int flux_grid_blocks(int n) { return nblk(nblk(n, TILE), 2 * FLUX_WARPS); }
+
+size_t grad_smem_bytes(int block) { return (size_t)block * STAGE_D * PAIRS_D * sizeof(double2); }
+size_t inner_smem_bytes(int block) { return (size_t)block * STAGE_I * PAIRS_I * sizeof(double2); }
 
 cudaError_t init_kernels() {
-    return cudaFuncSetAttribute(kb_flux, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                GROUPS * 20 * REC * (int)sizeof(double));
+    cudaError_t e = cudaFuncSetAttribute(kb_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)grad_smem_bytes(GRAD_BLOCK));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kb_inner, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)inner_smem_bytes(GRAD_BLOCK));
+    return e;
 }
 
 int wave_blocks(int dev, int kind, int block, size_t smem, bool fp32) {
+    // the D and I passes size their staging buffers by the block
+    if (kind == 0) smem = fp32 ? grad32_smem_bytes(block) : grad_smem_bytes(block);
+    if (kind == 1) smem = fp32 ? inner32_smem_bytes(block) : inner_smem_bytes(block);
     int sms = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     return std::max(sms, 1) * std::max(1, batch_occupancy(kind, fp32, block, smem));
@@ -646,7 +784,8 @@ int wave(int kind, int block, size_t smem, int grid) {
 }
 }  // namespace
 
-size_t flux_smem_bytes(int kp) { return (size_t)GROUPS * kp * REC * sizeof(double); }
+// the flux pass's shared memory is static (independent of the stencil size)
+size_t flux_smem_bytes(int) { return 0; }
 
 int batch_occupancy(int kind, bool fp32, int block, size_t smem) {
     if (fp32) return batch_occupancy32(kind, block, smem);
@@ -661,13 +800,15 @@ int batch_occupancy(int kind, bool fp32, int block, size_t smem) {
 void launch_grad(const Geom &g, const Consts &c, const Sched &s, const R4 *q, const double *spd,
                  double *dq, double *qm, double *delta, bool with_delta, int block, int grid,
                  cudaStream_t st) {
-    kb_grad<<<wave(0, block, 0, grid), block, 0, st>>>(g, c, s, q, spd, dq, qm, delta,
-                                                       with_delta ? 1 : 0);
+    const size_t smem = grad_smem_bytes(block);
+    kb_grad<<<wave(0, block, smem, grid), block, smem, st>>>(g, c, s, q, spd, dq, qm, delta,
+                                                             with_delta ? 1 : 0);
 }
 
 void launch_inner(const Geom &g, const Consts &c, const Sched &s, const R4 *q,
                   const double *dq_in, double *dq_out, int block, int grid, cudaStream_t st) {
-    kb_inner<<<wave(1, block, 0, grid), block, 0, st>>>(g, c, s, q, dq_in, dq_out);
+    const size_t smem = inner_smem_bytes(block);
+    kb_inner<<<wave(1, block, smem, grid), block, smem, st>>>(g, c, s, q, dq_in, dq_out);
 }
 
 void launch_flux(const Geom &g, const Consts &c, const Sched &s, const StageBufs &b, int rk,
