@@ -224,6 +224,13 @@ const char *mfcfd_last_error(mfcfd_t *h);
 /* Device kernels launched by the handle since creation (all kinds). */
 long long mfcfd_launch_count(mfcfd_t *h);
 
+/* Diagnostic, no counterpart in the reference: the FP64 FMA throughput of
+ * the current device in TFLOP/s (one FMA = 2 flops), measured with a
+ * kernel of independent FMA chains (best of five launches after a warm-up).
+ * The flux pass, which is bound by FP64 issue, is reported against it.
+ * Allocates a small scratch buffer. */
+int mfcfd_measure_fp64_peak(double *tflops);
+
 /* Largest n_iters one mfcfd_run_noalloc call accepts. */
 #define MFCFD_NOALLOC_MAX_ITERS 65536
 

@@ -29,6 +29,7 @@ EXPORTS = ("mfcfd_default_params", "mfcfd_create", "mfcfd_destroy", "mfcfd_set_s
            "mfcfd_get_state", "mfcfd_run", "mfcfd_forces", "mfcfd_set_stream",
            "mfcfd_get_array", "mfcfd_keep_diagnostics", "mfcfd_info", "mfcfd_strerror",
            "mfcfd_last_error", "mfcfd_launch_count", "mfcfd_profile_iteration",
+           "mfcfd_measure_fp64_peak",
            "mfcfd_run_noalloc", "mfcfd_adjoint", "mfcfd_adjoint_many", "mfcfd_tangent",
            "mfcfd_output_fields",
            "mfcfd_objective",
@@ -99,6 +100,7 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     lib.mfcfd_launch_count.argtypes = [P]
     lib.mfcfd_launch_count.restype = C.c_longlong
     lib.mfcfd_profile_iteration.argtypes = [P, C.c_int, D]
+    lib.mfcfd_measure_fp64_peak.argtypes = [D]
     lib.mfcfd_run_noalloc.argtypes = [P, C.c_int, C.c_int, D, I]
     lib.mfcfd_adjoint.argtypes = [P, C.c_int, C.c_int, C.c_size_t, D, D, D, I]
     lib.mfcfd_adjoint_many.argtypes = [C.c_int, C.POINTER(P), C.c_int, C.c_int, C.c_size_t, D,

@@ -17,7 +17,7 @@ HEADER = os.path.join(ROOT, "include", "mfcfd_b200.h")
 
 def declared_functions():
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:const\s+)?[a-z ]+\*?\s*\*?(mfcfd_[a-z_]+)\s*\(", text,
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[a-z ]+\*?\s*\*?(mfcfd_[a-z0-9_]+)\s*\(", text,
                                  re.M)))
 
 
