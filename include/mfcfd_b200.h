@@ -231,6 +231,43 @@ long long mfcfd_launch_count(mfcfd_t *h);
  * Allocates a small scratch buffer. */
 int mfcfd_measure_fp64_peak(double *tflops);
 
+/* A partitioned grid: one rank's part of a point set split over ranks, as
+ * the reference runs it on several MPI ranks (point.h5 groups /1 .. /P,
+ * point_preprocessor.F90:177-546; PETSc ghost vectors,
+ * petsc_data_structure.F90:21-54).  grid holds the rank's points: the first
+ * n_local are owned (full rows), the rest are ghosts, of which only x, y and
+ * min_dist are read (the reference's ghost rows, :489-501); stencils of owned
+ * points may name ghosts.  plen is the point count of all ranks (the residual
+ * norm's divisor, fpi_solver.F90:57-63).  FP64 loop only.  The handle runs
+ * iterations one phase at a time with mfcfd_part_phase (mfcfd_run refuses
+ * it); between phases the caller refreshes the ghost rows from their owners
+ * (mfcfd_part_rows gives the device rows, mfcfd_part_index their order). */
+int mfcfd_create_part(const mfcfd_grid *grid, const mfcfd_params *params, int n_local,
+                      int plen, mfcfd_t **out);
+
+/* Phases of one iteration of a partitioned grid (fpi_solver.F90:13-83):
+ * BEGIN; per stage rk = 1..rks: GRAD (eval_q_derivatives, and func_delta at
+ * rk 1) -> refresh dq and qm ghost rows; INNER t = 1..m -> refresh dq;
+ * FLUX (cal_flux_residual + state_update) -> refresh prim, then GHOSTS (q of
+ * the ghost rows from their prim); END writes the rank's sum of res_sqr to
+ * *value, which the caller adds over the ranks (MPI_Reduce + Bcast,
+ * fpi_solver.F90:57-61) before the residue. */
+#define MFCFD_PHASE_BEGIN  0
+#define MFCFD_PHASE_GRAD   1
+#define MFCFD_PHASE_INNER  2
+#define MFCFD_PHASE_FLUX   3
+#define MFCFD_PHASE_GHOSTS 4
+#define MFCFD_PHASE_END    5
+int mfcfd_part_phase(mfcfd_t *h, int phase, int rk, int t, double *value);
+
+/* Device rows the last phase wrote, for the ghost refresh: name "prim" (4
+ * doubles a row), "dq" or "qm" (8 doubles a row), in the handle's internal
+ * row order (mfcfd_part_index). */
+int mfcfd_part_rows(mfcfd_t *h, const char *name, void **rows, int *row_doubles);
+
+/* internal[i] = internal row of point i (caller order), for all grid.n points. */
+int mfcfd_part_index(mfcfd_t *h, int *internal);
+
 /* Largest n_iters one mfcfd_run_noalloc call accepts. */
 #define MFCFD_NOALLOC_MAX_ITERS 65536
 

@@ -29,7 +29,8 @@ EXPORTS = ("mfcfd_default_params", "mfcfd_create", "mfcfd_destroy", "mfcfd_set_s
            "mfcfd_get_state", "mfcfd_run", "mfcfd_forces", "mfcfd_set_stream",
            "mfcfd_get_array", "mfcfd_keep_diagnostics", "mfcfd_info", "mfcfd_strerror",
            "mfcfd_last_error", "mfcfd_launch_count", "mfcfd_profile_iteration",
-           "mfcfd_measure_fp64_peak",
+           "mfcfd_measure_fp64_peak", "mfcfd_create_part", "mfcfd_part_phase",
+           "mfcfd_part_rows", "mfcfd_part_index",
            "mfcfd_run_noalloc", "mfcfd_adjoint", "mfcfd_adjoint_many", "mfcfd_tangent",
            "mfcfd_output_fields",
            "mfcfd_objective",
@@ -42,6 +43,7 @@ MFCFD_ADJOINT_MANY_MAX = 256
 OBJECTIVES = {"cl": 0, "cd": 1, "entropy": 2, "enstrophy": 3, "stagnation": 4}
 BATCH_STATES = {0: "running", 1: "converged", 2: "max_iters", 3: "nonfinite"}
 MFCFD_NOALLOC_MAX_ITERS = 65536
+PHASE_BEGIN, PHASE_GRAD, PHASE_INNER, PHASE_FLUX, PHASE_GHOSTS, PHASE_END = range(6)
 
 
 class Grid(C.Structure):
@@ -101,6 +103,11 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     lib.mfcfd_launch_count.restype = C.c_longlong
     lib.mfcfd_profile_iteration.argtypes = [P, C.c_int, D]
     lib.mfcfd_measure_fp64_peak.argtypes = [D]
+    lib.mfcfd_create_part.argtypes = [C.POINTER(Grid), C.POINTER(Params), C.c_int, C.c_int,
+                                      C.POINTER(P)]
+    lib.mfcfd_part_phase.argtypes = [P, C.c_int, C.c_int, C.c_int, D]
+    lib.mfcfd_part_rows.argtypes = [P, C.c_char_p, C.POINTER(C.c_void_p), I]
+    lib.mfcfd_part_index.argtypes = [P, I]
     lib.mfcfd_run_noalloc.argtypes = [P, C.c_int, C.c_int, D, I]
     lib.mfcfd_adjoint.argtypes = [P, C.c_int, C.c_int, C.c_size_t, D, D, D, I]
     lib.mfcfd_adjoint_many.argtypes = [C.c_int, C.POINTER(P), C.c_int, C.c_int, C.c_size_t, D,

@@ -74,7 +74,7 @@ void free_all(mfcfd_t *h) {
                     h->d_sh_my, h->f_prim[0], h->f_prim[1], h->f_q[0], h->f_q[1],
                     h->f_dq[0], h->f_dq[1], h->f_dq[2], h->f_qm, h->f_eps2, h->f_dxy, h->f_w, h->f_lsq,
                     h->f_flsq, h->d_inst, h->d_sched,
-                    h->d_run};
+                    h->d_run, h->d_part_sum};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (h->h_ctl) cudaFreeHost(h->h_ctl);
@@ -375,9 +375,15 @@ void build_geom32(HostGrid &hg, int nw, int no, double power) {
 // Host half of mfcfd_create: checks of the grid and parameters, normals,
 // split membership, renumbering and the renumbered arrays, all in caller
 // arithmetic; no device call.  Errors are reported as by mfcfd_create.
-int lskum_host::prepare_grid(const mfcfd_grid &G, const mfcfd_params &P, HostGrid &hg) {
+int lskum_host::prepare_grid(const mfcfd_grid &G, const mfcfd_params &P, HostGrid &hg,
+                             int n_local) {
     const int n = G.n;
     if (n <= 0) return fail(nullptr, MFCFD_ERR_ARG, "grid.n must be positive");
+    // points [n_local, n) are ghosts of a partitioned grid: only their x, y
+    // and min_dist are used (the reference's ghost rows,
+    // point_preprocessor.F90:489-501)
+    const int nl = n_local < 0 ? n : n_local;
+    if (nl < 1 || nl > n) return fail(nullptr, MFCFD_ERR_ARG, "n_local out of range [1, n]");
     if (!G.x || !G.y || !G.nx || !G.ny || !G.min_dist || !G.flag_1 || !G.flag_2 || !G.left ||
         !G.right || !G.nbhs || !G.conn)
         return fail(nullptr, MFCFD_ERR_ARG, "a grid array is NULL");
@@ -397,7 +403,7 @@ int lskum_host::prepare_grid(const mfcfd_grid &G, const mfcfd_params &P, HostGri
 
     // grid checks (point_preprocessor.F90:32,73 reject bad partitions and shapes)
     int nw = 0, no = 0, kp = 1;
-    for (int i = 0; i < n; ++i) {
+    for (int i = 0; i < nl; ++i) {
         int f = G.flag_1[i], nb = G.nbhs[i];
         if (f < 0 || f > 2) return fail(nullptr, MFCFD_ERR_GRID, "flag_1 must be 0, 1 or 2");
         if (G.flag_2[i] < 0 || G.flag_2[i] > G.shapes)
@@ -422,8 +428,8 @@ int lskum_host::prepare_grid(const mfcfd_grid &G, const mfcfd_params &P, HostGri
     const double q_inf[4] = {1.0, P.mach * cos(theta), P.mach * sin(theta), 1.0 / 1.4};
 
     // point_normals.F90:8-105 (caller order)
-    std::vector<double> nx(n), ny(n);
-    for (int i = 0; i < n; ++i) {
+    std::vector<double> nx(n, 0.0), ny(n, 1.0);
+    for (int i = 0; i < nl; ++i) {
         int f = G.flag_1[i];
         if (f == 1) {
             if (P.interior_points_normal_flag == 0 && P.format != 2) {
@@ -449,7 +455,7 @@ int lskum_host::prepare_grid(const mfcfd_grid &G, const mfcfd_params &P, HostGri
 
     // generate_connectivity.F90:39-256 as bit masks (caller order, caller slots)
     std::vector<unsigned long long> mx(n, 0), my(n, 0);
-    for (int i = 0; i < n; ++i) {
+    for (int i = 0; i < nl; ++i) {
         int f = G.flag_1[i];
         double xi = G.x[i], yi = G.y[i], tx = ny[i], ty = -nx[i];
         unsigned cnt[4] = {0, 0, 0, 0};
@@ -481,11 +487,12 @@ int lskum_host::prepare_grid(const mfcfd_grid &G, const mfcfd_params &P, HostGri
         }
     }
     // shape points need ring neighbours for ds (compute_force_coeffs.F90:43-62)
-    for (int i = 0; i < n; ++i)
+    for (int i = 0; i < nl; ++i)
         if (G.flag_2[i] > 0 && (G.left[i] < 1 || G.left[i] > n || G.right[i] < 1 || G.right[i] > n))
             return fail(nullptr, MFCFD_ERR_GRID, "shape point without valid left/right");
 
     hg.n = n;
+    hg.n_local = nl;
     hg.kp = kp;
     hg.nw = nw;
     hg.no = no;
@@ -499,7 +506,7 @@ int lskum_host::prepare_grid(const mfcfd_grid &G, const mfcfd_params &P, HostGri
     std::vector<int> base(n);
     if (P.ordering == MFCFD_ORDER_RCM) {
         std::vector<std::vector<int>> adj(n);
-        for (int i = 0; i < n; ++i)
+        for (int i = 0; i < nl; ++i)
             for (int r = 0; r < G.nbhs[i]; ++r) {
                 int k = G.conn[(size_t)r * G.ld_conn + i] - 1;
                 if (k == i) continue;
@@ -517,7 +524,8 @@ int lskum_host::prepare_grid(const mfcfd_grid &G, const mfcfd_params &P, HostGri
     hg.perm.reserve(n);
     for (int want : {0, 2, 1})
         for (int i : base)
-            if (G.flag_1[i] == want) hg.perm.push_back(i);
+            if (i < nl && G.flag_1[i] == want) hg.perm.push_back(i);
+    for (int i = nl; i < n; ++i) hg.perm.push_back(i);  // ghosts last, in caller order
     std::vector<int> inv(n);
     for (int p = 0; p < n; ++p) inv[hg.perm[p]] = p;
 
@@ -535,9 +543,10 @@ int lskum_host::prepare_grid(const mfcfd_grid &G, const mfcfd_params &P, HostGri
         double epsi = P.vl_const * G.min_dist[i];
         epsi = pow(epsi, 3.0);  // limiters.F90:88-89
         heps[p] = epsi * epsi;
-        hnb[p] = G.nbhs[i];
+        const int nbi = i < nl ? G.nbhs[i] : 0;  // a ghost has no stencil
+        hnb[p] = nbi;
         for (int r = 0; r < kp; ++r) {
-            int k = r < G.nbhs[i] ? inv[G.conn[(size_t)r * G.ld_conn + i] - 1] : p;
+            int k = r < nbi ? inv[G.conn[(size_t)r * G.ld_conn + i] - 1] : p;
             hconn[(size_t)r * n + p] = k;
         }
         hmx[p] = mx[i];
@@ -562,7 +571,7 @@ int lskum_host::prepare_grid(const mfcfd_grid &G, const mfcfd_params &P, HostGri
     // shape points in grid order (compute_force_coeffs.F90:40-78)
     auto &sidx = hg.sidx, &sshape = hg.sshape;
     auto &sgeo = hg.sgeo, &smy = hg.smy;
-    for (int i = 0; i < n; ++i) {
+    for (int i = 0; i < nl; ++i) {
         if (G.flag_2[i] <= 0) continue;
         int l = G.left[i] - 1, r = G.right[i] - 1;
         double lx = G.x[l], ly = G.y[l], mxx = G.x[i], myy = G.y[i], rx = G.x[r], ry = G.y[r];
@@ -631,9 +640,32 @@ void noalloc_resolve(mfcfd_t *h) {
 
 }  // namespace
 
+static int create_handle(const mfcfd_grid *grid, const mfcfd_params *params, int n_local,
+                         int plen, mfcfd_t **out);
+
 extern "C" {
 
 int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **out) {
+    return create_handle(grid, params, -1, -1, out);
+}
+
+int mfcfd_create_part(const mfcfd_grid *grid, const mfcfd_params *params, int n_local,
+                      int plen, mfcfd_t **out) {
+    if (out) *out = nullptr;
+    if (!grid || !params || !out) return fail(nullptr, MFCFD_ERR_ARG, "NULL argument");
+    if (n_local < 1 || n_local > grid->n || plen < n_local)
+        return fail(nullptr, MFCFD_ERR_ARG, "need 1 <= n_local <= grid.n and plen >= n_local");
+    if (params->precision != MFCFD_FP64)
+        return fail(nullptr, MFCFD_ERR_ARG, "a partitioned grid runs the FP64 loop only");
+    return create_handle(grid, params, n_local, plen, out);
+}
+
+}  // extern "C"
+
+// The body of mfcfd_create; n_local / plen >= 0 make a partitioned handle
+// (points [n_local, n) are ghosts; the residual norm divides by plen).
+static int create_handle(const mfcfd_grid *grid, const mfcfd_params *params, int n_local,
+                         int plen, mfcfd_t **out) {
     mfcfd_t *h = nullptr;
     if (!out) return fail(nullptr, MFCFD_ERR_ARG, "out is NULL");
     *out = nullptr;
@@ -642,10 +674,11 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
     const mfcfd_params &P = *params;
     HostGrid hg;
     {
-        int st0 = lskum_host::prepare_grid(G, P, hg);
+        int st0 = lskum_host::prepare_grid(G, P, hg, n_local);
         if (st0) return st0;
     }
     const int n = hg.n, kp = hg.kp, nw = hg.nw, no = hg.no;
+    const int nl = hg.n_local;
     const auto &hxy = hg.xy, &hnrm = hg.nrm;
     const auto &heps = hg.eps2, &hobc = hg.obc;
     const auto &hconn = hg.conn, &hnb = hg.nbhs;
@@ -664,10 +697,11 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
     h = new (std::nothrow) mfcfd();
     if (!h) return fail(nullptr, MFCFD_ERR_OOM, "host allocation failed");
     h->n = n;
+    h->n_local = nl;
     h->kp = kp;
     h->nw = nw;
     h->no = no;
-    h->nint = n - nw - no;
+    h->nint = nl - nw - no;
     h->shapes = hg.shapes;
     h->nshape = hg.nshape;
     h->perm = std::move(hg.perm);
@@ -788,12 +822,12 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
     // the grid as a schedule of one instance; launch shape: one wave of
     // resident blocks per pass (measured 3% faster at 1M points than a
     // block per tile, which reloads the schedule in every block)
-    h->inst_h = InstInfo{0, n, nw, no, 0, 0, flux_blocks(n), 0};
+    h->inst_h = InstInfo{0, nl, nw, no, 0, 0, flux_blocks(nl), 0};
     h->sched = sched_view(h->d_inst, h->d_sched);
     h->point_block = default_point_block(h->fp32);
-    h->point_grid = std::min((n + h->point_block - 1) / h->point_block,
+    h->point_grid = std::min((nl + h->point_block - 1) / h->point_block,
                              point_wave_blocks(h->dev, h->point_block, h->fp32));
-    h->flux_grid = std::min(flux_grid_blocks(n),
+    h->flux_grid = std::min(flux_grid_blocks(nl),
                             wave_blocks(h->dev, 2, 128,
                                         h->fp32 ? flux32_smem_bytes(kp) : flux_smem_bytes(kp),
                                         h->fp32));
@@ -815,7 +849,7 @@ int mfcfd_create(const mfcfd_grid *grid, const mfcfd_params *params, mfcfd_t **o
         c.it = 1;
         c.it_first = 1;
         c.restart = P.restart;
-        c.plen = n;
+        c.plen = plen >= 0 ? plen : n;
         c.res_old = P.res_old;
         *h->h_ctl = c;
         cudaError_t e = cudaMemcpy(h->d_ctl, h->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice);
@@ -860,6 +894,8 @@ fail_create:
     return st;
 #undef ALLOC
 }
+
+extern "C" {
 
 int mfcfd_destroy(mfcfd_t *h) {
     if (!h) return MFCFD_OK;
@@ -977,6 +1013,8 @@ int mfcfd_get_state(mfcfd_t *h, double *prim) {
 int mfcfd_run(mfcfd_t *h, int it_first, int n_iters, double *residue, int *n_done) {
     if (n_done) *n_done = 0;
     if (!h || n_iters < 0) return MFCFD_ERR_ARG;
+    if (h->n_local != h->n)
+        return fail(h, MFCFD_ERR_STATE, "a partitioned grid runs with mfcfd_part_phase");
     if (n_iters == 0) return MFCFD_OK;
     // the history buffer and the graphs belong on the handle's device
     DevGuard dg(h->dev);
@@ -1210,6 +1248,8 @@ extern "C" int mfcfd_run_noalloc(mfcfd_t *h, int it_first, int n_iters, double *
         return fail(h, MFCFD_ERR_ARG,
                     "mfcfd_run_noalloc: n_iters exceeds MFCFD_NOALLOC_MAX_ITERS (65536); "
                     "split the run into several calls");
+    if (h->n_local != h->n)
+        return fail(h, MFCFD_ERR_STATE, "a partitioned grid runs with mfcfd_part_phase");
     if (n_iters == 0) return MFCFD_OK;
     double *hist = h->noalloc_hist;
     if (!hist) return fail(h, MFCFD_ERR_CUDA, h->noalloc_err);
@@ -1227,5 +1267,118 @@ extern "C" int mfcfd_run_noalloc(mfcfd_t *h, int it_first, int n_iters, double *
     if (n_done) *n_done = done;
     h->iters_done_total += done;
     if (h->h_ctl->halted) return fail(h, MFCFD_ERR_NONFINITE, "residue is NaN");
+    return MFCFD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// A partitioned grid, one phase at a time (the reference's multi-rank
+// fpi_solver, fpi_solver.F90:13-83 with the ghost updates of :34-52).  The
+// handle owns points [0, n_local) of its grid; the rest are ghosts whose
+// rows the caller refreshes from their owners between phases (PETSc's
+// VecGhostUpdate): dq and qm after MFCFD_PHASE_GRAD, dq after each
+// MFCFD_PHASE_INNER, prim after MFCFD_PHASE_FLUX followed by
+// MFCFD_PHASE_GHOSTS.  Kernels are the single-grid ones over the owned
+// points' tiles; ghost rows are read, never written, by them.
+namespace {
+
+int part_check(mfcfd_t *h) {
+    if (!h) return MFCFD_ERR_ARG;
+    if (h->fp32) return fail(h, MFCFD_ERR_STATE, "phases run the FP64 loop only");
+    return MFCFD_OK;
+}
+
+}  // namespace
+
+extern "C" int mfcfd_part_phase(mfcfd_t *h, int phase, int rk, int t, double *value) {
+    if (int st = part_check(h)) return st;
+    DevGuard dg(h->dev);
+    CK(dg.err);
+    cudaStream_t s = h->stream;
+    const int m = h->p.inner_iterations;
+    if (phase != MFCFD_PHASE_BEGIN && !h->part_in_iter)
+        return fail(h, MFCFD_ERR_STATE, "phase outside an iteration (MFCFD_PHASE_BEGIN first)");
+    if ((phase == MFCFD_PHASE_GRAD || phase == MFCFD_PHASE_INNER || phase == MFCFD_PHASE_FLUX) &&
+        (rk < 1 || rk > h->p.rks))
+        return fail(h, MFCFD_ERR_ARG, "rk out of range");
+    const int A = h->part_A, B = A ^ 1;
+    switch (phase) {
+    case MFCFD_PHASE_BEGIN:
+        if (!h->d_part_sum) CK(lskum_host::dmalloc(&h->d_part_sum, 1));
+        h->part_A = h->cur;
+        h->part_in_iter = true;
+        return MFCFD_OK;
+    case MFCFD_PHASE_GRAD:
+        launch_grad(h->geom, h->consts, h->sched, h->d_q[h->qcur], h->d_spd, h->d_dq[0],
+                    h->d_qm, h->d_delta, rk == 1, h->point_block, h->point_grid, s);
+        h->part_dq = 0;
+        break;
+    case MFCFD_PHASE_INNER:
+        if (t < 1 || t > m) return fail(h, MFCFD_ERR_ARG, "inner iteration t out of range");
+        launch_inner(h->geom, h->consts, h->sched, h->d_q[h->qcur], h->d_dq[(t - 1) & 1],
+                     h->d_dq[t & 1], h->point_block, h->point_grid, s);
+        h->part_dq = t & 1;
+        break;
+    case MFCFD_PHASE_FLUX: {
+        StageBufs b;
+        b.prim_in = rk == 1 ? h->d_prim[A] : h->d_prim[B];
+        b.prim_out = h->d_prim[B];
+        b.prim_old = h->d_prim[A];
+        b.q_in = h->d_q[h->qcur];
+        b.q_out = h->d_q[h->qcur ^ 1];
+        b.dq = h->d_dq[m & 1];
+        b.qm = h->d_qm;
+        b.delta = h->d_delta;
+        b.spd = h->d_spd;
+        b.res_part = h->d_res_part;
+        b.flux_dbg = h->keep_diag ? h->d_flux_dbg : nullptr;
+        launch_flux(h->geom, h->consts, h->sched, b, rk, rk == h->p.rks, h->flux_grid, s);
+        h->qcur ^= 1;
+        break;
+    }
+    case MFCFD_PHASE_GHOSTS:
+        launch_init_rows(h->geom, h->d_prim[B], h->d_q[h->qcur], h->d_spd, h->n_local, h->n, s);
+        break;
+    case MFCFD_PHASE_END:
+        launch_sum_parts(h->d_res_part, h->inst_h.ntiles, h->d_part_sum, s);
+        CK(cudaGetLastError());
+        if (value) {
+            CK(cudaMemcpyAsync(value, h->d_part_sum, sizeof(double), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+        }
+        h->cur = B;
+        h->part_in_iter = false;
+        h->launches += 1;
+        h->iters_done_total += 1;
+        return MFCFD_OK;
+    default:
+        return fail(h, MFCFD_ERR_ARG, "unknown phase");
+    }
+    h->launches += 1;
+    CK(cudaGetLastError());
+    return MFCFD_OK;
+}
+
+extern "C" int mfcfd_part_rows(mfcfd_t *h, const char *name, void **rows, int *row_doubles) {
+    if (int st = part_check(h)) return st;
+    if (!name || !rows) return fail(h, MFCFD_ERR_ARG, "NULL argument");
+    const int B = h->part_in_iter ? (h->part_A ^ 1) : h->cur;
+    if (!strcmp(name, "prim")) {
+        *rows = h->d_prim[B];
+        if (row_doubles) *row_doubles = 4;
+    } else if (!strcmp(name, "dq")) {
+        *rows = h->d_dq[h->part_dq];
+        if (row_doubles) *row_doubles = 8;
+    } else if (!strcmp(name, "qm")) {
+        *rows = h->d_qm;
+        if (row_doubles) *row_doubles = 8;
+    } else {
+        return fail(h, MFCFD_ERR_ARG, "rows: prim, dq or qm");
+    }
+    return MFCFD_OK;
+}
+
+extern "C" int mfcfd_part_index(mfcfd_t *h, int *internal) {
+    if (!h || !internal) return MFCFD_ERR_ARG;
+    for (int p = 0; p < h->n; ++p) internal[h->perm[p]] = p;
     return MFCFD_OK;
 }

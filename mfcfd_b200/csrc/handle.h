@@ -16,6 +16,7 @@ struct AdjointState;  // adjoint buffers (adjoint_api.cu), created on first use
 struct mfcfd {
     int dev = 0;
     int n = 0, kp = 1, nw = 0, no = 0, nint = 0, shapes = 1, nshape = 0;
+    int n_local = 0;  // owned points; [n_local, n) are ghosts of a partitioned grid
     mfcfd_params p{};
     std::vector<int> perm;  // new index -> caller index
     double pi = 0, theta = 0, cos_t = 0, sin_t = 0, q_inf[4] = {0, 0, 0, 0};
@@ -78,6 +79,11 @@ struct mfcfd {
     // lookup failed; noalloc_err then says why)
     double *noalloc_hist = nullptr;
     std::string noalloc_err;
+    // phase-by-phase iteration of a partitioned grid (mfcfd_part_phase)
+    bool part_in_iter = false;
+    int part_A = 0;                // prim buffer the iteration started from
+    int part_dq = 0;               // dq buffer the last D or I pass wrote
+    double *d_part_sum = nullptr;  // the rank's sum of res_sqr
     // caller-order ring neighbours of every point (for the adjoint set-up)
     std::vector<int> left0, right0, flag2_0;
 };
@@ -85,7 +91,7 @@ struct mfcfd {
 
 // Renumbered host arrays of one grid (the host half of mfcfd_create).
 struct HostGrid {
-    int n = 0, kp = 1, nw = 0, no = 0, shapes = 1, nshape = 0;
+    int n = 0, n_local = 0, kp = 1, nw = 0, no = 0, shapes = 1, nshape = 0;
     double pi = 0, theta = 0, cos_t = 0, sin_t = 0, q_inf[4] = {0, 0, 0, 0};
     std::vector<int> perm;  // new index -> caller index
     std::vector<double2> xy, nrm;
@@ -102,7 +108,8 @@ struct HostGrid {
 };
 
 namespace lskum_host {
-int prepare_grid(const mfcfd_grid &G, const mfcfd_params &P, HostGrid &hg);
+// n_local < 0: every point is owned; else points [n_local, n) are ghosts
+int prepare_grid(const mfcfd_grid &G, const mfcfd_params &P, HostGrid &hg, int n_local = -1);
 int fail(mfcfd_t *h, int code, const std::string &msg);
 int cuda_fail(mfcfd_t *h, cudaError_t e, const char *where);
 int enqueue_iteration_to(mfcfd_t *h, cudaStream_t s, double *hist);

@@ -145,6 +145,11 @@ inline int point_wave_blocks(int dev, int block, bool fp32) {
 inline int default_point_block(bool) { return 128; }
 // q and spd from prim (set_state)
 void launch_init_state(const Geom &g, const R4 *prim, R4 *q, double *spd, cudaStream_t s);
+// q and spd of rows [i0, i1) only (the ghost rows of a partitioned grid)
+void launch_init_rows(const Geom &g, const R4 *prim, R4 *q, double *spd, int i0, int i1,
+                      cudaStream_t s);
+// *out = the sum of nparts tile partials, in a fixed order
+void launch_sum_parts(const double *part, int nparts, double *out, cudaStream_t s);
 
 // FP32-mixed geometry, precomputed once per grid in FP64 and rounded:
 // offsets to the stencil neighbours [slot][point] (and weights when power

@@ -606,6 +606,23 @@ __device__ __forceinline__ double residual_block(const double *__restrict__ part
     return 0.0;
 }
 
+// Sum of nparts tile partials in the fixed order of residual_block (one
+// block of 1024 threads): a partitioned grid's share of the residual, which
+// the host adds over the ranks before the norm.
+__global__ void __launch_bounds__(1024)
+k_sum_parts(const double *__restrict__ part, int nparts, double *out) {
+    __shared__ double s[1024];
+    double acc = 0.0;
+    for (int t = threadIdx.x; t < nparts; t += blockDim.x) acc = acc + part[t];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) s[threadIdx.x] = s[threadIdx.x] + s[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = s[0];
+}
+
 // Per-instance residual (block b = instance b): the instance's tile partials
 // are reduced in the order of residual_block, then the retirement rule of the
 // run is applied (NaN residue, residue <= tol, max_iters iterations).  The
@@ -682,10 +699,12 @@ kb_residual(const InstInfo *__restrict__ inst, int n_inst, const double *__restr
     }
 }
 
+// q and spd of rows [i0, i1) from their prim (set_state: every row; a
+// partitioned grid: the ghost rows after their exchange)
 __global__ void k_init_state(Geom g, const R4 *__restrict__ prim, R4 *__restrict__ q,
-                             double *__restrict__ spd) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.n) return;
+                             double *__restrict__ spd, int i0, int i1) {
+    int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= i1) return;
     R4 P = ld4(prim + i);
     double qn[4];
     q_from_prim(P.a, P.b, P.c, P.d, qn);
@@ -825,7 +844,17 @@ void launch_residual(const InstInfo *inst, int n_inst, const double *res_part, C
 }
 
 void launch_init_state(const Geom &g, const R4 *prim, R4 *q, double *spd, cudaStream_t s) {
-    k_init_state<<<nblk(g.n, GRAD_BLOCK), GRAD_BLOCK, 0, s>>>(g, prim, q, spd);
+    k_init_state<<<nblk(g.n, GRAD_BLOCK), GRAD_BLOCK, 0, s>>>(g, prim, q, spd, 0, g.n);
+}
+
+void launch_init_rows(const Geom &g, const R4 *prim, R4 *q, double *spd, int i0, int i1,
+                      cudaStream_t s) {
+    if (i1 > i0)
+        k_init_state<<<nblk(i1 - i0, GRAD_BLOCK), GRAD_BLOCK, 0, s>>>(g, prim, q, spd, i0, i1);
+}
+
+void launch_sum_parts(const double *part, int nparts, double *out, cudaStream_t s) {
+    k_sum_parts<<<1, 1024, 0, s>>>(part, nparts, out);
 }
 
 void launch_forces(const ShapeTab &t, const R4 *prim, double mach, double cos_t, double sin_t,
