@@ -23,8 +23,10 @@ Here:
   partition in point.h5 (one group per rank, as the reference reads it);
 * ``exchange`` refreshes ghost rows over torch.distributed (gloo on the CPU,
   NCCL for device tensors): pack the send rows, isend/irecv per peer, unpack;
-* ``PartitionedOracle`` runs the reference's multi-rank pseudo-time loop on
-  the CPU oracle (test infrastructure), exchanging at the reference's points.
+* ``PartitionedSolver`` runs it on the GPU (a partitioned handle iterated
+  phase by phase, ghost rows refreshed between phases), and
+  ``PartitionedOracle`` on the CPU oracle (test infrastructure), both
+  exchanging at the reference's points.
 """
 from __future__ import annotations
 
@@ -201,29 +203,153 @@ def read_partition_h5(path: str, nranks: int, shapes: int = 1) -> list:
 # ---------------------------------------------------------------------------
 # the exchange
 
-def exchange(part: RankPart, rows, dist, group=None):
-    """Refreshes the ghost rows of `rows` ((n, w) numpy array or torch tensor,
-    the rank's local rows) from their owners: VecGhostUpdate with
-    INSERT_VALUES / SCATTER_FORWARD.  Every peer pair exchanges one message
-    each way (isend/irecv), so ranks never wait on a peer that waits on them."""
+def exchange_rows(rows, send: dict, recv: dict, dist, group=None):
+    """Copies rows between ranks: for every peer, the rows ``send[peer]`` of
+    this rank go to the peer and the rows ``recv[peer]`` are overwritten by
+    what the peer sends.  Every peer pair exchanges one message each way
+    (isend/irecv), so a rank never waits on a peer that waits on it.  `rows`
+    is an (n, w) numpy array or torch tensor, host or device; with the gloo
+    backend device rows travel through host buffers, with NCCL directly."""
     import torch
-    is_np = isinstance(rows, np.ndarray)
-    t = torch.from_numpy(rows) if is_np else rows
-    reqs, inbox = [], {}
-    for peer in sorted(set(part.send) | set(part.recv)):
-        if peer in part.send:
-            idx = torch.as_tensor(part.send[peer], device=t.device)
-            buf = t.index_select(0, idx).contiguous()
+    t = torch.from_numpy(rows) if isinstance(rows, np.ndarray) else rows
+    via_host = t.is_cuda and dist.get_backend(group) == "gloo"
+    wire = torch.device("cpu") if via_host else t.device
+    reqs, inbox, keep = [], {}, []
+    for peer in sorted(set(send) | set(recv)):
+        if peer in send:
+            idx = torch.as_tensor(np.asarray(send[peer]), device=t.device)
+            buf = t.index_select(0, idx).contiguous().to(wire)
+            keep.append(buf)
             reqs.append(dist.isend(buf, peer, group=group))
-        if peer in part.recv:
-            inbox[peer] = torch.empty((len(part.recv[peer]),) + tuple(t.shape[1:]),
-                                      dtype=t.dtype, device=t.device)
+        if peer in recv:
+            inbox[peer] = torch.empty((len(recv[peer]),) + tuple(t.shape[1:]), dtype=t.dtype,
+                                      device=wire)
             reqs.append(dist.irecv(inbox[peer], peer, group=group))
     for q in reqs:
         q.wait()
     for peer, buf in inbox.items():
-        t[torch.as_tensor(part.recv[peer], device=t.device)] = buf
+        t[torch.as_tensor(np.asarray(recv[peer]), device=t.device)] = buf.to(t.device)
     return rows
+
+
+def exchange(part: RankPart, rows, dist, group=None):
+    """Refreshes the ghost rows of `rows` (the rank's local rows, local
+    order) from their owners: VecGhostUpdate with INSERT_VALUES /
+    SCATTER_FORWARD."""
+    return exchange_rows(rows, part.send, part.recv, dist, group)
+
+
+class _DeviceRows:
+    """__cuda_array_interface__ view of rows the library owns on the device."""
+
+    def __init__(self, ptr: int, n: int, width: int):
+        self.__cuda_array_interface__ = {"shape": (n, width), "typestr": "<f8",
+                                         "data": (ptr, False), "version": 3, "strides": None}
+
+
+class PartitionedSolver:
+    """One rank of the reference's multi-rank pseudo-time loop on the GPU: the
+    rank's part as a partitioned handle (mfcfd_create_part), iterated phase
+    by phase (mfcfd_part_phase) with the ghost rows refreshed between phases
+    over torch.distributed (NCCL between GPUs, gloo through host buffers)
+    and one all-reduce of the residual per iteration."""
+
+    def __init__(self, part: RankPart, dist, device: int = 0, **flow):
+        import ctypes as C
+
+        import torch
+
+        from . import _lib
+        from .solver import make_params
+        self.part, self.dist, self.flow = part, dist, dict(flow)
+        self.torch = torch
+        self.device = torch.device("cuda", device)
+        torch.cuda.set_device(self.device)
+        self.lib = _lib.load()
+        self.params = make_params(**flow)
+        g = part.grid
+        self._arrays = [np.ascontiguousarray(a) for a in
+                        (g.x, g.y, g.nx, g.ny, g.min_dist, g.flag_1, g.flag_2, g.left, g.right,
+                         g.nbhs, g.conn)]
+        self._grid = _lib.Grid(g.n, *[a.ctypes.data_as(C.c_void_p) for a in self._arrays], g.n,
+                               g.shapes)
+        h = C.c_void_p()
+        st = self.lib.mfcfd_create_part(C.byref(self._grid), C.byref(self.params), part.n_local,
+                                        part.plen, C.byref(h))
+        _lib.check(st, None, "mfcfd_create_part")
+        self.h = h
+        self.stream = torch.cuda.current_stream(self.device)
+        _lib.check(self.lib.mfcfd_set_stream(h, C.c_void_p(self.stream.cuda_stream)), h,
+                   "mfcfd_set_stream")
+        internal = np.empty(g.n, np.int32)
+        _lib.check(self.lib.mfcfd_part_index(h, internal.ctypes.data_as(C.POINTER(C.c_int))), h,
+                   "mfcfd_part_index")
+        self.send = {k: internal[np.asarray(v)] for k, v in part.send.items()}
+        self.recv = {k: internal[np.asarray(v)] for k, v in part.recv.items()}
+        self.res_old = float(flow.get("res_old", 0.0))
+        self.restart = int(flow.get("restart", 0))
+        self._C, self._L = C, _lib
+
+    def _phase(self, phase, rk=0, t=0):
+        v = self._C.c_double(0.0)
+        self._L.check(self.lib.mfcfd_part_phase(self.h, phase, rk, t, self._C.byref(v)), self.h,
+                      "mfcfd_part_phase")
+        return v.value
+
+    def _refresh(self, name):
+        C = self._C
+        ptr, w = C.c_void_p(), C.c_int(0)
+        self._L.check(self.lib.mfcfd_part_rows(self.h, name.encode(), C.byref(ptr), C.byref(w)),
+                      self.h, "mfcfd_part_rows")
+        rows = self.torch.as_tensor(_DeviceRows(ptr.value, self.part.grid.n, w.value),
+                                    device=self.device)
+        exchange_rows(rows, self.send, self.recv, self.dist)
+
+    def run(self, n_iters: int, it_first: int = 1):
+        """Runs n_iters iterations; returns the residue of each (the same on
+        every rank)."""
+        L = self._L
+        rks = 4 if self.flow.get("tscheme", "ssprk43") == "ssprk43" else 1
+        m = int(self.flow.get("inner_iterations", 0))
+        out = []
+        for it in range(it_first, it_first + n_iters):
+            self._phase(L.PHASE_BEGIN)
+            for rk in range(1, rks + 1):
+                self._phase(L.PHASE_GRAD, rk)
+                self._refresh("dq")
+                self._refresh("qm")
+                for t in range(1, m + 1):
+                    self._phase(L.PHASE_INNER, rk, t)
+                    self._refresh("dq")
+                self._phase(L.PHASE_FLUX, rk)
+                self._refresh("prim")
+                self._phase(L.PHASE_GHOSTS)
+            on = self.device if self.dist.get_backend() == "nccl" else "cpu"
+            s = self.torch.tensor([self._phase(L.PHASE_END)], dtype=self.torch.float64,
+                                  device=on)
+            self.dist.all_reduce(s)
+            res_new = float(np.sqrt(s.item())) / self.part.plen
+            if it <= 2 and self.restart == 0:
+                self.res_old = res_new
+                residue = 0.0
+            else:
+                residue = float(np.log10(res_new / self.res_old))
+            out.append(residue)
+            if np.isnan(residue):
+                break
+        return np.array(out)
+
+    def owned_prim(self):
+        import ctypes as C
+        out = np.empty((self.part.grid.n, 4))
+        self._L.check(self.lib.mfcfd_get_state(self.h, out.ctypes.data_as(
+            C.POINTER(C.c_double))), self.h, "mfcfd_get_state")
+        return out[: self.part.n_local]
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mfcfd_destroy(self.h)
+            self.h = None
 
 
 class PartitionedOracle:
