@@ -52,6 +52,20 @@ __device__ __forceinline__ TileRef sched_tile(const Sched &s, const SchedSmem &s
     return TileRef{in.base, in.n, in.nw, in.no, in.obc_off, in.tile0 + k, k * TILE};
 }
 
+// sched_tile with the schedule read from global memory (through L1) instead
+// of a shared-memory copy: for kernels whose shared memory bounds residency.
+__device__ __forceinline__ TileRef sched_tile_global(const Sched &s, int v) {
+    int lo = 0, hi = __ldg(s.nact) - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(s.pre + mid) <= v) lo = mid;
+        else hi = mid - 1;
+    }
+    const InstInfo &in = s.inst[__ldg(s.act + lo)];
+    const int k = v - __ldg(s.pre + lo);
+    return TileRef{in.base, in.n, in.nw, in.no, in.obc_off, in.tile0 + k, k * TILE};
+}
+
 // Global point of virtual point vp, or -1 for a padding point.
 __device__ __forceinline__ int sched_point(const Sched &s, const SchedSmem &ss, int vp) {
     const int v = vp / TILE;

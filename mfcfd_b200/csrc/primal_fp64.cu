@@ -525,13 +525,21 @@ update_point(const Geom &g, const Consts &c, const StageBufs &b, int rk, int las
 __global__ void __launch_bounds__(FLUX_BLOCK, FLUX_MIN_BLOCKS)
 kb_flux(Geom g, Consts c, Sched s, StageBufs b, int rk, int last) {
     __shared__ double sm[FLUX_WARPS * WARP_SMEM];
+#ifdef FLUX_SCHED_GLOBAL
+    // the schedule stays in global memory: 2 KB more shared memory per block
+    // for the records (one more resident block per SM)
+    const int ntiles = __ldg(s.pre + __ldg(s.nact));
+#define FLUX_TILE(v) sched_tile_global(s, v)
+#else
     __shared__ SchedSmem ss;
     load_sched(s, ss);  // the kernel's only block barrier
+    const int ntiles = ss.pre[ss.nact];
+#define FLUX_TILE(v) sched_tile(s, ss, v)
+#endif
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     double *rec = sm + warp * WARP_SMEM;       // PPW groups of GROUP_SMEM
     double *wG = rec + PPW * GROUP_SMEM;       // CHUNK points x GST
     double *wres = wG + CHUNK * GST;           // CHUNK residual terms
-    const int ntiles = ss.pre[ss.nact];
     const int nchunks = (ntiles + 1) / 2;
     for (int ch = blockIdx.x * FLUX_WARPS + warp; ch < nchunks; ch += gridDim.x * FLUX_WARPS) {
         const bool has1 = 2 * ch + 1 < ntiles;
@@ -541,7 +549,7 @@ kb_flux(Geom g, Consts c, Sched s, StageBufs b, int rk, int last) {
             bool valid = false;
             int i = 0, kind = KIND_INTERIOR;
             if (v < ntiles) {
-                const TileRef t = sched_tile(s, ss, v);
+                const TileRef t = FLUX_TILE(v);
                 const int j = t.j0 + (pj % TILE);
                 valid = j < t.n;
                 i = t.base + j;
@@ -552,7 +560,7 @@ kb_flux(Geom g, Consts c, Sched s, StageBufs b, int rk, int last) {
         __syncwarp();
         // the chunk's state updates, one point per lane
         const int v = 2 * ch + (lane < TILE ? 0 : 1);
-        const TileRef t = sched_tile(s, ss, v < ntiles ? v : 2 * ch);
+        const TileRef t = FLUX_TILE(v < ntiles ? v : 2 * ch);
         const int j = t.j0 + (lane % TILE);
         const bool valid = v < ntiles && j < t.n;
         double rs = 0.0;
@@ -572,6 +580,7 @@ kb_flux(Geom g, Consts c, Sched s, StageBufs b, int rk, int last) {
         }
         __syncwarp();  // the next chunk reuses wG and wres
     }
+#undef FLUX_TILE
 }
 
 // fpi_solver.F90:57-70: res_new = sqrt(sum res_sqr)/plen and the residue.
