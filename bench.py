@@ -495,8 +495,19 @@ def main():
         kt32 = {} if halted32 else s32.profile_iteration()
         s32.close()
         v32 = world * grid.n * args.steps / (ms32 / 1e3) / 1e6
+        # the FP32-mixed flux pass against HBM: the FP64 pass table with the
+        # five FP32-stored state arrays (prim, prim_old, q, dq, qm) at 4
+        # bytes (280 - 112 = 168) plus the 8-byte slot offsets it stores
+        f32_bytes_pt = 168 + 12 * grid.mean_nbhs()
+        f32_roof = None
+        if kt32.get("flux"):
+            ach32 = f32_bytes_pt * grid.n / (kt32["flux"] / 1e3) / 1e9
+            peak32 = measured_peaks().get("hbm_gbs", FALLBACK_HBM_GBS)
+            f32_roof = {"kernel": "kb_flux32", "bound": "hbm", "algorithmic_bytes_per_point":
+                        f32_bytes_pt, "achieved": ach32, "peak": peak32, "unit": "GB/s",
+                        "frac": ach32 / peak32}
         fp32 = {"value": v32, "unit": UNIT, "ms_per_step": ms32 / args.steps,
-                "speedup_vs_fp64": v32 / value, "iterations": it64,
+                "speedup_vs_fp64": v32 / value, "iterations": it64, "roofline": f32_roof,
                 "dCl": abs(float(cl32[0] - cl64[0])), "dCd": abs(float(cd32[0] - cd64[0])),
                 "Cl_fp64": float(cl64[0]), "Cd_fp64": float(cd64[0]),
                 "kernel_ms": {k: float(v) for k, v in kt32.items()},
