@@ -35,10 +35,12 @@ void launch_update_b(const Geom &g, const Consts &c, const AdjConsts &a, const R
                      const R4 *prim_old, const R4 *fr, const double *pb_out, double *pb_in,
                      double *pb_old, double *frb, double *nxb, double *nyb, int rk,
                      cudaStream_t s);
+// kst: the stage's kinetic-state tape of the forward re-run ([n][kp][KS_TAPE],
+// written by the flux pass with StageBufs::kstape), or nullptr to recompute
 void launch_flux_b(const Geom &g, const Consts &c, const R4 *q_in, const double *dq,
                    const double *qm, const double *delta, const double *frb, double *qb,
                    double *dqb, double *qmb, double *xb, double *yb, double *nxb, double *nyb,
-                   double *deltab, double *contrib, cudaStream_t s);
+                   double *deltab, double *contrib, const double *kst, cudaStream_t s);
 void launch_inner_b(const Geom &g, const R4 *q, const double *dq_in, const double *dqb_out,
                     double *dqb_in, double *qb, double *xb, double *yb, double *contrib,
                     cudaStream_t s);

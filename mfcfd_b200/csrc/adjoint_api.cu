@@ -47,6 +47,9 @@ struct AdjointState {
     double *qb = nullptr, *dqb[2] = {nullptr, nullptr}, *qmb = nullptr, *deltab = nullptr;
     double *frb = nullptr, *xb = nullptr, *yb = nullptr, *nxb = nullptr, *nyb = nullptr;
     double *contrib = nullptr;
+    // kinetic-state tape of the re-run (rks stages of [n][kp][KS_TAPE]); null
+    // when it did not fit, and the reverse flux pass recomputes the states
+    double *tks = nullptr;
     double *hist = nullptr;
     int hist_cap = 0;
     std::vector<R4 *> snaps;  // snapshot pool (device buffers of n rows)
@@ -194,6 +197,10 @@ int adj_setup(mfcfd_t *h) {
     CK(dmalloc(&a->nxb, n));
     CK(dmalloc(&a->nyb, n));
     CK(dmalloc(&a->contrib, (size_t)n * kp * ADJ_CW));
+    if (dmalloc(&a->tks, (size_t)rks * n * kp * KS_TAPE) != cudaSuccess) {
+        a->tks = nullptr;
+        cudaGetLastError();  // an allocation failure is not sticky; clear it
+    }
     CK(dmalloc(&a->snap0, n));
     CK(dmalloc(&a->fin, n));
     cudaError_t e = init_adjoint_kernels();
@@ -202,6 +209,11 @@ int adj_setup(mfcfd_t *h) {
 }
 
 int reset_ctl(mfcfd_t *h) { return lskum_host::reset_run(h, 1); }
+
+// The kinetic-state tape of stage rk (1-based), or nullptr.
+double *ks_at(AdjointState *a, int rk) {
+    return a->tks ? a->tks + (size_t)(rk - 1) * a->n * a->kp * KS_TAPE : nullptr;
+}
 
 // Runs k plain iterations from state `from` and stores the result in `to`.
 int advance(mfcfd_t *h, AdjointState *a, const R4 *from, int k, R4 *to) {
@@ -247,6 +259,7 @@ int record(mfcfd_t *h, AdjointState *a, const R4 *from) {
         b.spd = h->d_spd;
         b.res_part = h->d_res_part;
         b.flux_dbg = reinterpret_cast<double *>(a->tfr[rk - 1]);
+        b.kstape = ks_at(a, rk);
         launch_flux(h->geom, h->consts, h->sched, b, rk, rk == rks, h->flux_grid, h->stream);
     }
     h->launches += 1 + (long long)rks * (2 + m);
@@ -276,7 +289,7 @@ int reverse_taped(mfcfd_t *h, AdjointState *a) {
         CK(cudaMemsetAsync(a->dqb[m & 1], 0, sizeof(double) * 8 * n, s));
         launch_flux_b(h->geom, h->consts, a->tq[rk - 1], dq_at(a, rk, m), qm_at(a, rk), a->tdelta,
                       a->frb, a->qb, a->dqb[m & 1], a->qmb, a->xb, a->yb, a->nxb, a->nyb,
-                      a->deltab, a->contrib, s);
+                      a->deltab, a->contrib, ks_at(a, rk), s);
         launch_gather(n, a->kp, a->d_tptr, a->d_tlist, a->contrib, ADJ_GATHER_FLUX, a->qb,
                       a->dqb[m & 1], a->qmb, a->xb, a->yb, s);
         for (int t = m; t >= 1; --t) {
@@ -377,7 +390,7 @@ void lskum_host::free_adjoint(mfcfd_t *h) {
                     a->d_nsrc, a->tdq, a->tqm, a->tdelta, a->tspd,
                     a->pb[0], a->pb[1], a->pbA, a->qb, a->dqb[0], a->dqb[1], a->qmb,
                     a->deltab, a->frb, a->xb, a->yb, a->nxb, a->nyb, a->contrib, a->hist,
-                    a->snap0, a->fin};
+                    a->snap0, a->fin, a->tks};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (int s = 0; s < 5; ++s) {

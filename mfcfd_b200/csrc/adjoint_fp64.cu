@@ -175,7 +175,7 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
          const double *__restrict__ frb, double *__restrict__ qb, double *__restrict__ dqb,
          double *__restrict__ qmb, double *__restrict__ xb, double *__restrict__ yb,
          double *__restrict__ nxb, double *__restrict__ nyb, double *__restrict__ deltab,
-         double *__restrict__ contrib) {
+         double *__restrict__ contrib, const double *__restrict__ kst) {
     extern __shared__ double sm[];
     __shared__ double lb[GROUPS][4][11];  // fx_b[4] fy_b[4] sdx2_b sdy2_b sdxy_b per list
     const int grp = threadIdx.x / LPP, lane = threadIdx.x % LPP;
@@ -214,12 +214,30 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
             ld8a(dq + 8 * (size_t)k, dxk, dyk);
             ld8a(qm + 8 * (size_t)k, qmaxk, qmink);
             double e_[8];
-            reconstruct(qi, dxi, dyi, qmaxi, qmini, g.eps2[i], delx, dely, c.gm1, e_[0], e_[1],
-                        e_[2], e_[3]);
-            reconstruct(qk, dxk, dyk, qmaxk, qmink, g.eps2[k], delx, dely, c.gm1, e_[4], e_[5],
-                        e_[6], e_[7]);
-            const KState si = kstate(e_[0], e_[1], e_[2], e_[3], nx, ny, c.pi);
-            const KState sk = kstate(e_[4], e_[5], e_[6], e_[7], nx, ny, c.pi);
+            KState si, sk;
+            if (kst) {
+                // the forward re-run taped both reconstructions of this slot
+                const double2 *tp =
+                    reinterpret_cast<const double2 *>(kst + ((size_t)i * g.kp + r) * KS_TAPE);
+                double v[KS_TAPE];
+#pragma unroll
+                for (int hh = 0; hh < KS_TAPE / 2; ++hh) {
+                    const double2 t2 = __ldg(tp + hh);
+                    v[2 * hh] = t2.x;
+                    v[2 * hh + 1] = t2.y;
+                }
+                si = KState{v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7], v[8]};
+                sk = KState{v[11], v[12], v[13], v[14], v[15], v[16], v[17], v[18], v[19]};
+                e_[0] = v[9]; e_[1] = v[10]; e_[2] = si.rho; e_[3] = si.rho * si.pbr;
+                e_[4] = v[20]; e_[5] = v[21]; e_[6] = sk.rho; e_[7] = sk.rho * sk.pbr;
+            } else {
+                reconstruct(qi, dxi, dyi, qmaxi, qmini, g.eps2[i], delx, dely, c.gm1, e_[0],
+                            e_[1], e_[2], e_[3]);
+                reconstruct(qk, dxk, dyk, qmaxk, qmink, g.eps2[k], delx, dely, c.gm1, e_[4],
+                            e_[5], e_[6], e_[7]);
+                si = kstate(e_[0], e_[1], e_[2], e_[3], nx, ny, c.pi);
+                sk = kstate(e_[4], e_[5], e_[6], e_[7], nx, ny, c.pi);
+            }
             double *e = rec + r * BREC;
             // one converged evaluation per direction and list holding the
             // neighbour (two only at a zero projection), lists in ascending
@@ -890,10 +908,10 @@ void launch_update_b(const Geom &g, const Consts &c, const AdjConsts &a, const R
 void launch_flux_b(const Geom &g, const Consts &c, const R4 *q_in, const double *dq,
                    const double *qm, const double *delta, const double *frb, double *qb,
                    double *dqb, double *qmb, double *xb, double *yb, double *nxb, double *nyb,
-                   double *deltab, double *contrib, cudaStream_t s) {
+                   double *deltab, double *contrib, const double *kst, cudaStream_t s) {
     size_t smem = (size_t)GROUPS * g.kp * BREC * sizeof(double);
     k_flux_b<<<nblk(g.n, GROUPS), BLK, smem, s>>>(g, c, q_in, dq, qm, delta, frb, qb, dqb, qmb,
-                                                  xb, yb, nxb, nyb, deltab, contrib);
+                                                  xb, yb, nxb, nyb, deltab, contrib, kst);
 }
 
 void launch_inner_b(const Geom &g, const R4 *q, const double *dq_in, const double *dqb_out,

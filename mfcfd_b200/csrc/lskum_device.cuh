@@ -159,7 +159,8 @@ template <class T>
 __device__ __forceinline__ KStateT<T> reconstruct_kstate(const T q[4], const T dqx[4],
                                                          const T dqy[4], const T qmax[4],
                                                          const T qmin[4], T eps2, T delx, T dely,
-                                                         T inv_gm1, T nx, T ny, T inv_sqrt_pi) {
+                                                         T inv_gm1, T nx, T ny, T inv_sqrt_pi,
+                                                         T *u_out = nullptr) {
     T qt[4];
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
@@ -170,6 +171,10 @@ __device__ __forceinline__ KStateT<T> reconstruct_kstate(const T q[4], const T d
     const T beta = -qt[3] * T(0.5);
     const T temp = T(0.5) / beta;  // p / rho
     const T u1 = qt[1] * temp, u2 = qt[2] * temp;
+    if (u_out) {  // the adjoint's tape keeps the reconstructed velocity
+        u_out[0] = u1;
+        u_out[1] = u2;
+    }
     const T temp1 = qt[0] + beta * (u1 * u1 + u2 * u2);
     const T temp2 = temp1 - log(beta) * inv_gm1;
     KStateT<T> s;

@@ -92,7 +92,13 @@ struct StageBufs {
     double *spd;         // |u| + 3 sqrt(p/rho) of prim_out (last stage)
     double *res_part;    // per-block sums of res_sqr (last stage)
     double *flux_dbg;    // [n][4] flux_res, or nullptr
+    // per (point, slot) the two reconstructed kinetic states and velocities
+    // ([n][kp][KS_TAPE], the adjoint's tape), or nullptr
+    double *kstape = nullptr;
 };
+// doubles per (point, slot) in the kinetic-state tape: for the point's and
+// then the neighbour's reconstruction rho ut un p/rho |u|^2 B1 B2 erf1 erf2 u1 u2
+constexpr int KS_TAPE = 22;
 
 // The passes of one stage.  Each is a grid-stride kernel over the tiles of
 // the scheduled instances; `block` threads per block for the point passes

@@ -304,6 +304,9 @@ constexpr int FLUX_WARPS = FLUX_BLOCK / 32;
 constexpr int GROUP_SMEM = LPP * REC + 7 * LPP;
 constexpr int WARP_SMEM = PPW * GROUP_SMEM + CHUNK * GST + CHUNK;
 
+// TAPE: also write both reconstructed kinetic states of every slot to
+// b.kstape (the adjoint's taped re-run; the primal runs TAPE = false).
+template <bool TAPE>
 __device__ __forceinline__ void
 flux_group(const Geom &g, const Consts &c, const StageBufs &b, int i, bool valid, int kind0,
            double *rec, double *Gout) {
@@ -350,6 +353,7 @@ flux_group(const Geom &g, const Consts &c, const StageBufs &b, int i, bool valid
             // then the point's own state, re-read per slot from L1 so nothing
             // but the neighbour's kinetic state stays live across the two
             KState sk, si;
+            double uk[2], ui[2];
             {
                 const R4 kv = ld4(b.q_in + k);
                 const double qk[4] = {kv.a, kv.b, kv.c, kv.d};
@@ -357,7 +361,7 @@ flux_group(const Geom &g, const Consts &c, const StageBufs &b, int i, bool valid
                 ld8w(b.dq + 8 * (size_t)k, dxk, dyk);
                 ld8w(b.qm + 8 * (size_t)k, qmaxk, qmink);
                 sk = reconstruct_kstate(qk, dxk, dyk, qmaxk, qmink, g.eps2[k], delx, dely,
-                                        inv_gm1, nx, ny, inv_sqrt_pi);
+                                        inv_gm1, nx, ny, inv_sqrt_pi, TAPE ? uk : nullptr);
             }
             {
                 const R4 qv = ld4(b.q_in + i);
@@ -366,7 +370,17 @@ flux_group(const Geom &g, const Consts &c, const StageBufs &b, int i, bool valid
                 ld8w(b.dq + 8 * (size_t)i, dxi, dyi);
                 ld8w(b.qm + 8 * (size_t)i, qmaxi, qmini);
                 si = reconstruct_kstate(qi, dxi, dyi, qmaxi, qmini, g.eps2[i], delx, dely,
-                                        inv_gm1, nx, ny, inv_sqrt_pi);
+                                        inv_gm1, nx, ny, inv_sqrt_pi, TAPE ? ui : nullptr);
+            }
+            if (TAPE) {
+                const double v[KS_TAPE] = {si.rho, si.ut, si.un, si.pbr, si.usq, si.B1, si.B2,
+                                           si.e1,  si.e2, ui[0], ui[1], sk.rho, sk.ut, sk.un,
+                                           sk.pbr, sk.usq, sk.B1, sk.B2, sk.e1, sk.e2, uk[0],
+                                           uk[1]};
+                double2 *tp = reinterpret_cast<double2 *>(
+                    b.kstape + ((size_t)i * g.kp + r) * KS_TAPE);
+#pragma unroll
+                for (int h = 0; h < KS_TAPE / 2; ++h) tp[h] = make_double2(v[2 * h], v[2 * h + 1]);
             }
             const double tx = ny, ty = -nx;
             const double dels = delx * tx + dely * ty;
@@ -522,6 +536,7 @@ update_point(const Geom &g, const Consts &c, const StageBufs &b, int rk, int las
 // lands in slot (instance's first tile + tile number), summed over its 16
 // points in point order, so an instance's residual sums do not depend on the
 // other instances or on the launch shape.
+template <bool TAPE>
 __global__ void __launch_bounds__(FLUX_BLOCK, FLUX_MIN_BLOCKS)
 kb_flux(Geom g, Consts c, Sched s, StageBufs b, int rk, int last) {
     __shared__ double sm[FLUX_WARPS * WARP_SMEM];
@@ -555,7 +570,8 @@ kb_flux(Geom g, Consts c, Sched s, StageBufs b, int rk, int last) {
                 i = t.base + j;
                 kind = j < t.nw ? KIND_WALL : (j < t.nw + t.no ? KIND_OUTER : KIND_INTERIOR);
             }
-            flux_group(g, c, b, i, valid, kind, rec + (lane / LPP) * GROUP_SMEM, wG + GST * pj);
+            flux_group<TAPE>(g, c, b, i, valid, kind, rec + (lane / LPP) * GROUP_SMEM,
+                             wG + GST * pj);
         }
         __syncwarp();
         // the chunk's state updates, one point per lane
@@ -821,7 +837,7 @@ int batch_occupancy(int kind, bool fp32, int block, size_t smem) {
     cudaError_t e = cudaErrorInvalidValue;
     if (kind == 0) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_grad, block, smem);
     else if (kind == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_inner, block, smem);
-    else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_flux, block, smem);
+    else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_flux<false>, block, smem);
     return e == cudaSuccess ? nb : 1;
 }
 
@@ -841,9 +857,9 @@ void launch_inner(const Geom &g, const Consts &c, const Sched &s, const R4 *q,
 
 void launch_flux(const Geom &g, const Consts &c, const Sched &s, const StageBufs &b, int rk,
                  bool last, int grid, cudaStream_t st) {
-    size_t smem = flux_smem_bytes(g.kp);
-    kb_flux<<<wave(2, FLUX_BLOCK, smem, grid), FLUX_BLOCK, smem, st>>>(g, c, s, b, rk,
-                                                                      last ? 1 : 0);
+    const int gr = wave(2, FLUX_BLOCK, 0, grid);
+    if (b.kstape) kb_flux<true><<<gr, FLUX_BLOCK, 0, st>>>(g, c, s, b, rk, last ? 1 : 0);
+    else kb_flux<false><<<gr, FLUX_BLOCK, 0, st>>>(g, c, s, b, rk, last ? 1 : 0);
 }
 
 void launch_residual(const InstInfo *inst, int n_inst, const double *res_part, Ctl *ctl,
