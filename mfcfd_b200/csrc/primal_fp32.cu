@@ -52,21 +52,17 @@ __device__ __forceinline__ void stf8(float *p, const float a[4], const float b[4
     v[1] = make_float4(b[0], b[1], b[2], b[3]);
 }
 
-// Staged neighbour gathers, as in the FP64 D and I passes: a thread copies
+// Staged neighbour gathers of the D pass, as in the FP64 D pass: a thread copies
 // the rows of a round of stencil slots into its own shared-memory slots with
 // cp.async (no registers held while the copies fly), waits once, and sums in
 // slot order from shared memory.  16-byte units, thread-minor
 // (sb[unit * blockDim + thread]).  D pass units: the neighbour's q row, then
-// (slot offset dx dy, neighbour spd); I pass: the two halves of the
-// neighbour's dq row, then (slot offset, -).
+// (slot offset dx dy, neighbour spd).  (The I pass gathers one 32-byte dq
+// row per slot in a 256-bit load; staging it was measured slower.)
 #ifndef STAGE32
 #define STAGE32 8    // slots per round, D pass
 #endif
-#ifndef STAGE32_I
-#define STAGE32_I 4  // slots per round, I pass
-#endif
 constexpr int UNITS32_D = 2;
-constexpr int UNITS32_I = 3;
 
 __device__ __forceinline__ void cp16(void *dst, const void *src) {
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
@@ -176,40 +172,21 @@ kb_grad32(Geom g, Consts c, Geom32 f, Sched s, const float4 *__restrict__ q,
 // arithmetic; only the neighbours' derivatives are gathered (no q).
 __device__ __forceinline__ void
 inner32_point(const Geom &g, const Geom32 &f, const float *__restrict__ dq0,
-              const float *__restrict__ dq_in, float *__restrict__ dq_out, int i, float4 *sb) {
-    const int T = blockDim.x;
+              const float *__restrict__ dq_in, float *__restrict__ dq_out, int i) {
     float tx[4] = {0.f, 0.f, 0.f, 0.f}, ty[4] = {0.f, 0.f, 0.f, 0.f};
     const int nb = g.nbhs[i];
-    for (int r0 = 0; r0 < nb; r0 += STAGE32_I) {
-        const int m = min(STAGE32_I, nb - r0);
-        int kk[STAGE32_I];
+    for (int r = 0; r < nb; ++r) {
+        const int k = g.conn[r * g.n + i];
+        const float2 d = __ldg(f.dxy + r * g.n + i);
+        const float w = f.w ? __ldg(f.w + r * g.n + i) : 1.0f;
+        float dxk[4], dyk[4];
+        ldf8w(dq_in + 8 * (size_t)k, dxk, dyk);
+        const float wdx = w * d.x, wdy = w * d.y;
 #pragma unroll
-        for (int t = 0; t < STAGE32_I; ++t)
-            kk[t] = t < m ? __ldg(g.conn + (r0 + t) * g.n + i) : 0;
-#pragma unroll
-        for (int t = 0; t < STAGE32_I; ++t) {
-            if (t < m) {
-                float4 *d = sb + t * UNITS32_I * T;
-                const float4 *row = reinterpret_cast<const float4 *>(dq_in + 8 * (size_t)kk[t]);
-                cp16(d, row);
-                cp16(d + T, row + 1);
-                cp8(d + 2 * T, f.dxy + (r0 + t) * g.n + i);
-            }
-        }
-        cp_wait_all();
-        for (int t = 0; t < m; ++t) {
-            const float4 *d = sb + t * UNITS32_I * T;
-            const float4 a = d[0], b = d[T], gs = d[2 * T];
-            const float dxk[4] = {a.x, a.y, a.z, a.w}, dyk[4] = {b.x, b.y, b.z, b.w};
-            const int r = r0 + t;
-            const float w = f.w ? __ldg(f.w + r * g.n + i) : 1.0f;
-            const float wdx = w * gs.x, wdy = w * gs.y;
-#pragma unroll
-            for (int mm = 0; mm < 4; ++mm) {
-                const float pk = gs.x * dxk[mm] + gs.y * dyk[mm];
-                tx[mm] = tx[mm] + wdx * pk;
-                ty[mm] = ty[mm] + wdy * pk;
-            }
+        for (int m = 0; m < 4; ++m) {
+            const float pk = d.x * dxk[m] + d.y * dyk[m];
+            tx[m] = tx[m] + wdx * pk;
+            ty[m] = ty[m] + wdy * pk;
         }
     }
     float dxi[4], dyi[4], dx0[4], dy0[4];
@@ -228,14 +205,13 @@ inner32_point(const Geom &g, const Geom32 &f, const float *__restrict__ dq0,
 __global__ void __launch_bounds__(GRAD_BLOCK)
 kb_inner32(Geom g, Geom32 f, Sched s, const float *__restrict__ dq0,
            const float *__restrict__ dq_in, float *__restrict__ dq_out) {
-    extern __shared__ float4 sbi32[];
     __shared__ SchedSmem ss;
     load_sched(s, ss);
     const int total = ss.pre[ss.nact] * TILE;
     for (int vp = blockIdx.x * blockDim.x + threadIdx.x; vp < total;
          vp += gridDim.x * blockDim.x) {
         const int i = sched_point(s, ss, vp);
-        if (i >= 0) inner32_point(g, f, dq0, dq_in, dq_out, i, sbi32 + threadIdx.x);
+        if (i >= 0) inner32_point(g, f, dq0, dq_in, dq_out, i);
     }
 }
 
@@ -537,15 +513,11 @@ inline int nblk(int n, int b) { return (n + b - 1) / b; }
 }  // namespace
 
 size_t grad32_smem_bytes(int block) { return (size_t)block * STAGE32 * UNITS32_D * 16; }
-size_t inner32_smem_bytes(int block) { return (size_t)block * STAGE32_I * UNITS32_I * 16; }
+size_t inner32_smem_bytes(int) { return 0; }
 
 cudaError_t init_kernels32() {
-    cudaError_t e = cudaFuncSetAttribute(kb_grad32, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)grad32_smem_bytes(GRAD_BLOCK));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(kb_inner32, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)inner32_smem_bytes(GRAD_BLOCK));
-    return e;
+    return cudaFuncSetAttribute(kb_grad32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)grad32_smem_bytes(GRAD_BLOCK));
 }
 
 // the flux pass's shared memory is static (independent of the stencil size)
@@ -582,8 +554,7 @@ void launch_inner32(const Geom &g, const Consts &c, const Geom32 &f, const Sched
                     const float *dq0, const float *dq_in, float *dq_out, int block, int grid,
                     cudaStream_t st) {
     (void)c;
-    const size_t smem = inner32_smem_bytes(block);
-    kb_inner32<<<wave32(1, block, smem, grid), block, smem, st>>>(g, f, s, dq0, dq_in, dq_out);
+    kb_inner32<<<wave32(1, block, 0, grid), block, 0, st>>>(g, f, s, dq0, dq_in, dq_out);
 }
 
 void launch_flux32(const Geom &g, const Consts &c, const Sched &s, const StageBufs32 &b,

@@ -83,11 +83,7 @@ __device__ __forceinline__ void ld8w(const double *p, double a[4], double b[4]) 
 #ifndef STAGE_D
 #define STAGE_D 8  // slots per round, D pass
 #endif
-#ifndef STAGE_I
-#define STAGE_I 4  // slots per round, I pass
-#endif
 constexpr int PAIRS_D = 4;  // q[0..1], q[2..3], (x, y), (spd, -)
-constexpr int PAIRS_I = 7;  // q[0..1], q[2..3], dq[0..1], dq[2..3], dq[4..5], dq[6..7], (x, y)
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
@@ -194,11 +190,13 @@ kb_grad(Geom g, Consts c, Sched s, const R4 *__restrict__ q, const double *__res
 
 // q_variables.F90:115-227 eval_q_inner_loop + eval_update_innerloop: reads
 // dq_in, writes dq_out (the buffers swap instead of copying temp into dq).
+// A thread per point with its neighbour rows in 256-bit loads: staging them
+// in shared memory as the D pass does was measured slower here (C2: 0.156
+// against 0.121 ms per launch), since a slot moves 112 bytes in seven 16-byte
+// copies where two 256-bit loads and two narrower ones fetch it directly.
 __device__ __forceinline__ void
 inner_point(const Geom &g, const Consts &c, const R4 *__restrict__ q,
-            const double *__restrict__ dq_in, double *__restrict__ dq_out, int i, double2 *sb) {
-    const int T = blockDim.x;
-    const int nb = g.nbhs[i];
+            const double *__restrict__ dq_in, double *__restrict__ dq_out, int i) {
     double2 pi_ = g.xy[i];
     R4 qv = ld4w(q + i);
     double qi[4] = {qv.a, qv.b, qv.c, qv.d};
@@ -206,48 +204,26 @@ inner_point(const Geom &g, const Consts &c, const R4 *__restrict__ q,
     ld8w(dq_in + 8 * (size_t)i, dxi, dyi);
     double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
     double sdxq[4] = {0.0, 0.0, 0.0, 0.0}, sdyq[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int r0 = 0; r0 < nb; r0 += STAGE_I) {
-        const int m = min(STAGE_I, nb - r0);
-        int kk[STAGE_I];
+    int nb = g.nbhs[i];
+    for (int r = 0; r < nb; ++r) {
+        int k = g.conn[r * g.n + i];
+        R4 kv = ld4w(q + k);
+        double qk[4] = {kv.a, kv.b, kv.c, kv.d};
+        double dxk[4], dyk[4];
+        ld8w(dq_in + 8 * (size_t)k, dxk, dyk);
+        double2 pk = g.xy[k];
+        double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
+        double w = 1.0;
+        if (!c.power_zero) w = pow(sqrt(delx * delx + dely * dely), c.power);
+        sdx2 = sdx2 + delx * delx * w;
+        sdy2 = sdy2 + dely * dely * w;
+        sdxy = sdxy + delx * dely * w;
 #pragma unroll
-        for (int t = 0; t < STAGE_I; ++t) kk[t] = t < m ? __ldg(g.conn + (r0 + t) * g.n + i) : 0;
-#pragma unroll
-        for (int t = 0; t < STAGE_I; ++t) {
-            if (t < m) {
-                double2 *d = sb + t * PAIRS_I * T;
-                const double2 *row = reinterpret_cast<const double2 *>(q + kk[t]);
-                const double2 *drow = reinterpret_cast<const double2 *>(dq_in + 8 * (size_t)kk[t]);
-                cp_async16(d, row);
-                cp_async16(d + T, row + 1);
-                cp_async16(d + 2 * T, drow);
-                cp_async16(d + 3 * T, drow + 1);
-                cp_async16(d + 4 * T, drow + 2);
-                cp_async16(d + 5 * T, drow + 3);
-                cp_async16(d + 6 * T, g.xy + kk[t]);
-            }
-        }
-        cp_async_wait_all();
-        for (int t = 0; t < m; ++t) {
-            const double2 *d = sb + t * PAIRS_I * T;
-            const double2 a = d[0], b = d[T];
-            const double2 e0 = d[2 * T], e1 = d[3 * T], e2 = d[4 * T], e3 = d[5 * T];
-            const double2 pk = d[6 * T];
-            const double qk[4] = {a.x, a.y, b.x, b.y};
-            const double dxk[4] = {e0.x, e0.y, e1.x, e1.y};
-            const double dyk[4] = {e2.x, e2.y, e3.x, e3.y};
-            double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
-            double w = 1.0;
-            if (!c.power_zero) w = pow(sqrt(delx * delx + dely * dely), c.power);
-            sdx2 = sdx2 + delx * delx * w;
-            sdy2 = sdy2 + dely * dely * w;
-            sdxy = sdxy + delx * dely * w;
-#pragma unroll
-            for (int mm = 0; mm < 4; ++mm) {
-                double temp1 = qi[mm] - 0.5 * (delx * dxi[mm] + dely * dyi[mm]);
-                double temp2 = qk[mm] - 0.5 * (delx * dxk[mm] + dely * dyk[mm]);
-                sdxq[mm] = sdxq[mm] + (w * delx * (temp2 - temp1));
-                sdyq[mm] = sdyq[mm] + (w * dely * (temp2 - temp1));
-            }
+        for (int m = 0; m < 4; ++m) {
+            double temp1 = qi[m] - 0.5 * (delx * dxi[m] + dely * dyi[m]);
+            double temp2 = qk[m] - 0.5 * (delx * dxk[m] + dely * dyk[m]);
+            sdxq[m] = sdxq[m] + (w * delx * (temp2 - temp1));
+            sdyq[m] = sdyq[m] + (w * dely * (temp2 - temp1));
         }
     }
     double det = sdx2 * sdy2 - sdxy * sdxy;
@@ -264,14 +240,13 @@ inner_point(const Geom &g, const Consts &c, const R4 *__restrict__ q,
 __global__ void __launch_bounds__(GRAD_BLOCK)
 kb_inner(Geom g, Consts c, Sched s, const R4 *__restrict__ q, const double *__restrict__ dq_in,
          double *__restrict__ dq_out) {
-    extern __shared__ double2 sbi[];
     __shared__ SchedSmem ss;
     load_sched(s, ss);
     const int total = ss.pre[ss.nact] * TILE;
     for (int vp = blockIdx.x * blockDim.x + threadIdx.x; vp < total;
          vp += gridDim.x * blockDim.x) {
         const int i = sched_point(s, ss, vp);
-        if (i >= 0) inner_point(g, c, q, dq_in, dq_out, i, sbi + threadIdx.x);
+        if (i >= 0) inner_point(g, c, q, dq_in, dq_out, i);
     }
 }
 
@@ -798,15 +773,11 @@ int flux_blocks(int n) { return nblk(n, TILE); }
 int flux_grid_blocks(int n) { return nblk(nblk(n, TILE), 2 * FLUX_WARPS); }
 
 size_t grad_smem_bytes(int block) { return (size_t)block * STAGE_D * PAIRS_D * sizeof(double2); }
-size_t inner_smem_bytes(int block) { return (size_t)block * STAGE_I * PAIRS_I * sizeof(double2); }
+size_t inner_smem_bytes(int) { return 0; }
 
 cudaError_t init_kernels() {
-    cudaError_t e = cudaFuncSetAttribute(kb_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)grad_smem_bytes(GRAD_BLOCK));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(kb_inner, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)inner_smem_bytes(GRAD_BLOCK));
-    return e;
+    return cudaFuncSetAttribute(kb_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)grad_smem_bytes(GRAD_BLOCK));
 }
 
 int wave_blocks(int dev, int kind, int block, size_t smem, bool fp32) {
@@ -851,8 +822,7 @@ void launch_grad(const Geom &g, const Consts &c, const Sched &s, const R4 *q, co
 
 void launch_inner(const Geom &g, const Consts &c, const Sched &s, const R4 *q,
                   const double *dq_in, double *dq_out, int block, int grid, cudaStream_t st) {
-    const size_t smem = inner_smem_bytes(block);
-    kb_inner<<<wave(1, block, smem, grid), block, smem, st>>>(g, c, s, q, dq_in, dq_out);
+    kb_inner<<<wave(1, block, 0, grid), block, 0, st>>>(g, c, s, q, dq_in, dq_out);
 }
 
 void launch_flux(const Geom &g, const Consts &c, const Sched &s, const StageBufs &b, int rk,

@@ -21,7 +21,7 @@ from tests.helpers import max_rel
 pytestmark = pytest.mark.gpu
 PRIM_RTOL = 1e-10
 RES_ATOL = 1e-9
-C1_STATED_ITERS = 400
+C1_STATED_ITERS = 300
 
 
 def _compare(g, flow, n):
