@@ -229,8 +229,12 @@ __device__ __forceinline__ void kahan_add(float &s, float &cmp, float v) {
 // their list derivatives in rounds of four points (eight lanes each, slots
 // taken eight at a time with the lane pairs' Kahan sums parked in shared
 // memory between slot rounds), then updates the 32 points one per lane.
+#ifndef FLUX32_CT
+#define FLUX32_CT 2  // tiles a warp owns: 2 (every lane updates a point) or 1
+#endif
 constexpr int PPW = 32 / LPP;
-constexpr int CHUNK = 2 * TILE;
+constexpr int CT = FLUX32_CT;
+constexpr int CHUNK = CT * TILE;
 constexpr int GST = 17;                                  // odd: no bank conflicts
 constexpr int FLUX_WARPS = FLUX_BLOCK / 32;
 constexpr int GROUP_SMEM = LPP * FREC + 4 * LPP;         // records + parked sums (doubles)
@@ -448,12 +452,11 @@ kb_flux32(Geom g, Consts c, Sched s, StageBufs32 b, int rk, int last) {
     double *wG = rec + PPW * GROUP_SMEM;
     double *wres = wG + CHUNK * GST;
     const int ntiles = ss.pre[ss.nact];
-    const int nchunks = (ntiles + 1) / 2;
+    const int nchunks = (ntiles + CT - 1) / CT;
     for (int ch = blockIdx.x * FLUX_WARPS + warp; ch < nchunks; ch += gridDim.x * FLUX_WARPS) {
-        const bool has1 = 2 * ch + 1 < ntiles;
         for (int rnd = 0; rnd < CHUNK / PPW; ++rnd) {
             const int pj = rnd * PPW + lane / LPP;
-            const int v = 2 * ch + (pj < TILE ? 0 : 1);
+            const int v = CT * ch + pj / TILE;
             bool valid = false;
             int i = 0, kind = KIND_INTERIOR;
             if (v < ntiles) {
@@ -466,10 +469,11 @@ kb_flux32(Geom g, Consts c, Sched s, StageBufs32 b, int rk, int last) {
             flux32_group(g, c, b, i, valid, kind, rec + (lane / LPP) * GROUP_SMEM, wG + GST * pj);
         }
         __syncwarp();
-        const int v = 2 * ch + (lane < TILE ? 0 : 1);
-        const TileRef t = sched_tile(s, ss, v < ntiles ? v : 2 * ch);
+        const int v = CT * ch + lane / TILE;  // lanes past the chunk idle here
+        const bool inchunk = lane < CHUNK && v < ntiles;
+        const TileRef t = sched_tile(s, ss, inchunk ? v : CT * ch);
         const int j = t.j0 + (lane % TILE);
-        const bool valid = v < ntiles && j < t.n;
+        const bool valid = inchunk && j < t.n;
         double rs = 0.0;
         if (valid) {
             const int kind = j < t.nw ? KIND_WALL : (j < t.nw + t.no ? KIND_OUTER : KIND_INTERIOR);
@@ -477,9 +481,9 @@ kb_flux32(Geom g, Consts c, Sched s, StageBufs32 b, int rk, int last) {
                                 wG + GST * lane);
         }
         if (last) {
-            wres[lane] = rs;
+            if (lane < CHUNK) wres[lane] = rs;
             __syncwarp();
-            if ((lane % TILE) == 0 && (lane < TILE || has1)) {
+            if ((lane % TILE) == 0 && inchunk) {
                 double acc = 0.0;
                 for (int q = 0; q < TILE; ++q) acc = acc + wres[lane + q];
                 b.res_part[t.tile] = acc;
