@@ -128,7 +128,7 @@ void launch_stage(mfcfd_t *h, cudaStream_t s, int rk, int A, int B, F after) {
         after();
         for (int t = 1; t <= m; ++t) {
             launch_inner(h->geom, h->consts, h->sched, q_in, h->d_dq[(t - 1) & 1],
-                         h->d_dq[t & 1], h->point_block, h->point_grid, s);
+                         h->d_dq[t & 1], h->point_block, h->inner_grid, s);
             after();
         }
         StageBufs b;
@@ -153,7 +153,7 @@ void launch_stage(mfcfd_t *h, cudaStream_t s, int rk, int A, int B, F after) {
         for (int t = 1; t <= m; ++t) {
             launch_inner32(h->geom, h->consts, h->geom32, h->sched, h->f_dq[0],
                            h->f_dq[dq32_src(t)], h->f_dq[dq32_dst(t)], h->point_block,
-                           h->point_grid, s);
+                           h->inner_grid, s);
             after();
         }
         StageBufs32 b;
@@ -826,7 +826,9 @@ static int create_handle(const mfcfd_grid *grid, const mfcfd_params *params, int
     h->sched = sched_view(h->d_inst, h->d_sched);
     h->point_block = default_point_block(h->fp32);
     h->point_grid = std::min((nl + h->point_block - 1) / h->point_block,
-                             point_wave_blocks(h->dev, h->point_block, h->fp32));
+                             wave_blocks(h->dev, 0, h->point_block, 0, h->fp32));
+    h->inner_grid = std::min((nl + h->point_block - 1) / h->point_block,
+                             wave_blocks(h->dev, 1, h->point_block, 0, h->fp32));
     h->flux_grid = std::min(flux_grid_blocks(nl),
                             wave_blocks(h->dev, 2, 128,
                                         h->fp32 ? flux32_smem_bytes(kp) : flux_smem_bytes(kp),
@@ -1315,7 +1317,7 @@ extern "C" int mfcfd_part_phase(mfcfd_t *h, int phase, int rk, int t, double *va
     case MFCFD_PHASE_INNER:
         if (t < 1 || t > m) return fail(h, MFCFD_ERR_ARG, "inner iteration t out of range");
         launch_inner(h->geom, h->consts, h->sched, h->d_q[h->qcur], h->d_dq[(t - 1) & 1],
-                     h->d_dq[t & 1], h->point_block, h->point_grid, s);
+                     h->d_dq[t & 1], h->point_block, h->inner_grid, s);
         h->part_dq = t & 1;
         break;
     case MFCFD_PHASE_FLUX: {

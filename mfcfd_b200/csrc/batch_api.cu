@@ -93,6 +93,7 @@ struct mfcfd_batch {
     cudaStream_t own = nullptr, stream = nullptr;
     cudaGraphExec_t pair_exec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     int point_block = 256, point_grid = 0, flux_grid = 0;  // effective launch shape
+    int inner_grid = 0;
     long long launches = 0;
     std::string err;
 };
@@ -151,7 +152,7 @@ void free_batch(mfcfd_batch_t *b) {
 
 // blocks in one wave of resident blocks of a batched pass
 int batch_wave(const mfcfd_batch_t *b, int kind, int block) {
-    if (kind == 0) return point_wave_blocks(b->dev, block, b->fp32);
+    if (kind < 2) return wave_blocks(b->dev, kind, block, 0, b->fp32);
     size_t smem = 0;
     if (kind == 2) smem = b->fp32 ? flux32_smem_bytes(b->kp) : flux_smem_bytes(b->kp);
     return wave_blocks(b->dev, kind, block, smem, b->fp32);
@@ -166,13 +167,16 @@ void set_shape(mfcfd_batch_t *b, int block, int waves, int ppt = 1) {
     const int fmax = flux_grid_blocks(b->ntiles * TILE);
     if (waves > 0) {
         b->point_grid = waves * batch_wave(b, 0, block);
+        b->inner_grid = waves * batch_wave(b, 1, block);
         b->flux_grid = waves * batch_wave(b, 2, 128);
     } else {
         ppt = std::max(1, ppt);
         b->point_grid = (b->ntot + block * ppt - 1) / (block * ppt);
+        b->inner_grid = b->point_grid;
         b->flux_grid = (fmax + ppt - 1) / ppt;
     }
     b->point_grid = std::max(1, std::min(b->point_grid, (b->ntot + block - 1) / block));
+    b->inner_grid = std::max(1, std::min(b->inner_grid, (b->ntot + block - 1) / block));
     b->flux_grid = std::max(1, std::min(b->flux_grid, fmax));
 }
 
@@ -181,14 +185,14 @@ void set_shape(mfcfd_batch_t *b, int block, int waves, int ppt = 1) {
 void batch_stage(mfcfd_batch_t *b, cudaStream_t s, int rk, int A, int B) {
     const int m = b->p.inner_iterations;
     const bool last = rk == b->p.rks;
-    const int pb = b->point_block, pg = b->point_grid, fg = b->flux_grid;
+    const int pb = b->point_block, pg = b->point_grid, ig = b->inner_grid, fg = b->flux_grid;
     if (!b->fp32) {
         const R4 *q_in = b->d_q[b->qcur];
         launch_grad(b->geom, b->consts, b->sched, q_in, b->d_spd, b->d_dq[0], b->d_qm,
                     b->d_delta, rk == 1, pb, pg, s);
         for (int t = 1; t <= m; ++t)
             launch_inner(b->geom, b->consts, b->sched, q_in, b->d_dq[(t - 1) & 1],
-                         b->d_dq[t & 1], pb, pg, s);
+                         b->d_dq[t & 1], pb, ig, s);
         StageBufs sb;
         sb.prim_in = rk == 1 ? b->d_prim[A] : b->d_prim[B];
         sb.prim_out = b->d_prim[B];
@@ -208,7 +212,7 @@ void batch_stage(mfcfd_batch_t *b, cudaStream_t s, int rk, int A, int B) {
                       b->f_qm, b->d_delta, rk == 1, pb, pg, s);
         for (int t = 1; t <= m; ++t)
             launch_inner32(b->geom, b->consts, b->geom32, b->sched, b->f_dq[0],
-                           b->f_dq[dq32_src(t)], b->f_dq[dq32_dst(t)], pb, pg, s);
+                           b->f_dq[dq32_src(t)], b->f_dq[dq32_dst(t)], pb, ig, s);
         StageBufs32 sb;
         sb.prim_in = rk == 1 ? b->f_prim[A] : b->f_prim[B];
         sb.prim_out = b->f_prim[B];
@@ -784,7 +788,9 @@ int mfcfd_batch_set_launch(mfcfd_batch_t *b, int point_block, int point_grid, in
         return bfail(b, MFCFD_ERR_ARG, "point_block must be 128 or 256, grids >= 0");
     BK(cudaStreamSynchronize(b->stream));
     set_shape(b, point_block, 1);
-    if (point_grid > 0) b->point_grid = std::min(point_grid, (b->ntot + point_block - 1) / point_block);
+    if (point_grid > 0)
+        b->point_grid = b->inner_grid =
+            std::min(point_grid, (b->ntot + point_block - 1) / point_block);
     if (flux_grid > 0) b->flux_grid = std::min(flux_grid, flux_grid_blocks(b->ntiles * TILE));
     drop_graphs(b);
     return MFCFD_OK;
@@ -806,6 +812,7 @@ int mfcfd_batch_tune(mfcfd_batch_t *b, int iters, double *ms_per_iter) {
     int st = MFCFD_OK;
     double best_ms = 0.0;
     int best_block = b->point_block, best_pg = b->point_grid, best_fg = b->flux_grid;
+    int best_ig = b->inner_grid;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     auto restore = [&]() -> int {
         BK(cudaMemcpyAsync(prim, save_prim, rows * row_bytes, cudaMemcpyDeviceToDevice, b->stream));
@@ -881,12 +888,14 @@ int mfcfd_batch_tune(mfcfd_batch_t *b, int iters, double *ms_per_iter) {
                 best_ms = per;
                 best_block = b->point_block;
                 best_pg = b->point_grid;
+                best_ig = b->inner_grid;
                 best_fg = b->flux_grid;
             }
         }
     if (save_prim && save_q && save_spd && st == MFCFD_OK) st = restore();
     b->point_block = best_block;
     b->point_grid = best_pg;
+    b->inner_grid = best_ig;
     b->flux_grid = best_fg;
     drop_graphs(b);
     if (save_prim) cudaFree(save_prim);

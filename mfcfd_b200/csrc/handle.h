@@ -59,6 +59,7 @@ struct mfcfd {
     BatchRun *d_run = nullptr; // no retirement but on a NaN residue
     Sched sched{};
     int point_block = 256, point_grid = 1, flux_grid = 1;  // launch shape
+    int inner_grid = 1;  // I pass (its residency differs from the D pass's)
 
     int cur = 0;   // prim buffer holding the state
     int qcur = 0;  // q buffer holding q of the state

@@ -141,11 +141,6 @@ size_t flux32_smem_bytes(int kp);
 // blocks of one wave of resident blocks of a pass on device dev (for the
 // point passes the staging memory of `block` replaces `smem`)
 int wave_blocks(int dev, int kind, int block, size_t smem, bool fp32);
-// blocks of one wave of both point passes (D and I share their launch shape)
-inline int point_wave_blocks(int dev, int block, bool fp32) {
-    const int a = wave_blocks(dev, 0, block, 0, fp32), b = wave_blocks(dev, 1, block, 0, fp32);
-    return a < b ? a : b;
-}
 // threads per block of the point passes (their staging buffers take up to
 // 512 B of shared memory a thread)
 inline int default_point_block(bool) { return 128; }

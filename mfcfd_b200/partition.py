@@ -278,7 +278,11 @@ class PartitionedSolver:
                                         part.plen, C.byref(h))
         _lib.check(st, None, "mfcfd_create_part")
         self.h = h
-        self.stream = torch.cuda.current_stream(self.device)
+        # one stream for the library's kernels and torch's packing: a stream
+        # of its own (the default stream's handle is 0, which the library
+        # reads as "keep your stream"), made torch's current stream
+        self.stream = torch.cuda.Stream(self.device)
+        torch.cuda.set_stream(self.stream)
         _lib.check(self.lib.mfcfd_set_stream(h, C.c_void_p(self.stream.cuda_stream)), h,
                    "mfcfd_set_stream")
         internal = np.empty(g.n, np.int32)

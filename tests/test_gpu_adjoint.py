@@ -111,18 +111,39 @@ def test_adjoint_leaves_the_final_state(gpu):
 @pytest.mark.parametrize("obj", ["cd", "cl"])
 def test_adjoint_on_the_16k_grid_from_a_developed_state(gpu, obj):
     """The adjoint configuration's 16,000-point grid (160 x 100, M 0.63, aoa 2
-    deg): a state developed for 500 iterations is held fixed, 100 iterations
-    are reversed, and dJ/dx, dJ/dy at 32 seeded points of the first four
-    rings (seed 3) are checked against central differences of the GPU primal
-    with h = 1e-6 chord."""
+    deg): a state developed for 500 iterations is held fixed and 100
+    iterations are reversed.  At 32 seeded points of the first four rings
+    (seed 3), dJ/dx and dJ/dy equal the forward-mode derivative along the
+    same coordinate (mfcfd_tangent, an independent linearisation) to 1e-9.
+    Central differences with h = 1e-6 chord agree only to about 0.5 % of the
+    largest derivative: over 100 iterations of a developed solution the
+    perturbation switches branches of the limiter (min(1, num/den) and its
+    1e-5 threshold), so the loop is not differentiable at that scale, and the
+    differences approach the linearisation only linearly in h (measured on
+    this grid: 3.5 %, 0.46 %, 0.13 % of the largest derivative at h = 1e-5,
+    1e-6, 1e-7)."""
     h = 1e-6
     g = naca_ogrid(160, 100, seed=3000, first_spacing="match", spacing="arc")
     flow = dict(cfl=0.2, vl_const=5.0, mach=0.63, aoa=2.0)
     n = 100
+    rng = np.random.default_rng(3)
+    pts = rng.choice(np.arange(4 * 160), size=32, replace=False)
     with Solver(g, **flow) as s:
         s.run(500)
         prim0 = s.get_state()
+        tan = []
+        for p in pts:
+            for ax in (0, 1):
+                e = np.zeros(g.n)
+                s.set_state(prim0)
+                tan.append(s.tangent(n, e if ax else _unit(g.n, p), _unit(g.n, p) if ax else e,
+                                     obj)[1])
+        s.set_state(prim0)
         J, dx, dy, _ = s.adjoint(n, obj)
+    adj = np.array([v for p in pts for v in (dx[p], dy[p])])
+    tan = np.array(tan)
+    scale = np.max(np.abs(tan))
+    assert np.max(np.abs(adj - tan)) <= 1e-9 * scale, np.max(np.abs(adj - tan)) / scale
 
     def J_of(gg):
         with Solver(gg, **flow) as t:
@@ -132,16 +153,17 @@ def test_adjoint_on_the_16k_grid_from_a_developed_state(gpu, obj):
         return float(cd.sum() if obj == "cd" else cl.sum())
 
     assert abs(J - J_of(g)) < 1e-12
-    rng = np.random.default_rng(3)
-    pts = rng.choice(np.arange(4 * 160), size=32, replace=False)
-    adj, fd = [], []
+    fd = []
     for p in pts:
-        for arr, grad in (("x", dx), ("y", dy)):
+        for arr in ("x", "y"):
             gp, gm = copy.deepcopy(g), copy.deepcopy(g)
             getattr(gp, arr)[p] += h
             getattr(gm, arr)[p] -= h
             fd.append((J_of(gp) - J_of(gm)) / (2 * h))
-            adj.append(grad[p])
-    adj, fd = np.array(adj), np.array(fd)
-    tol = 1e-6 * np.max(np.abs(fd)) + 1e-8
-    assert np.max(np.abs(adj - fd)) <= tol, (np.max(np.abs(adj - fd)), tol)
+    assert np.max(np.abs(np.array(fd) - adj)) <= 1e-2 * scale
+
+
+def _unit(n, p):
+    e = np.zeros(n)
+    e[p] = 1.0
+    return e
