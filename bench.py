@@ -226,9 +226,9 @@ def adjoint_cost(args, stream, world, dist):
     """Adjoint/primal cost on the adjoint configuration (640 x 400 = 256,000
     points, M 0.63, aoa 2 deg): a state developed for --adjoint-develop
     iterations is held fixed; the primal run of n iterations from it and the
-    reverse-mode gradient over the same n iterations (binomial checkpoints of
-    prim within 2 GB) are device-timed on the same stream, for J = Cd and
-    J = Cl.  The Cd call is the handle's first and also allocates its tape
+    reverse-mode gradient over the same n iterations (prim snapshots of every
+    iteration, or binomial checkpoints within --adjoint-ckpt-bytes) are
+    device-timed on the same stream, for J = Cd and J = Cl.  The Cd call is the handle's first and also allocates its tape
     and snapshot pool (tens of ms, inside its time)."""
     import torch
     from mfcfd_b200.grid import config_flow, config_grid
@@ -236,7 +236,11 @@ def adjoint_cost(args, stream, world, dist):
     grid = config_grid(args.adjoint_config)
     flow = config_flow(args.adjoint_config)
     n = args.adjoint_iters
-    budget = 2 << 30
+    # snapshots of every iteration's input state fit in HBM (32 B a point per
+    # iteration: 16.4 GB for 2,000 iterations of 256,000 points), so each
+    # iteration is run forward once and re-run once with its tape; a smaller
+    # --adjoint-ckpt-bytes places fewer snapshots by the binomial rule
+    budget = args.adjoint_ckpt_bytes or (n + 1) * 32 * grid.n
     # untimed warm-up: the first call of a kernel in a process loads its module
     from mfcfd_b200.grid import naca_ogrid
     with Solver(naca_ogrid(32, 12, seed=1, first_spacing=5e-3), **flow) as w:
@@ -267,13 +271,38 @@ def adjoint_cost(args, stream, world, dist):
     primal_ms, cd_ms, cl_ms = max_over_ranks([primal_ms, out["cd"][0], out["cl"][0]], dist)
     return {"config": (f"{args.adjoint_config}: {grid.n:,} points, M {flow['mach']}, aoa "
                        f"{flow['aoa']} deg, {n} iterations reversed from a state developed for "
-                       f"{args.adjoint_develop}, prim snapshots within 2 GB"),
+                       f"{args.adjoint_develop}, prim snapshots within "
+                       f"{budget / 2**30:.1f} GiB"),
             "primal_ms": primal_ms,
             "adjoint_ms": {"cd": cd_ms, "cl": cl_ms},
             "cost_ratio": cd_ms / primal_ms, "cost_ratio_cl": cl_ms / primal_ms,
             "forward_iterations": out["cd"][2], "checkpoint_budget_bytes": budget,
             "J": {"cd": out["cd"][1], "cl": out["cl"][1]},
             "grad_max": {"cd": out["cd"][3], "cl": out["cl"][3]}}
+
+
+def fp32_accuracy(grid, flow: dict, n_iters: int, stream, label: str) -> dict:
+    """The FP32-mixed loop against the FP64 loop after n_iters iterations from
+    freestream on the same grid: Cl, Cd and prim (RMS and max of the
+    difference relative to max(|prim|, 1e-3 max|prim| of the component))."""
+    from mfcfd_b200.solver import Solver
+    with Solver(grid, **flow) as a, Solver(grid, precision="fp32_mixed", **flow) as b:
+        a.set_stream(stream.cuda_stream)
+        b.set_stream(stream.cuda_stream)
+        ra, rb = a.run(n_iters), b.run(n_iters)
+        if len(ra) != n_iters or len(rb) != n_iters:
+            return {"config": label, "iterations": n_iters, "nonfinite": True,
+                    "iterations_done": [len(ra), len(rb)]}
+        pa, pb = a.get_state(), b.get_state()
+        cla, cda, _, _ = a.forces()
+        clb, cdb, _, _ = b.forces()
+    scale = np.maximum(np.abs(pa), 1e-3 * np.max(np.abs(pa), axis=0))
+    err = np.abs(pb - pa) / scale
+    return {"config": label, "iterations": n_iters,
+            "dCl": abs(float(clb[0] - cla[0])), "dCd": abs(float(cdb[0] - cda[0])),
+            "Cl_fp64": float(cla[0]), "Cd_fp64": float(cda[0]),
+            "prim_rms_rel": float(np.sqrt(np.mean(err ** 2))), "prim_max_rel": float(err.max()),
+            "residue_fp64": float(ra[-1]), "residue_fp32": float(rb[-1])}
 
 
 def adjoint_batch_leg(args, world, rank, dist):
@@ -401,11 +430,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--fp32-check-iters", type=int, default=300,
+                    help="iterations from freestream after which the FP32-mixed loop is "
+                         "compared with the FP64 loop on the bench grid (0 = skip)")
     ap.add_argument("--adjoint-iters", type=int, default=2000,
                     help="iterations reversed by the adjoint-cost leg (0 = skip)")
     ap.add_argument("--adjoint-develop", type=int, default=1000,
                     help="iterations that develop the adjoint leg's starting state")
     ap.add_argument("--adjoint-config", default="C3")
+    ap.add_argument("--adjoint-ckpt-bytes", type=int, default=0,
+                    help="snapshot budget of the adjoint leg (0 = one snapshot per iteration)")
     ap.add_argument("--batch-iters", type=int, default=100,
                     help="iterations of the batched-workload leg (0 = skip)")
     ap.add_argument("--batch-instances", type=int, default=64)
@@ -511,9 +545,13 @@ def main():
                 "dCl": abs(float(cl32[0] - cl64[0])), "dCd": abs(float(cd32[0] - cd64[0])),
                 "Cl_fp64": float(cl64[0]), "Cd_fp64": float(cd64[0]),
                 "kernel_ms": {k: float(v) for k, v in kt32.items()},
-                "note": "FP32 state, fluxes, sums and state update; geometry (LSQ "
-                        "inverses) formed in FP64 once; FP64 residual and forces; dCl/dCd "
-                        "against the FP64 run after the same iterations"}
+                "note": "FP32 state, fluxes and Kahan sums; the state update's arithmetic, "
+                        "the geometry (LSQ inverses, formed once), the residual and the "
+                        "forces in FP64; dCl/dCd against the FP64 run after the same "
+                        "iterations, 'accuracy' after --fp32-check-iters from freestream"}
+        if args.fp32_check_iters > 0 and not halted32:
+            fp32["accuracy"] = fp32_accuracy(grid, f, args.fp32_check_iters, stream,
+                                             cfg["workload"].split(":")[0])
         if halted32:
             fp32.update(value=None, speedup_vs_fp64=None, ms_per_step=None,
                         nonfinite=True, iterations_done=len(res32),

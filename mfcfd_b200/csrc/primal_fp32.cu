@@ -25,7 +25,7 @@ constexpr int LPP = 8;
 constexpr int FLUX_BLOCK = 128;  // four independent warps
 constexpr int FREC = 9;   // dGxp..dGyn as 16 floats, then dels*w, deln*w (18 floats)
 #ifndef FLUX32_MIN_BLOCKS
-#define FLUX32_MIN_BLOCKS 6              // <= 80 registers; shared memory allows 6 blocks
+#define FLUX32_MIN_BLOCKS 8              // <= 64 registers; a one-tile chunk's shared memory allows 8 blocks
 #endif
 constexpr double OBT = 1.0 / 3.0;
 constexpr double TBT = 2.0 / 3.0;
@@ -230,8 +230,51 @@ __device__ __forceinline__ void kahan_add(float &s, float &cmp, float v) {
 // taken eight at a time with the lane pairs' Kahan sums parked in shared
 // memory between slot rounds), then updates the 32 points one per lane.
 #ifndef FLUX32_CT
-#define FLUX32_CT 2  // tiles a warp owns: 2 (every lane updates a point) or 1
+#define FLUX32_CT 1  // tiles a warp owns: 1 (0.366 ms per C2 launch) or 2 (every lane updates a point; 0.375 ms)
 #endif
+// Arithmetic types of the flux pass: RT for the reconstruction to the
+// kinetic state, FT for the split fluxes and their differences, UT for the
+// state update.  The state is stored in FP32 throughout.  The update runs in
+// FP64: its conversions prim -> U -> prim, four times an iteration, are what
+// moved the FP32-mixed loop away from the FP64 loop (640x400 grid, 2,000
+// iterations from freestream: |dCd| 1.1e-5 with an FP32 update, 2.2e-7 with
+// an FP64 one, at 1.4 % of the pass's time), while FP64 reconstruction or
+// fluxes changed nothing measurable (|dCd| 1.10-1.12e-5 with either).
+#ifndef FLUX32_RT
+#define FLUX32_RT float
+#endif
+#ifndef FLUX32_FT
+#define FLUX32_FT float
+#endif
+#ifndef FLUX32_UT
+#define FLUX32_UT double
+#endif
+using RT = FLUX32_RT;
+using FT = FLUX32_FT;
+using UT = FLUX32_UT;
+template <class D, class S>
+__device__ __forceinline__ KStateT<D> kcast(const KStateT<S> &s) {
+    KStateT<D> d;
+    d.rho = (D)s.rho; d.ut = (D)s.ut; d.un = (D)s.un; d.pbr = (D)s.pbr; d.usq = (D)s.usq;
+    d.B1 = (D)s.B1; d.B2 = (D)s.B2; d.e1 = (D)s.e1; d.e2 = (D)s.e2;
+    return d;
+}
+// the reconstructed kinetic state of point p along (dx, dy)
+__device__ __forceinline__ KStateT<FT> kstate32(const StageBufs32 &b, int p, RT dx, RT dy, RT inv_gm1,
+                                                RT nx, RT ny, RT inv_sqrt_pi) {
+    const float4 v = __ldg(b.q_in + p);
+    float dxf[4], dyf[4], qmaxf[4], qminf[4];
+    ldf8w(b.dq + 8 * (size_t)p, dxf, dyf);
+    ldf8w(b.qm + 8 * (size_t)p, qmaxf, qminf);
+    const RT q[4] = {v.x, v.y, v.z, v.w};
+    RT ddx[4], ddy[4], qmax[4], qmin[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        ddx[j] = dxf[j]; ddy[j] = dyf[j]; qmax[j] = qmaxf[j]; qmin[j] = qminf[j];
+    }
+    return kcast<FT>(reconstruct_kstate<RT>(q, ddx, ddy, qmax, qmin, (RT)b.eps2f[p], dx, dy,
+                                            inv_gm1, nx, ny, inv_sqrt_pi));
+}
 constexpr int PPW = 32 / LPP;
 constexpr int CT = FLUX32_CT;
 constexpr int CHUNK = CT * TILE;
@@ -246,18 +289,18 @@ flux32_group(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool v
     const int lane = threadIdx.x % LPP;
     int nb = 0, kind = KIND_INTERIOR;
     unsigned long long mx = 0, my = 0;
-    float nxf = 0.f, nyf = 1.f;
+    RT nxf = 0, nyf = 1;
     if (valid) {
         nb = g.nbhs[i];
         kind = kind0;
         mx = g.mx[i];
         my = g.my[i];
         const double2 nn = g.nrm[i];
-        nxf = (float)nn.x;
-        nyf = (float)nn.y;
+        nxf = (RT)nn.x;
+        nyf = (RT)nn.y;
     }
-    const float inv_gm1 = (float)(1.0 / c.gm1), inv_sqrt_pi = (float)(1.0 / sqrt(c.pi));
-    const float s2q = kind == KIND_WALL ? -1.0f : 1.0f;
+    const RT inv_gm1 = (RT)(1.0 / c.gm1), inv_sqrt_pi = (RT)(1.0 / sqrt(c.pi));
+    const FT s2q = kind == KIND_WALL ? FT(-1) : FT(1);
     const int nbw = __reduce_max_sync(0xffffffffu, nb);
     const int L = lane >> 1, c0 = (lane & 1) * 2;
     const bool used =
@@ -275,30 +318,13 @@ flux32_group(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool v
             const int k = g.conn[r * g.n + i];
             const float2 d = __ldg(b.f.dxy + r * g.n + i);
             const float dxf = d.x, dyf = d.y;
-            KStateT<float> sk, si;
-            {
-                const float4 kv = __ldg(b.q_in + k);
-                const float qk[4] = {kv.x, kv.y, kv.z, kv.w};
-                float dxk[4], dyk[4], qmaxk[4], qmink[4];
-                ldf8w(b.dq + 8 * (size_t)k, dxk, dyk);
-                ldf8w(b.qm + 8 * (size_t)k, qmaxk, qmink);
-                sk = reconstruct_kstate<float>(qk, dxk, dyk, qmaxk, qmink, b.eps2f[k], dxf, dyf,
-                                               inv_gm1, nxf, nyf, inv_sqrt_pi);
-            }
-            {
-                const float4 qv = __ldg(b.q_in + i);
-                const float qi[4] = {qv.x, qv.y, qv.z, qv.w};
-                float dxi[4], dyi[4], qmaxi[4], qmini[4];
-                ldf8w(b.dq + 8 * (size_t)i, dxi, dyi);
-                ldf8w(b.qm + 8 * (size_t)i, qmaxi, qmini);
-                si = reconstruct_kstate<float>(qi, dxi, dyi, qmaxi, qmini, b.eps2f[i], dxf, dyf,
-                                               inv_gm1, nxf, nyf, inv_sqrt_pi);
-            }
+            const KStateT<FT> sk = kstate32(b, k, dxf, dyf, inv_gm1, nxf, nyf, inv_sqrt_pi);
+            const KStateT<FT> si = kstate32(b, i, dxf, dyf, inv_gm1, nxf, nyf, inv_sqrt_pi);
             const float dels = dxf * nyf - dyf * nxf;
             const float deln = dxf * nxf + dyf * nyf;
             const float w = b.f.w ? __ldg(b.f.w + r * g.n + i) : 1.0f;
             float *ef = reinterpret_cast<float *>(rec + lane * FREC);
-            float Gi[4], Gk[4];
+            FT Gi[4], Gk[4];
 #pragma unroll
             for (int dd = 0; dd < 2; ++dd) {
                 // one converged evaluation per direction, as in the FP64 pass
@@ -308,21 +334,21 @@ flux32_group(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool v
                 for (int pass = 0; pass < 2; ++pass) {
                     if (pass == 0 ? !(in0 || in1) : !(in0 && in1)) continue;
                     const int Lx = 2 * dd + ((pass == 1 || !in0) ? 1 : 0);
-                    const float sg = (Lx & 1) ? -1.0f : 1.0f;
+                    const FT sg = (Lx & 1) ? FT(-1) : FT(1);
                     if (dd == 0) {
                         if (kind == KIND_INTERIOR) {
-                            flux_gx<float>(si, sg, Gi);
-                            flux_gx<float>(sk, sg, Gk);
+                            flux_gx<FT>(si, sg, Gi);
+                            flux_gx<FT>(sk, sg, Gk);
                         } else {
-                            flux_quad<float>(si, sg, s2q, Gi);
-                            flux_quad<float>(sk, sg, s2q, Gk);
+                            flux_quad<FT>(si, sg, s2q, Gi);
+                            flux_quad<FT>(sk, sg, s2q, Gk);
                         }
                     } else {
-                        flux_gy<float>(si, sg, Gi);
-                        flux_gy<float>(sk, sg, Gk);
+                        flux_gy<FT>(si, sg, Gi);
+                        flux_gy<FT>(sk, sg, Gk);
                     }
 #pragma unroll
-                    for (int m = 0; m < 4; ++m) ef[4 * Lx + m] = Gk[m] - Gi[m];
+                    for (int m = 0; m < 4; ++m) ef[4 * Lx + m] = (float)(Gk[m] - Gi[m]);
                 }
             }
             ef[16] = dels * w;
@@ -370,7 +396,8 @@ flux32_group(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool v
 }
 
 // state_update.F90:10-141 of one point from its four list derivatives
-// Gs[4L+m], in FP32; returns its res_sqr term (FP64).
+// Gs[4L+m]: FP32 state in and out, arithmetic in UT; returns its res_sqr
+// term (FP64).
 __device__ __forceinline__ double
 update32_point(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, int last, int i,
                int kind, int orow, const double *Gs) {
@@ -392,45 +419,44 @@ update32_point(const Geom &g, const Consts &c, const StageBufs32 &b, int rk, int
             else fr[m] = delta * (G[0][m] + G[1][m] + G[2][m] + G[3][m]);
         }
         if (b.flux_dbg) st4(reinterpret_cast<R4 *>(b.flux_dbg) + i, fr[0], fr[1], fr[2], fr[3]);
-        // state_update in FP32 (the state is stored in FP32); the residual
+        // state_update in UT (the state is stored in FP32); the residual
         // from the increment itself, 0.5 euler fr(1), in FP64, which FP32
         // differences of U(1) would cancel (last stage: rk != 3)
         if (kind != KIND_OUTER) res_sqr = (0.5 * c.euler * fr[0]) * (0.5 * c.euler * fr[0]);
-        const float nxf = (float)nx, nyf = (float)ny, pif = (float)c.pi, gm1f = (float)c.gm1;
-        float frf[4] = {(float)fr[0], (float)fr[1], (float)fr[2], (float)fr[3]};
+        const UT nxf = (UT)nx, nyf = (UT)ny, pif = (UT)c.pi, gm1f = (UT)c.gm1;
+        UT frf[4] = {(UT)fr[0], (UT)fr[1], (UT)fr[2], (UT)fr[3]};
         const float4 P = b.prim_in[i];
-        float U[4], Uo[4] = {0.f, 0.f, 0.f, 0.f};
+        UT U[4], Uo[4] = {0, 0, 0, 0};
         if (kind == KIND_OUTER) {
             const double *inf = g.obc + 8 * (size_t)orow;
-            const float inff[5] = {(float)inf[0], (float)inf[1], (float)inf[2], (float)inf[3],
-                                   (float)inf[4]};
-            conserved_ubar_t<float>(P.x, P.y, P.z, P.w, nxf, nyf, inff, pif, gm1f, U);
+            const UT inff[5] = {(UT)inf[0], (UT)inf[1], (UT)inf[2], (UT)inf[3], (UT)inf[4]};
+            conserved_ubar_t<UT>(P.x, P.y, P.z, P.w, nxf, nyf, inff, pif, gm1f, U);
             if (rk == 3) {
                 const float4 O = b.prim_old[i];
-                conserved_ubar_t<float>(O.x, O.y, O.z, O.w, nxf, nyf, inff, pif, gm1f, Uo);
+                conserved_ubar_t<UT>(O.x, O.y, O.z, O.w, nxf, nyf, inff, pif, gm1f, Uo);
             }
         } else {
-            prim_to_conserved_t<float>(P.x, P.y, P.z, P.w, nxf, nyf, U);
+            prim_to_conserved_t<UT>(P.x, P.y, P.z, P.w, nxf, nyf, U);
             if (rk == 3) {
                 const float4 O = b.prim_old[i];
-                prim_to_conserved_t<float>(O.x, O.y, O.z, O.w, nxf, nyf, Uo);
+                prim_to_conserved_t<UT>(O.x, O.y, O.z, O.w, nxf, nyf, Uo);
             }
         }
-        const float half_euler = (float)(0.5 * c.euler);
+        const UT half_euler = (UT)(0.5 * c.euler);
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
             if (rk != 3) U[m] = U[m] - half_euler * frf[m];
-            else U[m] = (float)TBT * Uo[m] + (float)OBT * (U[m] - 0.5f * frf[m]);
+            else U[m] = (UT)TBT * Uo[m] + (UT)OBT * (U[m] - UT(0.5) * frf[m]);
         }
-        if (kind == KIND_WALL) U[2] = 0.f;
-        const float U2_rot = U[1], U3_rot = U[2];
+        if (kind == KIND_WALL) U[2] = 0;
+        const UT U2_rot = U[1], U3_rot = U[2];
         U[1] = U2_rot * nyf + U3_rot * nxf;
         U[2] = U3_rot * nyf - U2_rot * nxf;
-        const float rho = U[0];
-        const float temp = 1.0f / U[0];
-        const float u1 = U[1] * temp;
-        const float u2 = U[2] * temp;
-        const float pr = 0.4f * (U[3] - (0.5f * temp) * (U[1] * U[1] + U[2] * U[2]));
+        const UT temp = UT(1) / U[0];
+        const float rho = (float)U[0];
+        const float u1 = (float)(U[1] * temp);
+        const float u2 = (float)(U[2] * temp);
+        const float pr = (float)(UT(0.4) * (U[3] - (UT(0.5) * temp) * (U[1] * U[1] + U[2] * U[2])));
         b.prim_out[i] = make_float4(rho, u1, u2, pr);
         float qn[4];
         q_from_prim_t<float>(rho, u1, u2, pr, qn);

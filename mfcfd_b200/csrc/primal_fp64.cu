@@ -81,7 +81,7 @@ __device__ __forceinline__ void ld8w(const double *p, double a[4], double b[4]) 
 // reads of a warp hit distinct banks.  Each thread reads only what it
 // copied, so no block barrier is needed.
 #ifndef STAGE_D
-#define STAGE_D 8  // slots per round, D pass
+#define STAGE_D 4  // slots per round, D pass (4: 0.099 ms per C2 launch, 8: 0.107)
 #endif
 constexpr int PAIRS_D = 4;  // q[0..1], q[2..3], (x, y), (spd, -)
 

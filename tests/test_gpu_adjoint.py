@@ -115,13 +115,16 @@ def test_adjoint_on_the_16k_grid_from_a_developed_state(gpu, obj):
     iterations are reversed.  At 32 seeded points of the first four rings
     (seed 3), dJ/dx and dJ/dy equal the forward-mode derivative along the
     same coordinate (mfcfd_tangent, an independent linearisation) to 1e-9.
-    Central differences with h = 1e-6 chord agree only to about 0.5 % of the
-    largest derivative: over 100 iterations of a developed solution the
-    perturbation switches branches of the limiter (min(1, num/den) and its
-    1e-5 threshold), so the loop is not differentiable at that scale, and the
-    differences approach the linearisation only linearly in h (measured on
-    this grid: 3.5 %, 0.46 %, 0.13 % of the largest derivative at h = 1e-5,
-    1e-6, 1e-7)."""
+    Central differences with h = 1e-6 chord agree with it to about 1e-5 of
+    the largest derivative at half the points, and to about 1 % at the worst:
+    over 100 iterations of a developed solution the perturbation switches
+    branches of the limiter (min(1, num/den) and its 1e-5 threshold) at
+    points whose switch lies within h, so the loop is only piecewise smooth
+    at that scale and the differences approach the linearisation linearly in
+    h (measured on this grid, worst component for cd: 3.5 %, 0.46 %, 0.13 %
+    of the largest derivative at h = 1e-5, 1e-6, 1e-7; for cl 1.2 % at
+    1e-6).  The test bounds the median and the worst difference at h = 1e-6
+    and checks that the four worst shrink at h = 1e-7."""
     h = 1e-6
     g = naca_ogrid(160, 100, seed=3000, first_spacing="match", spacing="arc")
     flow = dict(cfl=0.2, vl_const=5.0, mach=0.63, aoa=2.0)
@@ -153,14 +156,19 @@ def test_adjoint_on_the_16k_grid_from_a_developed_state(gpu, obj):
         return float(cd.sum() if obj == "cd" else cl.sum())
 
     assert abs(J - J_of(g)) < 1e-12
-    fd = []
-    for p in pts:
-        for arr in ("x", "y"):
-            gp, gm = copy.deepcopy(g), copy.deepcopy(g)
-            getattr(gp, arr)[p] += h
-            getattr(gm, arr)[p] -= h
-            fd.append((J_of(gp) - J_of(gm)) / (2 * h))
-    assert np.max(np.abs(np.array(fd) - adj)) <= 1e-2 * scale
+    def central(p, arr, step):
+        gp, gm = copy.deepcopy(g), copy.deepcopy(g)
+        getattr(gp, arr)[p] += step
+        getattr(gm, arr)[p] -= step
+        return (J_of(gp) - J_of(gm)) / (2 * step)
+
+    comps = [(p, arr) for p in pts for arr in ("x", "y")]
+    err = np.abs(np.array([central(p, arr, h) for p, arr in comps]) - adj)
+    assert np.median(err) <= 1e-3 * scale, np.median(err) / scale
+    assert np.max(err) <= 3e-2 * scale, np.max(err) / scale
+    worst = np.argsort(err)[-4:]
+    err7 = np.abs(np.array([central(*comps[i], h / 10) for i in worst]) - adj[worst])
+    assert err7.sum() <= 0.5 * err[worst].sum(), (err7, err[worst])
 
 
 def _unit(n, p):

@@ -80,5 +80,5 @@ def test_fp32_mixed_on_a_developed_solution(gpu):
     assert abs(clb[0] - cla[0]) <= 1e-5 and abs(cdb[0] - cda[0]) <= 1e-5
     scale = np.maximum(np.abs(pa), 1e-3 * np.max(np.abs(pa), axis=0))
     assert float(np.sqrt(np.mean(((pb - pa) / scale) ** 2))) < 1e-4
-    # a developed solution: the residual has dropped
-    assert ra[-1] < -1.0
+    # a developed solution: the residual has dropped by 0.7 decades
+    assert ra[-1] < -0.7
