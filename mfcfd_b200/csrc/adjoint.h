@@ -8,7 +8,10 @@
 namespace lskum {
 
 constexpr int ADJ_CW = 22;  // contribution record per (point, slot)
-enum { ADJ_GATHER_FLUX = 0, ADJ_GATHER_INNER = 1, ADJ_GATHER_GRAD = 2 };
+// flux pass: per (point, slot) the neighbour side's record (adjoint of its
+// reconstructed u1, u2, rho, p; its rho; delx/dely adjoint; padding)
+constexpr int NBREC = 8;
+enum { ADJ_GATHER_INNER = 1, ADJ_GATHER_GRAD = 2 };
 
 struct AdjConsts {
     double q_inf[4];
@@ -37,10 +40,18 @@ void launch_update_b(const Geom &g, const Consts &c, const AdjConsts &a, const R
                      cudaStream_t s);
 // kst: the stage's kinetic-state tape of the forward re-run ([n][kp][KS_TAPE],
 // written by the flux pass with StageBufs::kstape), or nullptr to recompute
+// The flux pass reverses in two kernels: k_flux_b per point (its fluxes,
+// kinetic states and own reconstruction; writes nbrec [n][kp][NBREC]) and
+// k_flux_b_nbr per neighbour over the transposed stencil (the neighbour's
+// reconstruction; writes back [n][kp] (delx, dely) adjoint parts that
+// belong to the point as well), then k_back_sum adds those to the point.
+// nbrec and back may share the contribution buffer (n*kp*(NBREC+2) <=
+// n*kp*ADJ_CW doubles).
 void launch_flux_b(const Geom &g, const Consts &c, const R4 *q_in, const double *dq,
                    const double *qm, const double *delta, const double *frb, double *qb,
                    double *dqb, double *qmb, double *xb, double *yb, double *nxb, double *nyb,
-                   double *deltab, double *contrib, const double *kst, cudaStream_t s);
+                   double *deltab, double *nbrec, double *back, const int *tptr,
+                   const int *tlist, const double *kst, cudaStream_t s);
 void launch_inner_b(const Geom &g, const R4 *q, const double *dq_in, const double *dqb_out,
                     double *dqb_in, double *qb, double *xb, double *yb, double *contrib,
                     cudaStream_t s);

@@ -52,7 +52,8 @@ struct AdjointState {
     double *tks = nullptr;
     double *hist = nullptr;
     int hist_cap = 0;
-    std::vector<R4 *> snaps;  // snapshot pool (device buffers of n rows)
+    std::vector<R4 *> snaps;  // snapshot rows (n points each) in one device block
+    R4 *snap_pool = nullptr;
     R4 *snap0 = nullptr;      // the initial state
     R4 *fin = nullptr;        // the final state
     // run bookkeeping
@@ -289,9 +290,8 @@ int reverse_taped(mfcfd_t *h, AdjointState *a) {
         CK(cudaMemsetAsync(a->dqb[m & 1], 0, sizeof(double) * 8 * n, s));
         launch_flux_b(h->geom, h->consts, a->tq[rk - 1], dq_at(a, rk, m), qm_at(a, rk), a->tdelta,
                       a->frb, a->qb, a->dqb[m & 1], a->qmb, a->xb, a->yb, a->nxb, a->nyb,
-                      a->deltab, a->contrib, ks_at(a, rk), s);
-        launch_gather(n, a->kp, a->d_tptr, a->d_tlist, a->contrib, ADJ_GATHER_FLUX, a->qb,
-                      a->dqb[m & 1], a->qmb, a->xb, a->yb, s);
+                      a->deltab, a->contrib, a->contrib + (size_t)n * a->kp * NBREC, a->d_tptr,
+                      a->d_tlist, ks_at(a, rk), s);
         for (int t = m; t >= 1; --t) {
             launch_inner_b(h->geom, a->tq[rk - 1], dq_at(a, rk, t - 1), a->dqb[t & 1],
                            a->dqb[(t - 1) & 1], a->qb, a->xb, a->yb, a->contrib, s);
@@ -303,7 +303,7 @@ int reverse_taped(mfcfd_t *h, AdjointState *a) {
         launch_gather(n, a->kp, a->d_tptr, a->d_tlist, a->contrib, ADJ_GATHER_GRAD, a->qb,
                       nullptr, a->pbA, a->xb, a->yb, s);
         launch_qvar_b(n, a->tprim[rk - 1], a->qb, pb_in, s);
-        h->launches += 6 + 2LL * m;
+        h->launches += 7 + 2LL * m;
         out ^= 1;
     }
     CK(cudaMemcpyAsync(a->pb[0], a->pbA, sizeof(double) * 4 * n, cudaMemcpyDeviceToDevice, s));
@@ -399,7 +399,8 @@ void lskum_host::free_adjoint(mfcfd_t *h) {
     }
     for (int s = 0; s < 4; ++s)
         if (a->tfr[s]) cudaFree(a->tfr[s]);
-    for (R4 *p : a->snaps) cudaFree(p);
+    if (a->snap_pool) cudaFree(a->snap_pool);
+    a->snaps.clear();
     delete a;
     h->adj = nullptr;
 }
@@ -433,10 +434,12 @@ int adjoint_prepare(mfcfd_t *h, int objective, int n_iters, size_t ckpt_bytes, i
     }
     const long long want = ckpt_bytes > row ? (long long)(ckpt_bytes / row) - 1 : 0;
     *nsnap = (int)std::min<long long>(want, n_iters - 1);
-    while ((int)a->snaps.size() < *nsnap + 1) {  // + one scratch row
-        R4 *p = nullptr;
-        CK(dmalloc(&p, (size_t)h->n));
-        a->snaps.push_back(p);
+    if ((int)a->snaps.size() < *nsnap + 1) {  // + one scratch row; one allocation
+        if (a->snap_pool) cudaFree(a->snap_pool);
+        a->snap_pool = nullptr;
+        a->snaps.clear();
+        CK(dmalloc(&a->snap_pool, (size_t)h->n * (*nsnap + 1)));
+        for (int j = 0; j <= *nsnap; ++j) a->snaps.push_back(a->snap_pool + (size_t)j * h->n);
     }
     return MFCFD_OK;
 }

@@ -9,10 +9,14 @@
 // (the stage-by-stage order of the reference's FPI_SOLVER_B,
 // src_mpi_adjoint/sensitivity_files/fpi_solver_b.F90:28-156).
 //
-// A point's adjoint flows to its neighbours.  Instead of atomics, each
-// kernel writes its contribution for neighbour slot r of point i into
-// contrib[(i*kp + r)*CW + field] and k_gather adds them per neighbour in the
-// fixed (i, r) order of the transposed stencil: results are deterministic.
+// A point's adjoint flows to its neighbours, without atomics.  The q-
+// derivative reverses write their contribution for neighbour slot r of
+// point i into contrib[(i*kp + r)*CW + field] and k_gather adds them per
+// neighbour in the fixed (i, r) order of the transposed stencil.  The flux
+// reverse, whose neighbour side is most of the work, pulls instead:
+// k_flux_b leaves a short record per slot and k_flux_b_nbr, one thread per
+// neighbour, reverses the neighbour's reconstruction of each slot naming it
+// in that same order.  Results are deterministic either way.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -167,7 +171,7 @@ k_update_b(Geom g, Consts c, AdjConsts a, const R4 *__restrict__ prim_in,
 
 // cal_flux_residual_b: same lane layout as the forward flux pass.
 #ifndef FLUXB_MIN_BLOCKS
-#define FLUXB_MIN_BLOCKS 4
+#define FLUXB_MIN_BLOCKS 3  // 168 registers; 4 blocks (128) spill (C3: 6.39 against 6.68 ms per reversed iteration)
 #endif
 __global__ void __launch_bounds__(BLK, FLUXB_MIN_BLOCKS)
 k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict__ dq,
@@ -175,7 +179,7 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
          const double *__restrict__ frb, double *__restrict__ qb, double *__restrict__ dqb,
          double *__restrict__ qmb, double *__restrict__ xb, double *__restrict__ yb,
          double *__restrict__ nxb, double *__restrict__ nyb, double *__restrict__ deltab,
-         double *__restrict__ contrib, const double *__restrict__ kst) {
+         double *__restrict__ nbrec, const double *__restrict__ kst) {
     extern __shared__ double sm[];
     __shared__ double lb[GROUPS][4][11];  // fx_b[4] fy_b[4] sdx2_b sdy2_b sdxy_b per list
     const int grp = threadIdx.x / LPP, lane = threadIdx.x % LPP;
@@ -199,20 +203,10 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
     const double s2q = kind == KIND_WALL ? -1.0 : 1.0;
     // phase A: forward per slot
     if (valid) {
-        const R4 qv = ld4(q_in + i);
-        const double qi[4] = {qv.a, qv.b, qv.c, qv.d};
-        double dxi[4], dyi[4], qmaxi[4], qmini[4];
-        ld8a(dq + 8 * (size_t)i, dxi, dyi);
-        ld8a(qm + 8 * (size_t)i, qmaxi, qmini);
         for (int r = lane; r < nb; r += LPP) {
             const int k = g.conn[r * g.n + i];
             const double2 pk = g.xy[k];
             const double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
-            const R4 kv = ld4(q_in + k);
-            const double qk[4] = {kv.a, kv.b, kv.c, kv.d};
-            double dxk[4], dyk[4], qmaxk[4], qmink[4];
-            ld8a(dq + 8 * (size_t)k, dxk, dyk);
-            ld8a(qm + 8 * (size_t)k, qmaxk, qmink);
             double e_[8];
             KState si, sk;
             if (kst) {
@@ -231,6 +225,13 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
                 e_[0] = v[9]; e_[1] = v[10]; e_[2] = si.rho; e_[3] = si.rho * si.pbr;
                 e_[4] = v[20]; e_[5] = v[21]; e_[6] = sk.rho; e_[7] = sk.rho * sk.pbr;
             } else {
+                const R4 qv = ld4(q_in + i), kv = ld4(q_in + k);
+                const double qi[4] = {qv.a, qv.b, qv.c, qv.d}, qk[4] = {kv.a, kv.b, kv.c, kv.d};
+                double dxi[4], dyi[4], qmaxi[4], qmini[4], dxk[4], dyk[4], qmaxk[4], qmink[4];
+                ld8a(dq + 8 * (size_t)i, dxi, dyi);
+                ld8a(qm + 8 * (size_t)i, qmaxi, qmini);
+                ld8a(dq + 8 * (size_t)k, dxk, dyk);
+                ld8a(qm + 8 * (size_t)k, qmaxk, qmink);
                 reconstruct(qi, dxi, dyi, qmaxi, qmini, g.eps2[i], delx, dely, c.gm1, e_[0],
                             e_[1], e_[2], e_[3]);
                 reconstruct(qk, dxk, dyk, qmaxk, qmink, g.eps2[k], delx, dely, c.gm1, e_[4],
@@ -366,9 +367,9 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
         deltab[i] += db;
     }
     __syncwarp();
-    // phase C: per slot reverse (the neighbour's side first, its record
-    // written before the point's own inputs are loaded, so the two sides'
-    // working sets are not live together)
+    // phase C: per slot reverse of the fluxes, kinetic states and the
+    // point's own reconstruction; the neighbour's reconstruction is left to
+    // k_flux_b_nbr
     if (valid) {
         for (int r = lane; r < nb; r += LPP) {
             const int k = g.conn[r * g.n + i];
@@ -420,36 +421,12 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
             double nxbv = 0.0, nybv = 0.0;
             double piu1b = 0.0, piu2b = 0.0, pirb = 0.0, pipb = 0.0;
             double pku1b = 0.0, pku2b = 0.0, pkrb = 0.0, pkpb = 0.0;
-            kstate_b(pr_[0], pr_[1], pr_[2], pr_[3], nx, ny, c.pi, sib, piu1b, piu2b, pirb, pipb,
-                     nxbv, nybv);
-            kstate_b(pr_[4], pr_[5], pr_[6], pr_[7], nx, ny, c.pi, skb, pku1b, pku2b, pkrb, pkpb,
-                     nxbv, nybv);
+            kstate_b_s(si, pr_[0], pr_[1], nx, ny, sib, piu1b, piu2b, pirb, pipb, nxbv, nybv);
+            kstate_b_s(sk, pr_[4], pr_[5], nx, ny, skb, pku1b, pku2b, pkrb, pkpb, nxbv, nybv);
             double delxb = delsb * ny + delnb * nx;
             double delyb = -delsb * nx + delnb * ny;
             nxbv += -delsb * dely + delnb * delx;
             nybv += delsb * delx + delnb * dely;
-            // neighbour reconstruction
-            const R4 kv = ld4(q_in + k);
-            const double qk[4] = {kv.a, kv.b, kv.c, kv.d};
-            double dxk[4], dyk[4], qmaxk[4], qmink[4];
-            ld8a(dq + 8 * (size_t)k, dxk, dyk);
-            ld8a(qm + 8 * (size_t)k, qmaxk, qmink);
-            double qkb[4] = {0, 0, 0, 0}, dxkb[4] = {0, 0, 0, 0}, dykb[4] = {0, 0, 0, 0},
-                   qmaxkb[4] = {0, 0, 0, 0}, qminkb[4] = {0, 0, 0, 0};
-            reconstruct_b(qk, dxk, dyk, qmaxk, qmink, g.eps2[k], delx, dely, c.gm1, pr_[6], pku1b,
-                          pku2b, pkrb, pkpb, qkb, dxkb, dykb, qmaxkb, qminkb, delxb, delyb);
-            double *cb = contrib + ((size_t)i * g.kp + r) * ADJ_CW;
-            {
-                double v[20];
-                for (int m = 0; m < 4; ++m) {
-                    v[m] = qkb[m];
-                    v[4 + m] = dxkb[m];
-                    v[8 + m] = dykb[m];
-                    v[12 + m] = qmaxkb[m];
-                    v[16 + m] = qminkb[m];
-                }
-                st_pairs(cb, v, 20);
-            }
             const R4 qv = ld4(q_in + i);
             const double qi[4] = {qv.a, qv.b, qv.c, qv.d};
             double dxi[4], dyi[4], qmaxi[4], qmini[4];
@@ -459,7 +436,13 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
                    qmaxib[4] = {0, 0, 0, 0}, qminib[4] = {0, 0, 0, 0};
             reconstruct_b(qi, dxi, dyi, qmaxi, qmini, g.eps2[i], delx, dely, c.gm1, pr_[2], piu1b,
                           piu2b, pirb, pipb, qib, dxib, dyib, qmaxib, qminib, delxb, delyb);
-            reinterpret_cast<double2 *>(cb + 20)[0] = make_double2(delxb, delyb);
+            // the neighbour's side: its reconstruction is reversed by
+            // k_flux_b_nbr from this record (the adjoint of its reconstructed
+            // primitive state, its density, and delx/dely's adjoint so far)
+            {
+                const double v[NBREC] = {pku1b, pku2b, pkrb, pkpb, pr_[6], delxb, delyb, 0.0};
+                st_pairs(nbrec + ((size_t)i * g.kp + r) * NBREC, v, NBREC);
+            }
             // self contribution of this slot, summed in slot order below
             for (int m = 0; m < 4; ++m) {
                 e[m] = qib[m];
@@ -487,6 +470,85 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
         else if (f == 22) nxb[i] += s;
         else nyb[i] += s;
     }
+}
+
+// The neighbour side of cal_flux_residual_b, one thread per neighbour k:
+// over the slots (i, r) that name k (the transposed stencil, in (i, r)
+// order) it reverses k's reconstruction of that slot from k_flux_b's record
+// and adds the results to k's own adjoints in registers: no scatter and no
+// gather of contribution records.  The part of delx/dely's adjoint that this
+// reconstruction adds belongs to point i as well (delx = x_k - x_i): it is
+// left in back[(i, r)] for k_back_sum.
+constexpr int NBR_BLK = 128;
+#ifndef NBR_MIN_BLOCKS
+#define NBR_MIN_BLOCKS 3  // 168 registers (4: 128 with spills, 1 % slower)
+#endif
+__global__ void __launch_bounds__(NBR_BLK, NBR_MIN_BLOCKS)
+k_flux_b_nbr(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict__ dq,
+             const double *__restrict__ qm, const int *__restrict__ tptr,
+             const int *__restrict__ tlist, const double *__restrict__ nbrec,
+             double *__restrict__ qb, double *__restrict__ dqb, double *__restrict__ qmb,
+             double *__restrict__ xb, double *__restrict__ yb, double2 *__restrict__ back) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= g.n) return;
+    const R4 kv = ld4(q_in + k);
+    const double qk[4] = {kv.a, kv.b, kv.c, kv.d};
+    double dxk[4], dyk[4], qmaxk[4], qmink[4];
+    ld8a(dq + 8 * (size_t)k, dxk, dyk);
+    ld8a(qm + 8 * (size_t)k, qmaxk, qmink);
+    const double eps2 = g.eps2[k];
+    const double2 pk = g.xy[k];
+    double qkb[4] = {0, 0, 0, 0}, dxkb[4] = {0, 0, 0, 0}, dykb[4] = {0, 0, 0, 0},
+           qmaxkb[4] = {0, 0, 0, 0}, qminkb[4] = {0, 0, 0, 0};
+    double xkb = 0.0, ykb = 0.0;
+    const int e1 = tptr[k + 1];
+    for (int e = tptr[k]; e < e1; ++e) {
+        const int slot = tlist[e];
+        const int i = slot / g.kp;
+        const double2 pi_ = g.xy[i];
+        const double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
+        // the record: (u1b, u2b), (rhob, prb), (rho, delxb), (delyb, 0)
+        const double2 *rv = reinterpret_cast<const double2 *>(nbrec + (size_t)slot * NBREC);
+        const double2 ub = __ldg(rv), pb = __ldg(rv + 1), rd = __ldg(rv + 2), dy = __ldg(rv + 3);
+        double dxr = 0.0, dyr = 0.0;
+        reconstruct_b(qk, dxk, dyk, qmaxk, qmink, eps2, delx, dely, c.gm1, rd.x, ub.x, ub.y, pb.x,
+                      pb.y, qkb, dxkb, dykb, qmaxkb, qminkb, dxr, dyr);
+        xkb += rd.y + dxr;
+        ykb += dy.x + dyr;
+        back[slot] = make_double2(dxr, dyr);
+    }
+    add_pairs(qb + 4 * (size_t)k, qkb, 4);
+    double v8[8];
+    for (int m = 0; m < 4; ++m) {
+        v8[m] = dxkb[m];
+        v8[4 + m] = dykb[m];
+    }
+    add_pairs(dqb + 8 * (size_t)k, v8, 8);
+    for (int m = 0; m < 4; ++m) {
+        v8[m] = qmaxkb[m];
+        v8[4 + m] = qminkb[m];
+    }
+    add_pairs(qmb + 8 * (size_t)k, v8, 8);
+    xb[k] += xkb;
+    yb[k] += ykb;
+}
+
+// x_i, y_i receive minus the delx/dely adjoint parts of their slots'
+// neighbour reconstructions, in slot order.
+__global__ void __launch_bounds__(256)
+k_back_sum(Geom g, const double2 *__restrict__ back, double *__restrict__ xb,
+           double *__restrict__ yb) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.n) return;
+    const int nb = g.nbhs[i];
+    double sx = 0.0, sy = 0.0;
+    for (int r = 0; r < nb; ++r) {
+        const double2 v = __ldg(back + (size_t)i * g.kp + r);
+        sx = sx + v.x;
+        sy = sy + v.y;
+    }
+    xb[i] -= sx;
+    yb[i] -= sy;
 }
 
 // eval_q_inner_loop_b: one inner iteration; dqb_out is the adjoint of its
@@ -698,14 +760,14 @@ k_grad_b(Geom g, Consts c, const R4 *__restrict__ q, const R4 *__restrict__ prim
 }
 
 // Adds the neighbour contributions per point in the fixed transposed order.
-// MODE fixes the record width (22 flux, 14 inner, 10 grad fields) so the
+// MODE fixes the record width (14 inner, 10 grad fields) so the
 // accumulators stay in registers; records are read as 16-byte pairs.
 template <int MODE>
 __global__ void __launch_bounds__(256)
 k_gather(int n, const int *__restrict__ tptr, const int *__restrict__ tlist,
          const double *__restrict__ contrib, double *__restrict__ a4, double *__restrict__ a8,
          double *__restrict__ b8, double *__restrict__ xb, double *__restrict__ yb) {
-    constexpr int NF = MODE == ADJ_GATHER_FLUX ? 22 : (MODE == ADJ_GATHER_INNER ? 14 : 10);
+    constexpr int NF = MODE == ADJ_GATHER_INNER ? 14 : 10;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     double acc[NF];
@@ -722,10 +784,7 @@ k_gather(int n, const int *__restrict__ tptr, const int *__restrict__ tlist,
         }
     }
     add_pairs(a4 + 4 * (size_t)k, acc, 4);
-    if constexpr (MODE == ADJ_GATHER_FLUX) {
-        add_pairs(a8 + 8 * (size_t)k, acc + 4, 8);
-        add_pairs(b8 + 8 * (size_t)k, acc + 12, 8);
-    } else if constexpr (MODE == ADJ_GATHER_INNER) {
+    if constexpr (MODE == ADJ_GATHER_INNER) {
         add_pairs(a8 + 8 * (size_t)k, acc + 4, 8);
     } else {
         add_pairs(b8 + 4 * (size_t)k, acc + 4, 4);
@@ -908,10 +967,15 @@ void launch_update_b(const Geom &g, const Consts &c, const AdjConsts &a, const R
 void launch_flux_b(const Geom &g, const Consts &c, const R4 *q_in, const double *dq,
                    const double *qm, const double *delta, const double *frb, double *qb,
                    double *dqb, double *qmb, double *xb, double *yb, double *nxb, double *nyb,
-                   double *deltab, double *contrib, const double *kst, cudaStream_t s) {
+                   double *deltab, double *nbrec, double *back, const int *tptr,
+                   const int *tlist, const double *kst, cudaStream_t s) {
     size_t smem = (size_t)GROUPS * g.kp * BREC * sizeof(double);
     k_flux_b<<<nblk(g.n, GROUPS), BLK, smem, s>>>(g, c, q_in, dq, qm, delta, frb, qb, dqb, qmb,
-                                                  xb, yb, nxb, nyb, deltab, contrib, kst);
+                                                  xb, yb, nxb, nyb, deltab, nbrec, kst);
+    double2 *bk = reinterpret_cast<double2 *>(back);
+    k_flux_b_nbr<<<nblk(g.n, NBR_BLK), NBR_BLK, 0, s>>>(g, c, q_in, dq, qm, tptr, tlist, nbrec,
+                                                       qb, dqb, qmb, xb, yb, bk);
+    k_back_sum<<<nblk(g.n, 256), 256, 0, s>>>(g, bk, xb, yb);
 }
 
 void launch_inner_b(const Geom &g, const R4 *q, const double *dq_in, const double *dqb_out,
@@ -932,10 +996,7 @@ void launch_gather(int n, int kp, const int *tptr, const int *tlist, const doubl
                    int mode, double *a4, double *a8, double *b8, double *xb, double *yb,
                    cudaStream_t s) {
     (void)kp;
-    if (mode == ADJ_GATHER_FLUX)
-        k_gather<ADJ_GATHER_FLUX><<<nblk(n, 256), 256, 0, s>>>(n, tptr, tlist, contrib, a4, a8, b8,
-                                                              xb, yb);
-    else if (mode == ADJ_GATHER_INNER)
+    if (mode == ADJ_GATHER_INNER)
         k_gather<ADJ_GATHER_INNER><<<nblk(n, 256), 256, 0, s>>>(n, tptr, tlist, contrib, a4, a8,
                                                                b8, xb, yb);
     else

@@ -189,6 +189,39 @@ __device__ __forceinline__ void kstate_b(double u1, double u2, double rho, doubl
     nyb += utb * u1 + unb * u2;
 }
 
+// kstate_b from the forward's own kinetic state s (its rho, ut, un, p/rho,
+// B1, B2): exp(-S^2) / sqrt(pi beta) = 2 B and (2/sqrt(pi)) exp(-S^2) =
+// 4 B sqrt(beta), so the adjoint needs one square root and two divisions
+// instead of kstate_b's two exponentials, two square roots and seven
+// divisions.  (u1, u2) is the state's velocity.
+__device__ __forceinline__ void kstate_b_s(const KState &s, double u1, double u2, double nx,
+                                           double ny, const KStateB &sb_, double &u1b,
+                                           double &u2b, double &rhob, double &prb, double &nxb,
+                                           double &nyb) {
+    const double ut = s.ut, un = s.un, pbr = s.pbr;
+    const double beta = 0.5 / pbr;
+    const double ir = 1.0 / s.rho;
+    const double sb = sqrt(beta);
+    const double S1 = ut * sb, S2 = un * sb;
+    double utb = sb_.ut + 2.0 * ut * sb_.usq;
+    double unb = sb_.un + 2.0 * un * sb_.usq;
+    prb += sb_.pbr * ir;
+    rhob += sb_.rho - sb_.pbr * pbr * ir;
+    const double S1b = s.B1 * (4.0 * sb * sb_.e1 - 2.0 * S1 * sb_.B1);
+    const double S2b = s.B2 * (4.0 * sb * sb_.e2 - 2.0 * S2 * sb_.B2);
+    double betab = -(sb_.B1 * s.B1 + sb_.B2 * s.B2) * pbr;
+    utb += S1b * sb;
+    unb += S2b * sb;
+    betab += (S1b * ut + S2b * un) * sb * pbr;  // d sqrt(beta) / d beta = sqrt(beta) p/rho
+    // beta = rho / (2 pr): d/drho = beta / rho, d/dpr = -beta / pr = -2 beta^2 / rho
+    rhob += betab * beta * ir;
+    prb += -betab * 2.0 * beta * beta * ir;
+    u1b += utb * ny + unb * nx;
+    u2b += -utb * nx + unb * ny;
+    nxb += -utb * u2 + unb * u1;
+    nyb += utb * u1 + unb * u2;
+}
+
 // qtilde_to_primitive_b
 __device__ __forceinline__ void qtilde_to_primitive_b(const double qt[4], double gm1, double rho,
                                                       double u1b, double u2b, double rhob,
