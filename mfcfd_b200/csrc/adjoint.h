@@ -11,6 +11,8 @@ constexpr int ADJ_CW = 22;  // contribution record per (point, slot)
 // flux pass: per (point, slot) the neighbour side's record (adjoint of its
 // reconstructed u1, u2, rho, p; its rho; delx/dely adjoint; padding)
 constexpr int NBREC = 8;
+// q-derivative pass: per point the record its neighbours' side reads
+constexpr int GREC = 24;
 enum { ADJ_GATHER_INNER = 1, ADJ_GATHER_GRAD = 2 };
 
 struct AdjConsts {
@@ -55,11 +57,15 @@ void launch_flux_b(const Geom &g, const Consts &c, const R4 *q_in, const double 
 void launch_inner_b(const Geom &g, const R4 *q, const double *dq_in, const double *dqb_out,
                     double *dqb_in, double *qb, double *xb, double *yb, double *contrib,
                     cudaStream_t s);
-// spdA: |u| + 3 sqrt(p/rho) of primA as the forward pass used it (taped)
+// spdA: |u| + 3 sqrt(p/rho) of primA as the forward pass used it (taped).
+// Two kernels: k_grad_b per point (its own side; writes grec [n][GREC], which
+// may share the contribution buffer) and k_grad_b_nbr per neighbour over the
+// transposed stencil (adds to qb, pb = primA's adjoint, xb, yb).
 void launch_grad_b(const Geom &g, const Consts &c, const R4 *q, const R4 *primA,
                    const double *spdA, const double *dqb, const double *qmb,
-                   const double *deltab, bool with_delta, double *qb, double *xb, double *yb,
-                   double *contrib, cudaStream_t s);
+                   const double *deltab, bool with_delta, double *qb, double *pb, double *xb,
+                   double *yb, double *grec, const int *tptr, const int *tlist,
+                   cudaStream_t s);
 void launch_gather(int n, int kp, const int *tptr, const int *tlist, const double *contrib,
                    int mode, double *a4, double *a8, double *b8, double *xb, double *yb,
                    cudaStream_t s);

@@ -299,9 +299,8 @@ int reverse_taped(mfcfd_t *h, AdjointState *a) {
                           a->dqb[(t - 1) & 1], nullptr, a->xb, a->yb, s);
         }
         launch_grad_b(h->geom, h->consts, a->tq[rk - 1], a->tprim[0], a->tspd, a->dqb[0],
-                      a->qmb, a->deltab, rk == 1, a->qb, a->xb, a->yb, a->contrib, s);
-        launch_gather(n, a->kp, a->d_tptr, a->d_tlist, a->contrib, ADJ_GATHER_GRAD, a->qb,
-                      nullptr, a->pbA, a->xb, a->yb, s);
+                      a->qmb, a->deltab, rk == 1, a->qb, a->pbA, a->xb, a->yb, a->contrib,
+                      a->d_tptr, a->d_tlist, s);
         launch_qvar_b(n, a->tprim[rk - 1], a->qb, pb_in, s);
         h->launches += 7 + 2LL * m;
         out ^= 1;

@@ -644,12 +644,16 @@ k_inner_b(Geom g, const R4 *__restrict__ q, const double *__restrict__ dq_in,
 }
 
 // eval_q_derivatives_b (+ func_delta_b on the first stage)
+// eval_q_derivatives_b + func_delta_b, the point's own side.  The
+// neighbours' side reads the point's record grec[i] (GREC doubles: sxb[4],
+// syb[4], s0b, s1b, s2b, deltab, qmaxb[4], qminb[4], the packed arg-max /
+// arg-min slots, the time-step minimum's slot) in k_grad_b_nbr.
 __global__ void __launch_bounds__(BLK, ADJ_MIN_BLOCKS)
 k_grad_b(Geom g, Consts c, const R4 *__restrict__ q, const R4 *__restrict__ primA,
          const double *__restrict__ spdA, const double *__restrict__ dqb,
          const double *__restrict__ qmb,
          const double *__restrict__ deltab, int with_delta, double *__restrict__ qb,
-         double *__restrict__ xb, double *__restrict__ yb, double *__restrict__ contrib) {
+         double *__restrict__ xb, double *__restrict__ yb, double *__restrict__ grec) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.n) return;
     const double2 pi_ = g.xy[i];
@@ -704,6 +708,32 @@ k_grad_b(Geom g, Consts c, const R4 *__restrict__ q, const R4 *__restrict__ prim
     s1b += detb * s0;
     s2b += -2.0 * detb * s2;
     const double dlb = with_delta ? deltab[i] : 0.0;
+    const int amd_used = (with_delta && dlb != 0.0) ? amd : -1;
+    {
+        // the record: slots packed 5 bits each (+1, so -1 -> 0), arg-max in
+        // bits 0-19, arg-min in bits 20-39
+        long long code = 0;
+        for (int m = 0; m < 4; ++m) {
+            code |= (long long)(amax[m] + 1) << (5 * m);
+            code |= (long long)(amin[m] + 1) << (20 + 5 * m);
+        }
+        double v[GREC];
+        for (int m = 0; m < 4; ++m) {
+            v[m] = sxb[m];
+            v[4 + m] = syb[m];
+            v[12 + m] = qmxb[m];
+            v[16 + m] = qmnb[m];
+        }
+        v[8] = s0b;
+        v[9] = s1b;
+        v[10] = s2b;
+        v[11] = dlb;
+        v[20] = __longlong_as_double(code);
+        v[21] = (double)amd_used;
+        v[22] = 0.0;
+        v[23] = 0.0;
+        st_pairs(grec + (size_t)i * GREC, v, GREC);
+    }
     double qib[4] = {0, 0, 0, 0}, xib = 0.0, yib = 0.0;
     for (int m = 0; m < 4; ++m) {
         if (amax[m] < 0) qib[m] += qmxb[m];
@@ -717,20 +747,77 @@ k_grad_b(Geom g, Consts c, const R4 *__restrict__ q, const R4 *__restrict__ prim
         const double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
         double delxb = 2.0 * delx * s0b + dely * s2b;
         double delyb = 2.0 * dely * s1b + delx * s2b;
-        double *cb = contrib + ((size_t)i * g.kp + r) * ADJ_CW;
-        double v[10];  // the record, stored as 16-byte pairs at the end
         for (int m = 0; m < 4; ++m) {
             const double t = sxb[m] * delx + syb[m] * dely;
-            double qkb = t;
             qib[m] -= t;
-            if (amax[m] == r) qkb += qmxb[m];
-            if (amin[m] == r) qkb += qmnb[m];
             delxb += sxb[m] * (qk[m] - qi[m]);
             delyb += syb[m] * (qk[m] - qi[m]);
-            v[m] = qkb;
-            v[4 + m] = 0.0;
         }
-        if (with_delta && r == amd && dlb != 0.0) {
+        if (r == amd_used) {
+            const R4 P = ld4(primA + k);
+            const double modu = sqrt(P.b * P.b + P.c * P.c);
+            const double cs = sqrt(P.d / P.a);
+            const double spd = modu + 3.0 * cs;
+            const double dist = sqrt(delx * delx + dely * dely);
+            const double distb = dlb * c.cfl / spd;
+            delxb += distb * delx / dist;
+            delyb += distb * dely / dist;
+        }
+        xib -= delxb;
+        yib -= delyb;
+    }
+    for (int m = 0; m < 4; ++m) qb[4 * (size_t)i + m] += qib[m];
+    xb[i] += xib;
+    yb[i] += yib;
+}
+
+// The neighbours' side of eval_q_derivatives_b + func_delta_b, one thread
+// per neighbour k over the slots (i, r) naming it, in the transposed
+// stencil's (i, r) order: q_k's adjoint from the point's least-squares sums
+// and max/min, the time-step minimum's adjoint through k's taped state, and
+// delx/dely's (the point's side takes the same value with the other sign).
+__global__ void __launch_bounds__(BLK)
+k_grad_b_nbr(Geom g, Consts c, const R4 *__restrict__ q, const R4 *__restrict__ primA,
+             const int *__restrict__ tptr, const int *__restrict__ tlist,
+             const double *__restrict__ grec, double *__restrict__ qb, double *__restrict__ pb,
+             double *__restrict__ xb, double *__restrict__ yb) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= g.n) return;
+    const R4 kv = ld4(q + k);
+    const double qk[4] = {kv.a, kv.b, kv.c, kv.d};
+    const double2 pk = g.xy[k];
+    double qkb[4] = {0, 0, 0, 0}, pkb[4] = {0, 0, 0, 0}, xkb = 0.0, ykb = 0.0;
+    const int e1 = tptr[k + 1];
+    for (int e = tptr[k]; e < e1; ++e) {
+        const int slot = tlist[e];
+        const int i = slot / g.kp, r = slot - i * g.kp;
+        const double2 *rv = reinterpret_cast<const double2 *>(grec + (size_t)i * GREC);
+        double v[GREC];
+#pragma unroll
+        for (int h = 0; h < 6; ++h) {  // sxb, syb, s0b..s2b, deltab
+            const double2 t2 = __ldg(rv + h);
+            v[2 * h] = t2.x;
+            v[2 * h + 1] = t2.y;
+        }
+        const double2 cd = __ldg(rv + 10);
+        const long long code = __double_as_longlong(cd.x);
+        const int amd = (int)cd.y;
+        const R4 qv = ld4(q + i);
+        const double qi[4] = {qv.a, qv.b, qv.c, qv.d};
+        const double2 pi_ = g.xy[i];
+        const double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
+        double delxb = 2.0 * delx * v[8] + dely * v[10];
+        double delyb = 2.0 * dely * v[9] + delx * v[10];
+        for (int m = 0; m < 4; ++m) {
+            qkb[m] += v[m] * delx + v[4 + m] * dely;
+            if ((int)((code >> (5 * m)) & 31) == r + 1) qkb[m] += grec[(size_t)i * GREC + 12 + m];
+            if ((int)((code >> (20 + 5 * m)) & 31) == r + 1)
+                qkb[m] += grec[(size_t)i * GREC + 16 + m];
+            delxb += v[m] * (qk[m] - qi[m]);
+            delyb += v[4 + m] * (qk[m] - qi[m]);
+        }
+        if (r == amd) {
+            const double dlb = v[11];
             const R4 P = ld4(primA + k);
             const double modu = sqrt(P.b * P.b + P.c * P.c);
             const double cs = sqrt(P.d / P.a);
@@ -741,22 +828,20 @@ k_grad_b(Geom g, Consts c, const R4 *__restrict__ q, const R4 *__restrict__ prim
             delxb += distb * delx / dist;
             delyb += distb * dely / dist;
             if (modu > 0.0) {
-                v[5] = spdb * P.b / modu;
-                v[6] = spdb * P.c / modu;
+                pkb[1] += spdb * P.b / modu;
+                pkb[2] += spdb * P.c / modu;
             }
             const double csb = 3.0 * spdb;
-            v[7] = csb * 0.5 / (cs * P.a);
-            v[4] = -csb * 0.5 * P.d / (cs * P.a * P.a);
+            pkb[3] += csb * 0.5 / (cs * P.a);
+            pkb[0] += -csb * 0.5 * P.d / (cs * P.a * P.a);
         }
-        v[8] = delxb;
-        v[9] = delyb;
-        st_pairs(cb, v, 10);
-        xib -= delxb;
-        yib -= delyb;
+        xkb += delxb;
+        ykb += delyb;
     }
-    for (int m = 0; m < 4; ++m) qb[4 * (size_t)i + m] += qib[m];
-    xb[i] += xib;
-    yb[i] += yib;
+    add_pairs(qb + 4 * (size_t)k, qkb, 4);
+    add_pairs(pb + 4 * (size_t)k, pkb, 4);
+    xb[k] += xkb;
+    yb[k] += ykb;
 }
 
 // Adds the neighbour contributions per point in the fixed transposed order.
@@ -986,10 +1071,13 @@ void launch_inner_b(const Geom &g, const R4 *q, const double *dq_in, const doubl
 
 void launch_grad_b(const Geom &g, const Consts &c, const R4 *q, const R4 *primA,
                    const double *spdA, const double *dqb, const double *qmb,
-                   const double *deltab, bool with_delta, double *qb, double *xb, double *yb,
-                   double *contrib, cudaStream_t s) {
+                   const double *deltab, bool with_delta, double *qb, double *pb, double *xb,
+                   double *yb, double *grec, const int *tptr, const int *tlist,
+                   cudaStream_t s) {
     k_grad_b<<<nblk(g.n, BLK), BLK, 0, s>>>(g, c, q, primA, spdA, dqb, qmb, deltab,
-                                           with_delta ? 1 : 0, qb, xb, yb, contrib);
+                                           with_delta ? 1 : 0, qb, xb, yb, grec);
+    k_grad_b_nbr<<<nblk(g.n, BLK), BLK, 0, s>>>(g, c, q, primA, tptr, tlist, grec, qb, pb, xb,
+                                               yb);
 }
 
 void launch_gather(int n, int kp, const int *tptr, const int *tlist, const double *contrib,

@@ -222,18 +222,21 @@ __device__ __forceinline__ void kstate_b_s(const KState &s, double u1, double u2
     nyb += utb * u1 + unb * u2;
 }
 
-// qtilde_to_primitive_b
+// qtilde_to_primitive_b (one division: 1/beta; 1/gm1 is loop-invariant
+// where this is inlined)
 __device__ __forceinline__ void qtilde_to_primitive_b(const double qt[4], double gm1, double rho,
                                                       double u1b, double u2b, double rhob,
                                                       double prb, double qtb[4]) {
     const double beta = -qt[3] * 0.5;
-    const double temp = 0.5 / beta;
+    const double ib = 1.0 / beta;
+    const double igm1 = 1.0 / gm1;
+    const double temp = 0.5 * ib;
     const double u1 = qt[1] * temp, u2 = qt[2] * temp;
     rhob += prb * temp;
     double tempb = prb * rho;
     const double temp2b = rhob * rho;
     const double temp1b = temp2b;
-    double betab = -temp2b / (gm1 * beta);
+    double betab = -temp2b * ib * igm1;
     qtb[0] += temp1b;
     betab += temp1b * (u1 * u1 + u2 * u2);
     u1b += temp1b * 2.0 * beta * u1;
@@ -241,46 +244,14 @@ __device__ __forceinline__ void qtilde_to_primitive_b(const double qt[4], double
     qtb[1] += u1b * temp;
     qtb[2] += u2b * temp;
     tempb += u1b * qt[1] + u2b * qt[2];
-    betab += -tempb * temp / beta;
+    betab += -tempb * temp * ib;
     qtb[3] += -0.5 * betab;
 }
 
-// venkat_limiter_b for one component: phi_b -> qtilde_b, q_b, qmax_b/qmin_b
-__device__ __forceinline__ void venkat_phi_b(double qtilde, double q, double qmax, double qmin,
-                                             double eps2, double phib, double &qtildeb,
-                                             double &qb, double &qmaxb, double &qminb) {
-    const double dn = qtilde - q;
-    if (fabs(dn) <= MFCFD_VENKAT_THR) return;
-    const bool up = dn > 0.0;
-    const double dp = up ? qmax - q : qmin - q;
-    const double num1 = (dp * dp) + eps2;
-    const double num = num1 * dn + 2.0 * dn * dn * dp;
-    const double den1 = dp * dp + 2.0 * dn * dn;
-    const double den2 = den1 + dn * dp + eps2;
-    const double den = den2 * dn;
-    const double temp = num / den;
-    if (!(temp < 1.0)) return;
-    const double numb = phib / den;
-    const double denb = -phib * temp / den;
-    const double den2b = denb * dn;
-    double dnb = denb * den2;
-    const double den1b = den2b;
-    dnb += den2b * dp;
-    double dpb = den2b * dn;
-    dpb += den1b * 2.0 * dp;
-    dnb += den1b * 4.0 * dn;
-    const double num1b = numb * dn;
-    dnb += numb * (num1 + 4.0 * dn * dp);
-    dpb += numb * 2.0 * dn * dn;
-    dpb += num1b * 2.0 * dp;
-    if (up) qmaxb += dpb;
-    else qminb += dpb;
-    qb -= dpb;
-    qtildeb += dnb;
-    qb -= dnb;
-}
-
-// reconstruct_b: adjoint of the limited reconstruction to primitive variables.
+// reconstruct_b: adjoint of the limited reconstruction to primitive
+// variables.  The Venkatakrishnan limiter of each component (its forward
+// value and venkat_limiter_b) shares one reciprocal of its denominator:
+// phi = num (1/den), num_b = phi_b (1/den), den_b = -phi_b phi (1/den).
 __device__ __forceinline__ void reconstruct_b(const double q[4], const double dqx[4],
                                               const double dqy[4], const double qmax[4],
                                               const double qmin[4], double eps2, double delx,
@@ -288,12 +259,26 @@ __device__ __forceinline__ void reconstruct_b(const double q[4], const double dq
                                               double u2b, double rhob, double prb, double qb[4],
                                               double dqxb[4], double dqyb[4], double qmaxb[4],
                                               double qminb[4], double &delxb, double &delyb) {
-    double qt[4], t[4], qt0[4], phi[4];
+    double qt[4], t[4], phi[4], idn[4];
+    unsigned active = 0;  // bit r: the limiter of component r is below 1
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         t[r] = delx * dqx[r] + dely * dqy[r];
-        qt0[r] = q[r] - 0.5 * t[r];
-        phi[r] = venkat_phi<double>(qt0[r], q[r], qmax[r], qmin[r], eps2);
+        const double dn = (q[r] - 0.5 * t[r]) - q[r];
+        phi[r] = 1.0;
+        idn[r] = 0.0;
+        if (fabs(dn) > MFCFD_VENKAT_THR) {
+            const double dp = dn > 0.0 ? qmax[r] - q[r] : qmin[r] - q[r];
+            const double num = ((dp * dp) + eps2) * dn + 2.0 * dn * dn * dp;
+            const double den = ((dp * dp + 2.0 * dn * dn) + dn * dp + eps2) * dn;
+            const double id = 1.0 / den;
+            const double temp = num * id;
+            if (temp < 1.0) {
+                phi[r] = temp;
+                idn[r] = id;
+                active |= 1u << r;
+            }
+        }
         qt[r] = q[r] - 0.5 * phi[r] * t[r];
     }
     double qtb[4] = {0.0, 0.0, 0.0, 0.0};
@@ -301,13 +286,35 @@ __device__ __forceinline__ void reconstruct_b(const double q[4], const double dq
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         qb[r] += qtb[r];
-        const double phib = -0.5 * t[r] * qtb[r];
         double tb = -0.5 * phi[r] * qtb[r];
-        double qt0b = 0.0;
-        venkat_phi_b(qt0[r], q[r], qmax[r], qmin[r], eps2, phib, qt0b, qb[r], qmaxb[r],
-                     qminb[r]);
-        qb[r] += qt0b;
-        tb += -0.5 * qt0b;
+        if ((active >> r) & 1u) {
+            // venkat_limiter_b of component r
+            const double phib = -0.5 * t[r] * qtb[r];
+            const double dn = (q[r] - 0.5 * t[r]) - q[r];
+            const bool up = dn > 0.0;
+            const double dp = up ? qmax[r] - q[r] : qmin[r] - q[r];
+            const double num1 = (dp * dp) + eps2;
+            const double den1 = dp * dp + 2.0 * dn * dn;
+            const double den2 = den1 + dn * dp + eps2;
+            const double numb = phib * idn[r];
+            const double denb = -phib * phi[r] * idn[r];
+            const double den2b = denb * dn;
+            double dnb = denb * den2;
+            const double den1b = den2b;
+            dnb += den2b * dp;
+            double dpb = den2b * dn;
+            dpb += den1b * 2.0 * dp;
+            dnb += den1b * 4.0 * dn;
+            const double num1b = numb * dn;
+            dnb += numb * (num1 + 4.0 * dn * dp);
+            dpb += numb * 2.0 * dn * dn;
+            dpb += num1b * 2.0 * dp;
+            if (up) qmaxb[r] += dpb;
+            else qminb[r] += dpb;
+            qb[r] -= dpb;
+            // dn = qt0 - q with qt0 = q - t/2: q's two shares of dnb cancel
+            tb += -0.5 * dnb;
+        }
         delxb += tb * dqx[r];
         delyb += tb * dqy[r];
         dqxb[r] += tb * delx;
