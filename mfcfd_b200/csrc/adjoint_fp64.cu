@@ -46,6 +46,22 @@ __device__ __forceinline__ void kst_store(double *e, const KState &s) {
     e[0] = s.rho; e[1] = s.ut; e[2] = s.un; e[3] = s.pbr; e[4] = s.usq;
     e[5] = s.B1; e[6] = s.B2; e[7] = s.e1; e[8] = s.e2;
 }
+// A kinetic state from its tape entry (rho, p/rho, B1, B2, e1, e2, u1, u2)
+// and the point's normal, as reconstruct_kstate forms ut, un and |u|^2.
+__device__ __forceinline__ KState kst_taped(const double *v, double nx, double ny) {
+    KState s;
+    const double tx = ny, ty = -nx;
+    s.rho = v[0];
+    s.pbr = v[1];
+    s.B1 = v[2];
+    s.B2 = v[3];
+    s.e1 = v[4];
+    s.e2 = v[5];
+    s.ut = v[6] * tx + v[7] * ty;
+    s.un = v[6] * nx + v[7] * ny;
+    s.usq = s.ut * s.ut + s.un * s.un;
+    return s;
+}
 __device__ __forceinline__ KState kst_load(const double *e) {
     KState s;
     s.rho = e[0]; s.ut = e[1]; s.un = e[2]; s.pbr = e[3]; s.usq = e[4];
@@ -220,10 +236,10 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
                     v[2 * hh] = t2.x;
                     v[2 * hh + 1] = t2.y;
                 }
-                si = KState{v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7], v[8]};
-                sk = KState{v[11], v[12], v[13], v[14], v[15], v[16], v[17], v[18], v[19]};
-                e_[0] = v[9]; e_[1] = v[10]; e_[2] = si.rho; e_[3] = si.rho * si.pbr;
-                e_[4] = v[20]; e_[5] = v[21]; e_[6] = sk.rho; e_[7] = sk.rho * sk.pbr;
+                si = kst_taped(v, nx, ny);
+                sk = kst_taped(v + 8, nx, ny);
+                e_[0] = v[6]; e_[1] = v[7]; e_[2] = si.rho; e_[3] = si.rho * si.pbr;
+                e_[4] = v[14]; e_[5] = v[15]; e_[6] = sk.rho; e_[7] = sk.rho * sk.pbr;
             } else {
                 const R4 qv = ld4(q_in + i), kv = ld4(q_in + k);
                 const double qi[4] = {qv.a, qv.b, qv.c, qv.d}, qk[4] = {kv.a, kv.b, kv.c, kv.d};

@@ -97,8 +97,8 @@ struct StageBufs {
     double *kstape = nullptr;
 };
 // doubles per (point, slot) in the kinetic-state tape: for the point's and
-// then the neighbour's reconstruction rho ut un p/rho |u|^2 B1 B2 erf1 erf2 u1 u2
-constexpr int KS_TAPE = 22;
+// then the neighbour's reconstruction rho p/rho B1 B2 erf1 erf2 u1 u2
+constexpr int KS_TAPE = 16;
 
 // The passes of one stage.  Each is a grid-stride kernel over the tiles of
 // the scheduled instances; `block` threads per block for the point passes

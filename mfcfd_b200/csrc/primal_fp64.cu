@@ -348,10 +348,11 @@ flux_group(const Geom &g, const Consts &c, const StageBufs &b, int i, bool valid
                                         inv_gm1, nx, ny, inv_sqrt_pi, TAPE ? ui : nullptr);
             }
             if (TAPE) {
-                const double v[KS_TAPE] = {si.rho, si.ut, si.un, si.pbr, si.usq, si.B1, si.B2,
-                                           si.e1,  si.e2, ui[0], ui[1], sk.rho, sk.ut, sk.un,
-                                           sk.pbr, sk.usq, sk.B1, sk.B2, sk.e1, sk.e2, uk[0],
-                                           uk[1]};
+                // per state rho, p/rho, B1, B2, e1, e2, u1, u2 (ut, un and
+                // |u|^2 follow from u and the point's normal)
+                const double v[KS_TAPE] = {si.rho, si.pbr, si.B1, si.B2, si.e1, si.e2, ui[0],
+                                           ui[1],  sk.rho, sk.pbr, sk.B1, sk.B2, sk.e1, sk.e2,
+                                           uk[0],  uk[1]};
                 double2 *tp = reinterpret_cast<double2 *>(
                     b.kstape + ((size_t)i * g.kp + r) * KS_TAPE);
 #pragma unroll
