@@ -243,7 +243,7 @@ int record(mfcfd_t *h, AdjointState *a, const R4 *from) {
         launch_grad(h->geom, h->consts, h->sched, a->tq[rk - 1], a->tspd, dq_at(a, rk, 0),
                     qm_at(a, rk), a->tdelta, rk == 1, h->point_block, h->point_grid, h->stream);
         for (int t = 1; t <= m; ++t)
-            launch_inner(h->geom, h->consts, h->sched, a->tq[rk - 1], dq_at(a, rk, t - 1),
+            launch_inner(h->geom, h->consts, h->sched, dq_at(a, rk, 0), dq_at(a, rk, t - 1),
                          dq_at(a, rk, t), h->point_block, h->inner_grid, h->stream);
         StageBufs b;
         b.prim_in = a->tprim[rk - 1];

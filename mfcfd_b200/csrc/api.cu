@@ -68,8 +68,8 @@ void free_all(mfcfd_t *h) {
         for (auto &g : row)
             if (g) cudaGraphExecDestroy(g);
     void *bufs[] = {h->d_xy, h->d_nrm, h->d_eps2, h->d_obc, h->d_conn, h->d_nbhs, h->d_mx,
-                    h->d_my, h->d_prim[0], h->d_prim[1], h->d_q[0], h->d_q[1], h->d_dq[0],
-                    h->d_dq[1], h->d_qm, h->d_delta, h->d_spd, h->d_res_part, h->d_flux_dbg,
+                    h->d_my, h->d_hoff, h->d_hrow, h->d_hloc, h->d_prim[0], h->d_prim[1], h->d_q[0], h->d_q[1], h->d_dq[0],
+                    h->d_dq[1], h->d_dq[2], h->d_qm, h->d_delta, h->d_spd, h->d_res_part, h->d_flux_dbg,
                     h->d_hist, h->d_forces, h->d_ctl, h->d_sh_idx, h->d_sh_shape, h->d_sh_geo,
                     h->d_sh_my, h->f_prim[0], h->f_prim[1], h->f_q[0], h->f_q[1],
                     h->f_dq[0], h->f_dq[1], h->f_dq[2], h->f_qm, h->f_eps2, h->f_dxy, h->f_w, h->f_lsq,
@@ -127,8 +127,8 @@ void launch_stage(mfcfd_t *h, cudaStream_t s, int rk, int A, int B, F after) {
                     h->d_delta, rk == 1, h->point_block, h->point_grid, s);
         after();
         for (int t = 1; t <= m; ++t) {
-            launch_inner(h->geom, h->consts, h->sched, q_in, h->d_dq[(t - 1) & 1],
-                         h->d_dq[t & 1], h->point_block, h->inner_grid, s);
+            launch_inner(h->geom, h->consts, h->sched, h->d_dq[0], h->d_dq[dq_src(t)],
+                         h->d_dq[dq_dst(t)], h->point_block, h->inner_grid, s);
             after();
         }
         StageBufs b;
@@ -137,7 +137,7 @@ void launch_stage(mfcfd_t *h, cudaStream_t s, int rk, int A, int B, F after) {
         b.prim_old = h->d_prim[A];
         b.q_in = q_in;
         b.q_out = h->d_q[h->qcur ^ 1];
-        b.dq = h->d_dq[m & 1];
+        b.dq = h->d_dq[dq_final(m)];
         b.qm = h->d_qm;
         b.delta = h->d_delta;
         b.spd = h->d_spd;
@@ -273,6 +273,56 @@ int lskum_host::upload_state_aux(mfcfd_t *h) {
 }
 
 using lskum_host::upload_state_aux;
+
+// A tile's halo lists its rows in ascending order, so that the rows of
+// neighbouring rings come in contiguous runs and the staging copies
+// coalesce; the local indices are positions in that list.
+void lskum_host::build_halo(int n, int kp, const int *conn, const int *nbhs,
+                            const std::vector<std::pair<int, int>> &ranges, HostHalo &out) {
+    const int ntile = (n + TILE - 1) / TILE;
+    out.hkp = ((kp + 1 + 7) / 8) * 8;
+    out.hc = 0;
+    out.off.assign((size_t)ntile + 1, 0);
+    out.rows.clear();
+    out.loc.assign((size_t)n * out.hkp, 0);
+    if (out.hkp > 24) {  // local row bytes beyond three words: no halos
+        out.off.assign((size_t)ntile + 1, 0);
+        out.loc.clear();
+        return;
+    }
+    std::vector<int> tend(ntile, -1);  // end of the tile's owned points (-1: not scheduled)
+    for (const auto &rg : ranges)
+        for (int p0 = rg.first; p0 < rg.first + rg.second; p0 += TILE)
+            tend[p0 / TILE] = std::min(p0 + TILE, rg.first + rg.second);
+    std::vector<int> rows;
+    rows.reserve((size_t)TILE * (kp + 1));
+    for (int t = 0; t < ntile; ++t) {
+        out.off[t] = (int)out.rows.size();
+        if (tend[t] < 0) continue;
+        rows.clear();
+        for (int p = t * TILE; p < tend[t]; ++p) {
+            rows.push_back(p);
+            for (int r = 0; r < nbhs[p]; ++r) rows.push_back(conn[(size_t)r * n + p]);
+        }
+        std::sort(rows.begin(), rows.end());
+        rows.erase(std::unique(rows.begin(), rows.end()), rows.end());
+        if ((int)rows.size() > HALO_CAP) continue;  // gathered directly
+        auto pos = [&](int k) {
+            return (unsigned char)(std::lower_bound(rows.begin(), rows.end(), k) - rows.begin());
+        };
+        for (int p = t * TILE; p < tend[t]; ++p) {
+            unsigned char *l = out.loc.data() + (size_t)p * out.hkp;
+            for (int r = 0; r < nbhs[p]; ++r) l[r] = pos(conn[(size_t)r * n + p]);
+            l[out.hkp - 1] = pos(p);
+        }
+        out.hc = std::max(out.hc, (int)rows.size());
+        out.rows.insert(out.rows.end(), rows.begin(), rows.end());
+    }
+    out.off[ntile] = (int)out.rows.size();
+    // the staging stride: one more than a multiple of eight rows, so that a
+    // row's 16-byte pieces in consecutive arrays fall on different banks
+    if (out.hc > 0) out.hc += (9 - out.hc % 8) % 8;
+}
 
 int lskum_host::reset_run(mfcfd_t *h, int it_first) {
     h->h_ctl->it = it_first;
@@ -719,6 +769,7 @@ static int create_handle(const mfcfd_grid *grid, const mfcfd_params *params, int
     for (int c = 0; c < 4; ++c) h->q_inf[c] = hg.q_inf[c];
 
     // device arrays
+    HostHalo halo;  // FP64 D and I passes
     int st = MFCFD_OK;
     auto up = [&](auto *d, const auto &v) -> int {
         cudaError_t e = cudaMemcpy(d, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice);
@@ -749,11 +800,19 @@ static int create_handle(const mfcfd_grid *grid, const mfcfd_params *params, int
     ALLOC(h->d_mx, n);
     ALLOC(h->d_my, n);
     if (!h->fp32) {
+        lskum_host::build_halo(n, kp, hconn.data(), hnb.data(), {{0, nl}}, halo);
+        if (halo.hc > 0) {
+            ALLOC(h->d_hoff, halo.off.size());
+            ALLOC(h->d_hrow, halo.rows.size());
+            ALLOC(h->d_hloc, halo.loc.size());
+        }
+    }
+    if (!h->fp32) {
         for (int b = 0; b < 2; ++b) {
             ALLOC(h->d_prim[b], n);
             ALLOC(h->d_q[b], n);
-            ALLOC(h->d_dq[b], (size_t)8 * n);
         }
+        for (int b = 0; b < 3; ++b) ALLOC(h->d_dq[b], (size_t)8 * n);
         ALLOC(h->d_qm, (size_t)8 * n);
     } else {
         ALLOC(h->d_prim[0], n);  // FP64 copy of the state for forces/diagnostics
@@ -796,6 +855,9 @@ static int create_handle(const mfcfd_grid *grid, const mfcfd_params *params, int
         (st = up(h->d_obc, hobc)) || (st = up(h->d_conn, hconn)) || (st = up(h->d_nbhs, hnb)) ||
         (st = up(h->d_mx, hmx)) || (st = up(h->d_my, hmy)))
         goto fail_create;
+    if (h->d_hoff && ((st = up(h->d_hoff, halo.off)) || (st = up(h->d_hrow, halo.rows)) ||
+                      (st = up(h->d_hloc, halo.loc))))
+        goto fail_create;
     if (h->fp32) {
         std::vector<float> feps(heps.begin(), heps.end());
         if ((st = up(h->f_eps2, feps)) || (st = up(h->f_dxy, hg.dxy)) ||
@@ -811,6 +873,13 @@ static int create_handle(const mfcfd_grid *grid, const mfcfd_params *params, int
     }
     h->geom = Geom{n, kp, nw, no, h->d_xy, h->d_nrm, h->d_eps2, h->d_conn, h->d_nbhs,
                    h->d_mx, h->d_my, h->d_obc};
+    if (h->d_hoff) {
+        h->geom.hoff = h->d_hoff;
+        h->geom.hrow = h->d_hrow;
+        h->geom.hloc = h->d_hloc;
+        h->geom.hkp = halo.hkp;
+        h->geom.hc = halo.hc;
+    }
     h->consts.cfl = P.cfl;
     h->consts.power = P.power;
     h->consts.euler = P.euler;
@@ -1127,7 +1196,7 @@ int mfcfd_get_array(mfcfd_t *h, const char *name, double *out) {
         return MFCFD_OK;
     }
     if (s == "q") { src = reinterpret_cast<const double *>(h->d_q[h->qcur ^ 1]); w = 4; }
-    else if (s == "dq") { src = h->d_dq[h->p.inner_iterations & 1]; w = 8; }
+    else if (s == "dq") { src = h->d_dq[dq_final(h->p.inner_iterations)]; w = 8; }
     else if (s == "qm") { src = h->d_qm; w = 8; }
     else if (s == "delta") { src = h->d_delta; w = 1; }
     else if (s == "flux_res") {
@@ -1316,9 +1385,9 @@ extern "C" int mfcfd_part_phase(mfcfd_t *h, int phase, int rk, int t, double *va
         break;
     case MFCFD_PHASE_INNER:
         if (t < 1 || t > m) return fail(h, MFCFD_ERR_ARG, "inner iteration t out of range");
-        launch_inner(h->geom, h->consts, h->sched, h->d_q[h->qcur], h->d_dq[(t - 1) & 1],
-                     h->d_dq[t & 1], h->point_block, h->inner_grid, s);
-        h->part_dq = t & 1;
+        launch_inner(h->geom, h->consts, h->sched, h->d_dq[0], h->d_dq[dq_src(t)],
+                     h->d_dq[dq_dst(t)], h->point_block, h->inner_grid, s);
+        h->part_dq = dq_dst(t);
         break;
     case MFCFD_PHASE_FLUX: {
         StageBufs b;
@@ -1327,7 +1396,7 @@ extern "C" int mfcfd_part_phase(mfcfd_t *h, int phase, int rk, int t, double *va
         b.prim_old = h->d_prim[A];
         b.q_in = h->d_q[h->qcur];
         b.q_out = h->d_q[h->qcur ^ 1];
-        b.dq = h->d_dq[m & 1];
+        b.dq = h->d_dq[dq_final(m)];
         b.qm = h->d_qm;
         b.delta = h->d_delta;
         b.spd = h->d_spd;

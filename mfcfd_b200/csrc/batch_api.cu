@@ -61,8 +61,10 @@ struct mfcfd_batch {
     double *d_eps2 = nullptr, *d_obc = nullptr;
     int *d_conn = nullptr, *d_nbhs = nullptr;
     unsigned long long *d_mx = nullptr, *d_my = nullptr;
+    int *d_hoff = nullptr, *d_hrow = nullptr;  // tile halos of the FP64 D and I passes
+    unsigned char *d_hloc = nullptr;
     R4 *d_prim[2] = {nullptr, nullptr}, *d_q[2] = {nullptr, nullptr};
-    double *d_dq[2] = {nullptr, nullptr};
+    double *d_dq[3] = {nullptr, nullptr, nullptr};
     double *d_qm = nullptr;
     float4 *f_prim[2] = {nullptr, nullptr}, *f_q[2] = {nullptr, nullptr};
     float *f_dq[3] = {nullptr, nullptr, nullptr};
@@ -134,8 +136,8 @@ void drop_graphs(mfcfd_batch_t *b) {
 void free_batch(mfcfd_batch_t *b) {
     drop_graphs(b);
     void *bufs[] = {b->d_xy, b->d_nrm, b->d_eps2, b->d_obc, b->d_conn, b->d_nbhs, b->d_mx,
-                    b->d_my, b->d_prim[0], b->d_prim[1], b->d_q[0], b->d_q[1], b->d_dq[0],
-                    b->d_dq[1], b->d_qm, b->f_prim[0], b->f_prim[1], b->f_q[0], b->f_q[1],
+                    b->d_my, b->d_hoff, b->d_hrow, b->d_hloc, b->d_prim[0], b->d_prim[1], b->d_q[0], b->d_q[1], b->d_dq[0],
+                    b->d_dq[1], b->d_dq[2], b->d_qm, b->f_prim[0], b->f_prim[1], b->f_q[0], b->f_q[1],
                     b->f_dq[0], b->f_dq[1], b->f_dq[2], b->f_qm, b->f_eps2, b->f_dxy, b->f_w, b->f_lsq,
                     b->f_flsq, b->d_delta, b->d_spd,
                     b->d_res_part, b->d_hist, b->d_forces, b->d_inst, b->d_sched, b->d_run,
@@ -191,15 +193,15 @@ void batch_stage(mfcfd_batch_t *b, cudaStream_t s, int rk, int A, int B) {
         launch_grad(b->geom, b->consts, b->sched, q_in, b->d_spd, b->d_dq[0], b->d_qm,
                     b->d_delta, rk == 1, pb, pg, s);
         for (int t = 1; t <= m; ++t)
-            launch_inner(b->geom, b->consts, b->sched, q_in, b->d_dq[(t - 1) & 1],
-                         b->d_dq[t & 1], pb, ig, s);
+            launch_inner(b->geom, b->consts, b->sched, b->d_dq[0], b->d_dq[dq_src(t)],
+                         b->d_dq[dq_dst(t)], pb, ig, s);
         StageBufs sb;
         sb.prim_in = rk == 1 ? b->d_prim[A] : b->d_prim[B];
         sb.prim_out = b->d_prim[B];
         sb.prim_old = b->d_prim[A];
         sb.q_in = q_in;
         sb.q_out = b->d_q[b->qcur ^ 1];
-        sb.dq = b->d_dq[m & 1];
+        sb.dq = b->d_dq[dq_final(m)];
         sb.qm = b->d_qm;
         sb.delta = b->d_delta;
         sb.spd = b->d_spd;
@@ -526,6 +528,7 @@ int mfcfd_batch_create(int n_inst, const mfcfd_grid *const *grids, const mfcfd_p
         h = HostGrid();
     }
 
+    HostHalo halo;  // FP64 D and I passes
     int st = MFCFD_OK;
     auto up = [&](auto *d, const auto &v) -> int {
         if (v.empty()) return MFCFD_OK;
@@ -559,11 +562,21 @@ int mfcfd_batch_create(int n_inst, const mfcfd_grid *const *grids, const mfcfd_p
     BALLOC(b->d_mx, N);
     BALLOC(b->d_my, N);
     if (!b->fp32) {
+        std::vector<std::pair<int, int>> ranges;
+        for (int i = 0; i < n_inst; ++i) ranges.emplace_back(b->inst[i].base, info[i].n);
+        lskum_host::build_halo(N, kp, conn.data(), nbhs.data(), ranges, halo);
+        if (halo.hc > 0) {
+            BALLOC(b->d_hoff, halo.off.size());
+            BALLOC(b->d_hrow, halo.rows.size());
+            BALLOC(b->d_hloc, halo.loc.size());
+        }
+    }
+    if (!b->fp32) {
         for (int k = 0; k < 2; ++k) {
             BALLOC(b->d_prim[k], N);
             BALLOC(b->d_q[k], N);
-            BALLOC(b->d_dq[k], (size_t)8 * N);
         }
+        for (int k = 0; k < 3; ++k) BALLOC(b->d_dq[k], (size_t)8 * N);
         BALLOC(b->d_qm, (size_t)8 * N);
     } else {
         BALLOC(b->d_prim[0], N);  // FP64 copy of the state for the force sums
@@ -611,6 +624,9 @@ int mfcfd_batch_create(int n_inst, const mfcfd_grid *const *grids, const mfcfd_p
         (st = up(b->d_sh_idx, sidx)) || (st = up(b->d_sh_shape, sshape)) ||
         (st = up(b->d_sh_geo, sgeo)) || (st = up(b->d_sh_my, smy)))
         goto fail_create;
+    if (b->d_hoff && ((st = up(b->d_hoff, halo.off)) || (st = up(b->d_hrow, halo.rows)) ||
+                      (st = up(b->d_hloc, halo.loc))))
+        goto fail_create;
     if (b->fp32) {
         std::vector<float> feps(eps2.begin(), eps2.end());
         if ((st = up(b->f_eps2, feps)) || (st = up(b->f_dxy, dxy)) || (st = up(b->f_lsq, lsq)) ||
@@ -621,6 +637,13 @@ int mfcfd_batch_create(int n_inst, const mfcfd_grid *const *grids, const mfcfd_p
     }
     b->geom = Geom{N, kp, 0, 0, b->d_xy, b->d_nrm, b->d_eps2, b->d_conn, b->d_nbhs,
                    b->d_mx, b->d_my, b->d_obc};
+    if (b->d_hoff) {
+        b->geom.hoff = b->d_hoff;
+        b->geom.hrow = b->d_hrow;
+        b->geom.hloc = b->d_hloc;
+        b->geom.hkp = halo.hkp;
+        b->geom.hc = halo.hc;
+    }
     b->consts.cfl = P0.cfl;
     b->consts.power = P0.power;
     b->consts.euler = P0.euler;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "mfcfd_b200.h"
@@ -30,8 +31,10 @@ struct mfcfd {
     double *d_eps2 = nullptr, *d_obc = nullptr;
     int *d_conn = nullptr, *d_nbhs = nullptr;
     unsigned long long *d_mx = nullptr, *d_my = nullptr;
+    int *d_hoff = nullptr, *d_hrow = nullptr;  // tile halos of the D and I passes
+    unsigned char *d_hloc = nullptr;
     R4 *d_prim[2] = {nullptr, nullptr}, *d_q[2] = {nullptr, nullptr};
-    double *d_dq[2] = {nullptr, nullptr};
+    double *d_dq[3] = {nullptr, nullptr, nullptr};  // D-pass result, then the inner iterations'
     double *d_qm = nullptr, *d_delta = nullptr, *d_spd = nullptr, *d_res_part = nullptr;
     double *d_flux_dbg = nullptr, *d_hist = nullptr, *d_forces = nullptr;
     int hist_cap = 0;
@@ -108,7 +111,19 @@ struct HostGrid {
     std::vector<float4> flsq;   // [2n] per split list, two solve coefficients
 };
 
+// Tile halos (Geom::hoff, hrow, hloc) of a renumbered point set of n points
+// with ELL stencils conn[r * n + p] (nbhs[p] slots used), for the tiles of
+// the point ranges [b, b + m) of `ranges` (each b a multiple of TILE); every
+// other tile gets an empty halo.
+struct HostHalo {
+    std::vector<int> off, rows;
+    std::vector<unsigned char> loc;
+    int hkp = 0, hc = 0;
+};
+
 namespace lskum_host {
+void build_halo(int n, int kp, const int *conn, const int *nbhs,
+                const std::vector<std::pair<int, int>> &ranges, HostHalo &out);
 // n_local < 0: every point is owned; else points [n_local, n) are ghosts
 int prepare_grid(const mfcfd_grid &G, const mfcfd_params &P, HostGrid &hg, int n_local = -1);
 int fail(mfcfd_t *h, int code, const std::string &msg);

@@ -45,7 +45,20 @@ struct Geom {
     const unsigned long long *mx;  // bit r: slot r in xpos; bit 32+r: in xneg
     const unsigned long long *my;  // bit r: slot r in ypos; bit 32+r: in yneg
     const double *obc;             // outer points: u1_inf_rot, u2_inf_rot, e_inf, A2n_inf, B2_inf, 0,0,0
+    // Tile halos of the D and I passes (nullptr: no halo, every row is
+    // gathered directly).  The halo of a TILE-point tile is the sorted set of
+    // rows its points read (the points themselves and their neighbours);
+    // hoff[tile] .. hoff[tile + 1] index its rows in hrow (an empty range: the
+    // tile's halo exceeds HALO_CAP and its rows are gathered directly).
+    // hloc[p * hkp + r] is slot r's row within the tile's halo, hloc[p * hkp
+    // + hkp - 1] the point's own; hc = the largest halo, the staging stride.
+    const int *hoff = nullptr;
+    const int *hrow = nullptr;
+    const unsigned char *hloc = nullptr;
+    int hkp = 0, hc = 0;
 };
+// rows a tile halo stages at most (its local row indices are bytes)
+constexpr int HALO_CAP = 64;
 
 struct Consts {
     double cfl, power, euler, pi, gm1;  // gm1 = gamma - 1
@@ -152,9 +165,10 @@ __device__ __forceinline__ KStateT<T> kstate(T u1, T u2, T rho, T pr, T nx, T ny
 // qtilde itself (beta = -qtilde_4/2, p/rho = 1/(2 beta)), which the
 // reference's 0.5 rho/p and p/rho of the same state equal in exact
 // arithmetic; 0.5/sqrt(pi beta) is formed as (p/rho) sqrt(beta) / sqrt(pi)
-// and log(beta)/(gamma-1) as log(beta) * (1/(gamma-1)).  Five divisions
-// and one square root per state instead of ten and two; the results differ
-// from reconstruct + kstate by rounding only.
+// and beta**(-1/(gamma-1)) without a log (below).  Five divisions and one
+// reciprocal square root per state instead of ten divisions, two square
+// roots and a log; the results differ from reconstruct + kstate by rounding
+// only.
 template <class T>
 __device__ __forceinline__ KStateT<T> reconstruct_kstate(const T q[4], const T dqx[4],
                                                          const T dqy[4], const T qmax[4],
@@ -176,13 +190,19 @@ __device__ __forceinline__ KStateT<T> reconstruct_kstate(const T q[4], const T d
         u_out[1] = u2;
     }
     const T temp1 = qt[0] + beta * (u1 * u1 + u2 * u2);
-    const T temp2 = temp1 - log(beta) * inv_gm1;
     KStateT<T> s;
-    s.rho = exp(temp2);
+    // rho = exp(temp1 - log(beta)/(gamma-1)) with gamma = 1.4, a constant of
+    // the reference (parameter.F90:10): beta**(-1/(gamma-1)) = beta**(-2.5)
+    // = (1/beta)**2 / sqrt(beta), 1/beta = 2 p/rho -- no log, and sqrt(beta)
+    // from the same reciprocal square root (C2: 0.705 -> 0.649 ms a flux
+    // pass).  inv_gm1 is kept in the signature for the callers.
+    const T rb = rsqrt(beta);
+    const T sb = beta * rb;
+    s.rho = exp(temp1) * ((T(4.0) * temp * temp) * rb);
+    (void)inv_gm1;
     const T tx = ny, ty = -nx;
     s.ut = u1 * tx + u2 * ty;
     s.un = u1 * nx + u2 * ny;
-    const T sb = sqrt(beta);
     const T S1 = s.ut * sb, S2 = s.un * sb;
     const T h = temp * sb * inv_sqrt_pi;  // 0.5 / sqrt(pi beta)
     s.B1 = exp(-S1 * S1) * h;

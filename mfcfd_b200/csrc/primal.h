@@ -109,7 +109,9 @@ void launch_grad(const Geom &g, const Consts &c, const Sched &s, const R4 *q, co
                  double *dq, double *qm, double *delta, bool with_delta, int block, int grid,
                  cudaStream_t st);
 // I pass: one inner iteration (eval_q_inner_loop + eval_update_innerloop).
-void launch_inner(const Geom &g, const Consts &c, const Sched &s, const R4 *q,
+// dq0: the stage's D-pass derivatives (kept through its inner iterations;
+// the FP64 dq buffers rotate as dq_src / dq_dst say).
+void launch_inner(const Geom &g, const Consts &c, const Sched &s, const double *dq0,
                   const double *dq_in, double *dq_out, int block, int grid, cudaStream_t st);
 // F pass: flux residual + state update of stage rk (1-based).
 void launch_flux(const Geom &g, const Consts &c, const Sched &s, const StageBufs &b, int rk,
@@ -195,6 +197,10 @@ void launch_inner32(const Geom &g, const Consts &c, const Geom32 &f, const Sched
 inline int dq32_src(int t) { return t == 1 ? 0 : 1 + ((t - 2) & 1); }
 inline int dq32_dst(int t) { return 1 + ((t - 1) & 1); }
 inline int dq32_final(int m) { return m == 0 ? 0 : dq32_dst(m); }
+// the FP64 dq buffers of a stage rotate the same way
+inline int dq_src(int t) { return dq32_src(t); }
+inline int dq_dst(int t) { return dq32_dst(t); }
+inline int dq_final(int m) { return dq32_final(m); }
 void launch_flux32(const Geom &g, const Consts &c, const Sched &s, const StageBufs32 &b, int rk,
                    bool last, int grid, cudaStream_t st);
 void launch_init_state32(const Geom &g, const float4 *prim, float4 *q, double *spd,

@@ -188,65 +188,392 @@ kb_grad(Geom g, Consts c, Sched s, const R4 *__restrict__ q, const double *__res
     }
 }
 
-// q_variables.F90:115-227 eval_q_inner_loop + eval_update_innerloop: reads
-// dq_in, writes dq_out (the buffers swap instead of copying temp into dq).
-// A thread per point with its neighbour rows in 256-bit loads: staging them
-// in shared memory as the D pass does was measured slower here (C2: 0.156
-// against 0.121 ms per launch), since a slot moves 112 bytes in seven 16-byte
-// copies where two 256-bit loads and two narrower ones fetch it directly.
-__device__ __forceinline__ void
-inner_point(const Geom &g, const Consts &c, const R4 *__restrict__ q,
-            const double *__restrict__ dq_in, double *__restrict__ dq_out, int i) {
-    double2 pi_ = g.xy[i];
-    R4 qv = ld4w(q + i);
-    double qi[4] = {qv.a, qv.b, qv.c, qv.d};
-    double dxi[4], dyi[4];
-    ld8w(dq_in + 8 * (size_t)i, dxi, dyi);
+// Row sources of the per-point sums of the D and I passes: the rows of a
+// point's stencil gathered from global memory, or from its tile's halo
+// staged in shared memory (kb_grad_h, kb_inner_h).  Both give the same
+// values, so the sums below do not depend on where their rows come from.
+struct GlobalRows {
+    const Geom &g;
+    const R4 *q;
+    const double *dq;   // I pass: dq_in
+    const double *spd;  // D pass
+    int i;
+    __device__ __forceinline__ int self() const { return i; }
+    __device__ __forceinline__ int nbr(int r) const { return g.conn[r * g.n + i]; }
+    __device__ __forceinline__ double2 xy(int k) const { return g.xy[k]; }
+    __device__ __forceinline__ void qrow(int k, double v[4]) const {
+        const R4 a = ld4w(q + k);
+        v[0] = a.a; v[1] = a.b; v[2] = a.c; v[3] = a.d;
+    }
+    __device__ __forceinline__ void dqrow(int k, double x[4], double y[4]) const {
+        ld8w(dq + 8 * (size_t)k, x, y);
+    }
+    __device__ __forceinline__ double spdv(int k) const { return spd[k]; }
+};
+
+// Shared-memory arrays of a staged tile halo, hc rows each (hc is the
+// staging stride, one more than a multiple of eight, so that the arrays of a
+// row start on different banks): D pass q[0..1], q[2..3], (x, y), (spd, -);
+// I pass (x, y), dq/dx[0..1], dq/dx[2..3], dq/dy[0..1], dq/dy[2..3].  One
+// 16-byte array per pair keeps a warp's reads of neighbouring rows on
+// distinct banks.
+constexpr int HA_I = 5, HA_D = 4;
+constexpr int HALO_BLOCK = 128;  // four warps, a half-warp per tile
+// resident blocks per SM the register budget allows, measured at C2: the D
+// pass 0.090 ms at 4 (128 registers), 0.102 at 5, 0.132 at 6; the I pass
+// 0.119 ms at 4, 0.087 at 5 (96 registers), 0.092 at 6
+#ifndef HALO_MIN_BLOCKS_D
+#define HALO_MIN_BLOCKS_D 4
+#endif
+#ifndef HALO_MIN_BLOCKS_I
+#define HALO_MIN_BLOCKS_I 5
+#endif
+
+template <int nA>
+struct HaloRows {
+    static constexpr int OXY = nA == HA_I ? 0 : 2, ODQ = 1, OSPD = 3;
+    const double2 *sm;
+    int hc;
+    unsigned long long w0, w1, w2;  // the point's local row bytes (slots, then its own)
+    int own;
+    // i < 0: no point (nothing is loaded)
+    __device__ __forceinline__ HaloRows(const Geom &g, const double2 *sm_, int i)
+        : sm(sm_), hc(g.hc), w0(0ull), w1(0ull), w2(0ull), own(0) {
+        if (i < 0) return;
+        const unsigned long long *lw =
+            reinterpret_cast<const unsigned long long *>(g.hloc + (size_t)i * g.hkp);
+        w0 = __ldg(lw);
+        if (g.hkp > 8) w1 = __ldg(lw + 1);
+        if (g.hkp > 16) w2 = __ldg(lw + 2);
+        const unsigned long long last = g.hkp > 16 ? w2 : (g.hkp > 8 ? w1 : w0);
+        own = (int)(last >> 56);
+    }
+    __device__ __forceinline__ int self() const { return own; }
+    __device__ __forceinline__ int nbr(int r) const {
+        const unsigned long long w = r < 8 ? w0 : (r < 16 ? w1 : w2);
+        return (int)((w >> (8 * (r & 7))) & 0xffull);
+    }
+    __device__ __forceinline__ double2 xy(int l) const { return sm[OXY * hc + l]; }
+    __device__ __forceinline__ void qrow(int l, double v[4]) const {
+        const double2 a = sm[l], b = sm[hc + l];
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    }
+    __device__ __forceinline__ void dqrow(int l, double x[4], double y[4]) const {
+        const double2 a = sm[ODQ * hc + l], b = sm[(ODQ + 1) * hc + l],
+                      e = sm[(ODQ + 2) * hc + l], f = sm[(ODQ + 3) * hc + l];
+        x[0] = a.x; x[1] = a.y; x[2] = b.x; x[3] = b.y;
+        y[0] = e.x; y[1] = e.y; y[2] = f.x; y[3] = f.y;
+    }
+    __device__ __forceinline__ double spdv(int l) const { return sm[OSPD * hc + l].x; }
+};
+
+// q_variables.F90:41-112 eval_q_derivatives and state_update.F90:190-236
+// func_delta over the rows of R, in slot order.
+template <class Rows>
+__device__ __forceinline__ void grad_sums(const Consts &c, const Rows &R, int nb, int with_delta,
+                                          double dx[4], double dy[4], double qmax[4],
+                                          double qmin[4], double &min_delt) {
+    const int me = R.self();
+    const double2 pi_ = R.xy(me);
+    double qi[4];
+    R.qrow(me, qi);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) qmax[m] = qmin[m] = qi[m];
     double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
     double sdxq[4] = {0.0, 0.0, 0.0, 0.0}, sdyq[4] = {0.0, 0.0, 0.0, 0.0};
-    int nb = g.nbhs[i];
+    min_delt = 1.0;
     for (int r = 0; r < nb; ++r) {
-        int k = g.conn[r * g.n + i];
-        R4 kv = ld4w(q + k);
-        double qk[4] = {kv.a, kv.b, kv.c, kv.d};
+        const int k = R.nbr(r);
+        double qk[4];
+        R.qrow(k, qk);
+        const double2 pk = R.xy(k);
+#pragma unroll
+        for (int mm = 0; mm < 4; ++mm) {
+            if (qk[mm] > qmax[mm]) qmax[mm] = qk[mm];
+            if (qk[mm] < qmin[mm]) qmin[mm] = qk[mm];
+        }
+        double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
+        double dist = sqrt(delx * delx + dely * dely);
+        double w = c.power_zero ? 1.0 : pow(dist, c.power);
+        sdx2 = sdx2 + delx * delx * w;
+        sdy2 = sdy2 + dely * dely * w;
+        sdxy = sdxy + delx * dely * w;
+#pragma unroll
+        for (int mm = 0; mm < 4; ++mm) {
+            sdxq[mm] = sdxq[mm] + w * delx * (qk[mm] - qi[mm]);
+            sdyq[mm] = sdyq[mm] + w * dely * (qk[mm] - qi[mm]);
+        }
+        if (with_delta) {
+            double delta_t = dist / R.spdv(k);
+            delta_t = c.cfl * delta_t;
+            if (min_delt > delta_t) min_delt = delta_t;
+        }
+    }
+    double det = sdx2 * sdy2 - sdxy * sdxy;
+    double one_by_det = 1.0 / det;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        dx[m] = (sdxq[m] * sdy2 - sdyq[m] * sdxy) * one_by_det;
+        dy[m] = (sdyq[m] * sdx2 - sdxq[m] * sdxy) * one_by_det;
+    }
+}
+
+// q_variables.F90:115-227 eval_q_inner_loop + eval_update_innerloop over the
+// rows of R, rearranged.  q is fixed within a stage, so the reference's
+// L sum_k w d (qtilde_k - qtilde_i), with qtilde = q - d.dq/2 and L the
+// inverse of the stencil's normal matrix M = sum_k w d d^T, equals
+//     dq0 + dq_i / 2 - L sum_k w d (d . dq_k) / 2,
+// dq0 = L sum_k w d (q_k - q_i) being the D pass's result (kept through the
+// stage's inner iterations) and L M dq_i = dq_i: the same value up to
+// rounding, from the neighbours' dq and (x, y) alone (no q gathers).  dq0x,
+// dq0y: the point's D-pass derivatives; the point's own dq_i and the
+// neighbours' come through R.
+template <class Rows>
+__device__ __forceinline__ void inner_sums(const Consts &c, const Rows &R, int nb,
+                                           const double dq0x[4], const double dq0y[4],
+                                           double dx[4], double dy[4]) {
+    const int me = R.self();
+    const double2 pi_ = R.xy(me);
+    double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
+    double sA[4] = {0.0, 0.0, 0.0, 0.0}, sB[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int r = 0; r < nb; ++r) {
+        const int k = R.nbr(r);
         double dxk[4], dyk[4];
-        ld8w(dq_in + 8 * (size_t)k, dxk, dyk);
-        double2 pk = g.xy[k];
+        R.dqrow(k, dxk, dyk);
+        const double2 pk = R.xy(k);
         double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
         double w = 1.0;
         if (!c.power_zero) w = pow(sqrt(delx * delx + dely * dely), c.power);
         sdx2 = sdx2 + delx * delx * w;
         sdy2 = sdy2 + dely * dely * w;
         sdxy = sdxy + delx * dely * w;
+        const double wx = w * delx, wy = w * dely;
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-            double temp1 = qi[m] - 0.5 * (delx * dxi[m] + dely * dyi[m]);
-            double temp2 = qk[m] - 0.5 * (delx * dxk[m] + dely * dyk[m]);
-            sdxq[m] = sdxq[m] + (w * delx * (temp2 - temp1));
-            sdyq[m] = sdyq[m] + (w * dely * (temp2 - temp1));
+            const double t = delx * dxk[m] + dely * dyk[m];
+            sA[m] = sA[m] + wx * t;
+            sB[m] = sB[m] + wy * t;
         }
     }
+    double dxi[4], dyi[4];
+    R.dqrow(me, dxi, dyi);
     double det = sdx2 * sdy2 - sdxy * sdxy;
     double one_by_det = 1.0 / det;
-    double dx[4], dy[4];
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
-        dx[m] = one_by_det * (sdxq[m] * sdy2 - sdyq[m] * sdxy);
-        dy[m] = one_by_det * (sdyq[m] * sdx2 - sdxq[m] * sdxy);
+        const double Lx = one_by_det * (sA[m] * sdy2 - sB[m] * sdxy);
+        const double Ly = one_by_det * (sB[m] * sdx2 - sA[m] * sdxy);
+        dx[m] = (dq0x[m] + 0.5 * dxi[m]) - 0.5 * Lx;
+        dy[m] = (dq0y[m] + 0.5 * dyi[m]) - 0.5 * Ly;
     }
-    st8(dq_out + 8 * (size_t)i, dx, dy);
 }
 
+// I pass without tile halos: a thread per point with its neighbour rows in
+// 256-bit loads.
 __global__ void __launch_bounds__(GRAD_BLOCK)
-kb_inner(Geom g, Consts c, Sched s, const R4 *__restrict__ q, const double *__restrict__ dq_in,
-         double *__restrict__ dq_out) {
+kb_inner(Geom g, Consts c, Sched s, const double *__restrict__ dq0,
+         const double *__restrict__ dq_in, double *__restrict__ dq_out) {
     __shared__ SchedSmem ss;
     load_sched(s, ss);
     const int total = ss.pre[ss.nact] * TILE;
     for (int vp = blockIdx.x * blockDim.x + threadIdx.x; vp < total;
          vp += gridDim.x * blockDim.x) {
         const int i = sched_point(s, ss, vp);
-        if (i >= 0) inner_point(g, c, q, dq_in, dq_out, i);
+        if (i < 0) continue;
+        double ax[4], ay[4], dx[4], dy[4];
+        ld8w(dq0 + 8 * (size_t)i, ax, ay);
+        inner_sums(c, GlobalRows{g, nullptr, dq_in, nullptr, i}, g.nbhs[i], ax, ay, dx, dy);
+        st8(dq_out + 8 * (size_t)i, dx, dy);
+    }
+}
+
+// 64-byte rows in two 256-bit stores (st.global.v4.f64, sm_100): a warp's
+// store of 32 rows touches each 128-byte line once per store instead of
+// once per 16-byte piece.
+__device__ __forceinline__ void st8w(double *p, const double a[4], const double b[4]) {
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a[0]), "d"(a[1]),
+                 "d"(a[2]), "d"(a[3]) : "memory");
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p + 4), "d"(b[0]), "d"(b[1]),
+                 "d"(b[2]), "d"(b[3]) : "memory");
+}
+
+// Copies the halo rows of a warp's two tiles (hrow ranges [h0, h0 + hn0) and
+// [h1, h1 + hn1), row u of the pair being row u of the first tile's halo or
+// row u - hn0 of the second's) into their shared-memory arrays sm0 / sm1.
+// Consecutive lanes copy consecutive 16-byte pieces of a row array -- the
+// pieces of one row, then those of the next row in the halo's ascending
+// order -- so that runs of neighbouring rows come in whole 128-byte lines.
+// Lane l first loads the row indices of pair rows l, l + 32, l + 64 and
+// l + 96; a copy takes its row index from the lane holding it (a shuffle
+// whose source register is the same for the whole warp).  nA = HA_I copies
+// q, (x, y) and dq; nA = HA_D copies q, (x, y) and, with spd != nullptr, spd.
+// The row indices of a warp's two tiles: lane l holds those of pair rows l,
+// l + 32, l + 64 and l + 96 (row u of the pair being row u of the first
+// tile's halo, hrow[h0 + u], or row u - hn0 of the second's).
+struct HaloIdx {
+    int h0 = 0, hn0 = 0, h1 = 0, hn1 = 0;
+    int kr[2 * HALO_CAP / 32] = {0, 0, 0, 0};
+};
+__device__ __forceinline__ void load_halo_idx(const Geom &g, int lane, HaloIdx &x) {
+    const int hn = x.hn0 + x.hn1;
+#pragma unroll
+    for (int w = 0; w < 2 * HALO_CAP / 32; ++w) {
+        const int u = 32 * w + lane;
+        x.kr[w] = u < hn ? __ldg(g.hrow + (u < x.hn0 ? x.h0 + u : x.h1 + u - x.hn0)) : 0;
+    }
+}
+
+// Copies the halo rows of a warp's two tiles into their shared-memory arrays
+// sm0 / sm1.  Consecutive lanes copy consecutive 16-byte pieces of a row
+// array -- the pieces of one row, then those of the next row in the halo's
+// ascending order -- so that runs of neighbouring rows come in whole
+// 128-byte lines; a copy takes its row index from the lane holding it (a
+// shuffle whose source register is the same for the whole warp).  nA = HA_I
+// copies q, (x, y) and dq; nA = HA_D copies q, (x, y) and, with spd !=
+// nullptr, spd.
+template <int nA>
+__device__ __forceinline__ void stage_halo(const Geom &g, const R4 *q, const double *dq,
+                                           const double *spd, const HaloIdx &x, int lane,
+                                           double2 *sm0, double2 *sm1) {
+    const int hc = g.hc, hn0 = x.hn0, hn = x.hn0 + x.hn1;
+    constexpr int OXY = HaloRows<nA>::OXY, ODQ = HaloRows<nA>::ODQ, OSPD = HaloRows<nA>::OSPD;
+    auto dst = [&](int u) { return u < hn0 ? sm0 + u : sm1 + (u - hn0); };
+    if (nA == HA_D) {
+        // q: two pieces a row (arrays 0 and 1)
+#pragma unroll
+        for (int t = 0; t < 2 * HALO_CAP * 2 / 32; ++t) {
+            if (32 * t >= 2 * hn) break;
+            const int pc = 32 * t + lane, u = pc >> 1, part = pc & 1;
+            const int k = __shfl_sync(0xffffffffu, x.kr[t >> 1], u & 31);
+            if (u < hn)
+                cp_async16(dst(u) + part * hc, reinterpret_cast<const double2 *>(q + k) + part);
+        }
+    }
+    // (x, y): one piece a row
+#pragma unroll
+    for (int t = 0; t < 2 * HALO_CAP / 32; ++t) {
+        if (32 * t >= hn) break;
+        const int u = 32 * t + lane;
+        if (u < hn) cp_async16(dst(u) + OXY * hc, g.xy + x.kr[t]);
+    }
+    if (nA == HA_I) {
+        // dq: four pieces a row
+#pragma unroll
+        for (int t = 0; t < 2 * HALO_CAP * 4 / 32; ++t) {
+            if (32 * t >= 4 * hn) break;
+            const int pc = 32 * t + lane, u = pc >> 2, part = pc & 3;
+            const int k = __shfl_sync(0xffffffffu, x.kr[t >> 2], u & 31);
+            if (u < hn)
+                cp_async16(dst(u) + (ODQ + part) * hc,
+                           reinterpret_cast<const double2 *>(dq + 8 * (size_t)k) + part);
+        }
+    } else if (spd) {
+        // spd: 8 bytes a row (first half of its array)
+#pragma unroll
+        for (int t = 0; t < 2 * HALO_CAP / 32; ++t) {
+            if (32 * t >= hn) break;
+            const int u = 32 * t + lane;
+            if (u < hn) cp_async8(dst(u) + OSPD * hc, spd + x.kr[t]);
+        }
+    }
+}
+
+// The D and I passes with tile halos.  A warp takes chunks of two scheduled
+// tiles (a half-warp's points a tile): it stages both tiles' halo rows into
+// shared memory (every row the tiles read, once, with cp.async), waits, and
+// then computes one point per lane from shared memory.  A tile whose halo
+// was too large to stage (an empty halo range) gathers its rows directly.
+// No block barrier but the schedule load; the
+// lanes of a warp meet at __syncwarp before the rows are read and before
+// they are overwritten.
+struct HaloChunk {
+    HaloIdx x;
+    int i = -1, nb = 0, hn = 0;  // this lane's point, its stencil size, its tile's halo size
+};
+__device__ __forceinline__ void halo_chunk(const Geom &g, const Sched &s, const SchedSmem &ss,
+                                           int ntiles, int ch, int lane, HaloChunk &c) {
+    c = HaloChunk();
+    if (2 * ch >= ntiles) return;
+    const int half = lane / TILE, jl = lane % TILE;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int v = 2 * ch + h;
+        if (v >= ntiles) break;
+        const TileRef t = sched_tile(s, ss, v);
+        const int h0 = __ldg(g.hoff + t.tile), hn = __ldg(g.hoff + t.tile + 1) - h0;
+        if (h == 0) { c.x.h0 = h0; c.x.hn0 = hn; }
+        else { c.x.h1 = h0; c.x.hn1 = hn; }
+        if (h == half) {
+            c.hn = hn;
+            if (t.j0 + jl < t.n) {
+                c.i = t.base + t.j0 + jl;
+                c.nb = __ldg(g.nbhs + c.i);
+            }
+        }
+    }
+    load_halo_idx(g, lane, c.x);
+}
+
+__global__ void __launch_bounds__(HALO_BLOCK, HALO_MIN_BLOCKS_I)
+kb_inner_h(Geom g, Consts c, Sched s, const double *__restrict__ dq0,
+           const double *__restrict__ dq_in, double *__restrict__ dq_out) {
+    extern __shared__ double2 hsm[];
+    __shared__ SchedSmem ss;
+    load_sched(s, ss);
+    const int ntiles = ss.pre[ss.nact];
+    const int wpb = blockDim.x / 32, warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int half = lane / TILE, stride = gridDim.x * wpb;
+    double2 *sm0 = hsm + (size_t)(2 * warp) * HA_I * g.hc, *sm1 = sm0 + HA_I * g.hc;
+    HaloChunk cur;
+    for (int ch = blockIdx.x * wpb + warp; 2 * ch < ntiles; ch += stride) {
+        halo_chunk(g, s, ss, ntiles, ch, lane, cur);
+        stage_halo<HA_I>(g, nullptr, dq_in, nullptr, cur.x, lane, sm0, sm1);
+        const HaloRows<HA_I> hr(g, half ? sm1 : sm0, cur.hn > 0 ? cur.i : -1);
+        double ax[4], ay[4];
+        if (cur.i >= 0) ld8w(dq0 + 8 * (size_t)cur.i, ax, ay);
+        cp_async_wait_all();
+        __syncwarp();
+        if (cur.i >= 0) {
+            double dx[4], dy[4];
+            if (cur.hn > 0) inner_sums(c, hr, cur.nb, ax, ay, dx, dy);
+            else
+                inner_sums(c, GlobalRows{g, nullptr, dq_in, nullptr, cur.i}, cur.nb, ax, ay, dx,
+                           dy);
+            st8w(dq_out + 8 * (size_t)cur.i, dx, dy);
+        }
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(HALO_BLOCK, HALO_MIN_BLOCKS_D)
+kb_grad_h(Geom g, Consts c, Sched s, const R4 *__restrict__ q, const double *__restrict__ spd,
+          double *__restrict__ dq, double *__restrict__ qm, double *__restrict__ delta,
+          int with_delta) {
+    extern __shared__ double2 hsm[];
+    __shared__ SchedSmem ss;
+    load_sched(s, ss);
+    const int ntiles = ss.pre[ss.nact];
+    const int wpb = blockDim.x / 32, warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int half = lane / TILE, stride = gridDim.x * wpb;
+    double2 *sm0 = hsm + (size_t)(2 * warp) * HA_D * g.hc, *sm1 = sm0 + HA_D * g.hc;
+    HaloChunk cur;
+    for (int ch = blockIdx.x * wpb + warp; 2 * ch < ntiles; ch += stride) {
+        halo_chunk(g, s, ss, ntiles, ch, lane, cur);
+        stage_halo<HA_D>(g, q, nullptr, with_delta ? spd : nullptr, cur.x, lane, sm0, sm1);
+        const HaloRows<HA_D> hr(g, half ? sm1 : sm0, cur.hn > 0 ? cur.i : -1);
+        cp_async_wait_all();
+        __syncwarp();
+        if (cur.i >= 0) {
+            double dx[4], dy[4], qmax[4], qmin[4], min_delt;
+            if (cur.hn > 0) grad_sums(c, hr, cur.nb, with_delta, dx, dy, qmax, qmin, min_delt);
+            else
+                grad_sums(c, GlobalRows{g, q, nullptr, spd, cur.i}, cur.nb, with_delta, dx, dy,
+                          qmax, qmin, min_delt);
+            st8w(dq + 8 * (size_t)cur.i, dx, dy);
+            st8w(qm + 8 * (size_t)cur.i, qmax, qmin);
+            if (with_delta) delta[cur.i] = min_delt;
+        }
+        __syncwarp();
     }
 }
 
@@ -775,10 +1102,21 @@ int flux_grid_blocks(int n) { return nblk(nblk(n, TILE), 2 * FLUX_WARPS); }
 
 size_t grad_smem_bytes(int block) { return (size_t)block * STAGE_D * PAIRS_D * sizeof(double2); }
 size_t inner_smem_bytes(int) { return 0; }
+// staging memory of a block of the halo kernels: two tiles a warp
+size_t halo_smem_bytes(int kind, int hc) {
+    return (size_t)(HALO_BLOCK / 32) * 2 * (kind == 0 ? HA_D : HA_I) * hc * sizeof(double2);
+}
 
 cudaError_t init_kernels() {
-    return cudaFuncSetAttribute(kb_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)grad_smem_bytes(GRAD_BLOCK));
+    cudaError_t e = cudaFuncSetAttribute(kb_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)grad_smem_bytes(GRAD_BLOCK));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kb_grad_h, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)halo_smem_bytes(0, HALO_CAP + 1));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kb_inner_h, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)halo_smem_bytes(1, HALO_CAP + 1));
+    return e;
 }
 
 int wave_blocks(int dev, int kind, int block, size_t smem, bool fp32) {
@@ -807,23 +1145,51 @@ int batch_occupancy(int kind, bool fp32, int block, size_t smem) {
     if (fp32) return batch_occupancy32(kind, block, smem);
     int nb = 0;
     cudaError_t e = cudaErrorInvalidValue;
-    if (kind == 0) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_grad, block, smem);
-    else if (kind == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_inner, block, smem);
+    // the D and I passes: their tile-halo kernels (blocks of HALO_BLOCK
+    // threads, the largest staging stride), which every grid with halos runs
+    if (kind == 0)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_grad_h, HALO_BLOCK,
+                                                          halo_smem_bytes(0, HALO_CAP + 1));
+    else if (kind == 1)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_inner_h, HALO_BLOCK,
+                                                          halo_smem_bytes(1, HALO_CAP + 1));
     else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_flux<false>, block, smem);
     return e == cudaSuccess ? nb : 1;
+}
+
+// one wave of resident blocks of a halo kernel (kind 0: D pass, 1: I pass)
+int halo_wave(int kind, int hc) {
+    int dev = 0, sms = 1, nb = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t smem = halo_smem_bytes(kind, hc);
+    cudaError_t e = kind == 0
+        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_grad_h, HALO_BLOCK, smem)
+        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_inner_h, HALO_BLOCK, smem);
+    return std::max(sms, 1) * std::max(1, e == cudaSuccess ? nb : 1);
 }
 
 void launch_grad(const Geom &g, const Consts &c, const Sched &s, const R4 *q, const double *spd,
                  double *dq, double *qm, double *delta, bool with_delta, int block, int grid,
                  cudaStream_t st) {
+    if (g.hoff) {
+        kb_grad_h<<<grid > 0 ? grid : halo_wave(0, g.hc), HALO_BLOCK, halo_smem_bytes(0, g.hc),
+                    st>>>(g, c, s, q, spd, dq, qm, delta, with_delta ? 1 : 0);
+        return;
+    }
     const size_t smem = grad_smem_bytes(block);
     kb_grad<<<wave(0, block, smem, grid), block, smem, st>>>(g, c, s, q, spd, dq, qm, delta,
                                                              with_delta ? 1 : 0);
 }
 
-void launch_inner(const Geom &g, const Consts &c, const Sched &s, const R4 *q,
+void launch_inner(const Geom &g, const Consts &c, const Sched &s, const double *dq0,
                   const double *dq_in, double *dq_out, int block, int grid, cudaStream_t st) {
-    kb_inner<<<wave(1, block, 0, grid), block, 0, st>>>(g, c, s, q, dq_in, dq_out);
+    if (g.hoff) {
+        kb_inner_h<<<grid > 0 ? grid : halo_wave(1, g.hc), HALO_BLOCK, halo_smem_bytes(1, g.hc),
+                     st>>>(g, c, s, dq0, dq_in, dq_out);
+        return;
+    }
+    kb_inner<<<wave(1, block, 0, grid), block, 0, st>>>(g, c, s, dq0, dq_in, dq_out);
 }
 
 void launch_flux(const Geom &g, const Consts &c, const Sched &s, const StageBufs &b, int rk,
