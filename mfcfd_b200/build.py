@@ -15,7 +15,7 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libmfcfd_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in ("primal_fp64.cu", "primal_fp32.cu", "adjoint_fp64.cu", "api.cu", "adjoint_api.cu", "batch_api.cu", "tangent_fp64.cu", "post_fp64.cu", "objective_fp64.cu", "peak_fp64.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in ("primal.h", "lskum_device.cuh", "adjoint.h",
-                                                   "lskum_adjoint.cuh", "handle.h", "batch.cuh", "dual.cuh", "objective.h")] + [
+                                                   "lskum_adjoint.cuh", "handle.h", "batch.cuh", "dual.cuh", "objective.h", "halo.cuh")] + [
     os.path.join(ROOT, "include", "mfcfd_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -769,7 +769,7 @@ static int create_handle(const mfcfd_grid *grid, const mfcfd_params *params, int
     for (int c = 0; c < 4; ++c) h->q_inf[c] = hg.q_inf[c];
 
     // device arrays
-    HostHalo halo;  // FP64 D and I passes
+    HostHalo halo;  // tile halos of the D and I passes
     int st = MFCFD_OK;
     auto up = [&](auto *d, const auto &v) -> int {
         cudaError_t e = cudaMemcpy(d, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice);
@@ -799,7 +799,7 @@ static int create_handle(const mfcfd_grid *grid, const mfcfd_params *params, int
     ALLOC(h->d_nbhs, n);
     ALLOC(h->d_mx, n);
     ALLOC(h->d_my, n);
-    if (!h->fp32) {
+    {
         lskum_host::build_halo(n, kp, hconn.data(), hnb.data(), {{0, nl}}, halo);
         if (halo.hc > 0) {
             ALLOC(h->d_hoff, halo.off.size());

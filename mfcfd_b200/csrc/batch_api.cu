@@ -61,7 +61,7 @@ struct mfcfd_batch {
     double *d_eps2 = nullptr, *d_obc = nullptr;
     int *d_conn = nullptr, *d_nbhs = nullptr;
     unsigned long long *d_mx = nullptr, *d_my = nullptr;
-    int *d_hoff = nullptr, *d_hrow = nullptr;  // tile halos of the FP64 D and I passes
+    int *d_hoff = nullptr, *d_hrow = nullptr;  // tile halos of the D and I passes
     unsigned char *d_hloc = nullptr;
     R4 *d_prim[2] = {nullptr, nullptr}, *d_q[2] = {nullptr, nullptr};
     double *d_dq[3] = {nullptr, nullptr, nullptr};
@@ -528,7 +528,7 @@ int mfcfd_batch_create(int n_inst, const mfcfd_grid *const *grids, const mfcfd_p
         h = HostGrid();
     }
 
-    HostHalo halo;  // FP64 D and I passes
+    HostHalo halo;  // tile halos of the D and I passes
     int st = MFCFD_OK;
     auto up = [&](auto *d, const auto &v) -> int {
         if (v.empty()) return MFCFD_OK;
@@ -561,7 +561,7 @@ int mfcfd_batch_create(int n_inst, const mfcfd_grid *const *grids, const mfcfd_p
     BALLOC(b->d_nbhs, N);
     BALLOC(b->d_mx, N);
     BALLOC(b->d_my, N);
-    if (!b->fp32) {
+    {
         std::vector<std::pair<int, int>> ranges;
         for (int i = 0; i < n_inst; ++i) ranges.emplace_back(b->inst[i].base, info[i].n);
         lskum_host::build_halo(N, kp, conn.data(), nbhs.data(), ranges, halo);

@@ -160,6 +160,29 @@ __device__ __forceinline__ KStateT<T> kstate(T u1, T u2, T rho, T pr, T nx, T ny
     return s;
 }
 
+// erf(x) given exp(-x*x).  FP64: the library erf.  FP32: Abramowitz &
+// Stegun 7.1.26 (after Hastings), erf(|x|) = 1 - t (a1 + t (a2 + t (a3 + t
+// (a4 + t a5)))) exp(-x^2), t = 1 / (1 + p |x|), absolute error below
+// 1.5e-7 -- the split fluxes use erf only in 1 +- erf, so the absolute error
+// is what counts -- reusing the exponential the Maxwellian moments take
+// anyway (C2: FP32 flux pass 0.316 -> 0.304 ms; |dCl| against the FP64
+// loop after 50 iterations 1.0e-7 with the library erff, 6e-9 with this).
+template <class T>
+__device__ __forceinline__ T erf_with_exp(T x, T) {
+    return erf(x);
+}
+template <>
+__device__ __forceinline__ float erf_with_exp<float>(float x, float e) {
+    const float ax = fabsf(x);
+    const float t = 1.0f / (1.0f + 0.3275911f * ax);
+    float p = 1.061405429f;
+    p = p * t - 1.453152027f;
+    p = p * t + 1.421413741f;
+    p = p * t - 0.284496736f;
+    p = p * t + 0.254829592f;
+    return copysignf(1.0f - (p * t) * e, x);
+}
+
 // reconstruct + kstate in one, for the flux passes: the kinetic state of the
 // limited reconstruction towards one neighbour.  beta and p/rho come from
 // qtilde itself (beta = -qtilde_4/2, p/rho = 1/(2 beta)), which the
@@ -205,10 +228,11 @@ __device__ __forceinline__ KStateT<T> reconstruct_kstate(const T q[4], const T d
     s.un = u1 * nx + u2 * ny;
     const T S1 = s.ut * sb, S2 = s.un * sb;
     const T h = temp * sb * inv_sqrt_pi;  // 0.5 / sqrt(pi beta)
-    s.B1 = exp(-S1 * S1) * h;
-    s.B2 = exp(-S2 * S2) * h;
-    s.e1 = erf(S1);
-    s.e2 = erf(S2);
+    const T E1 = exp(-S1 * S1), E2 = exp(-S2 * S2);
+    s.B1 = E1 * h;
+    s.B2 = E2 * h;
+    s.e1 = erf_with_exp(S1, E1);
+    s.e2 = erf_with_exp(S2, E2);
     s.pbr = temp;
     s.usq = s.ut * s.ut + s.un * s.un;
     return s;

@@ -13,7 +13,10 @@
 // residual norm (from the FP64 increment) and the force coefficients.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "batch.cuh"
+#include "halo.cuh"
 #include "primal.h"
 
 namespace lskum {
@@ -215,6 +218,140 @@ kb_inner32(Geom g, Geom32 f, Sched s, const float *__restrict__ dq0,
     }
 }
 
+// The D pass with tile halos (halo.cuh).  The per-slot FP32 offsets come
+// from the staged FP64 (x, y) rows, rounded as the host rounds the offsets
+// it stores ((float)(x_k - x_i)), so the halo and the stored-offset forms
+// see the same offsets.  Row sources: GlobalRows32 reads the stored offsets
+// and the rows from global memory (tiles without a staged halo); HaloRows32
+// reads the staged q (float4), (x, y) and spd.  (The I pass keeps its direct
+// 256-bit gathers of the 32-byte dq rows: a halo I pass staging (x, y) and dq
+// measured slower, 0.057 against 0.050 ms per C2 launch.)
+constexpr int HALO32_BLOCK = 128;
+constexpr int HA32 = 3;  // staged arrays
+#ifndef HALO32_MIN_BLOCKS
+#define HALO32_MIN_BLOCKS 8
+#endif
+
+struct GlobalRows32 {
+    const Geom &g;
+    const Geom32 &f;
+    const float4 *q;
+    const double *spd;
+    int i;
+    __device__ __forceinline__ void begin() {}
+    __device__ __forceinline__ int self() const { return i; }
+    __device__ __forceinline__ int nbr(int r) const { return g.conn[r * g.n + i]; }
+    __device__ __forceinline__ float2 off(int r, int) const { return __ldg(f.dxy + r * g.n + i); }
+    __device__ __forceinline__ float4 qrow(int k) const { return __ldg(q + k); }
+    __device__ __forceinline__ double spdv(int k) const { return spd[k]; }
+};
+
+// staged arrays: q 0, (x, y) 1, spd 2
+struct HaloRows32 {
+    static constexpr int OQ = 0, OXY = 1, OSPD = 2;
+    const double2 *sm;
+    int hc;
+    HaloLoc loc;
+    double2 pi;
+    __device__ __forceinline__ HaloRows32(const Geom &g, const double2 *sm_, int i)
+        : sm(sm_), hc(g.hc), loc(g, i), pi(make_double2(0.0, 0.0)) {}
+    __device__ __forceinline__ void begin() { pi = sm[OXY * hc + loc.own]; }
+    __device__ __forceinline__ int self() const { return loc.own; }
+    __device__ __forceinline__ int nbr(int r) const { return loc.slot(r); }
+    __device__ __forceinline__ float2 off(int, int l) const {
+        const double2 pk = sm[OXY * hc + l];
+        return make_float2((float)(pk.x - pi.x), (float)(pk.y - pi.y));
+    }
+    __device__ __forceinline__ float4 qrow(int l) const {
+        return *reinterpret_cast<const float4 *>(sm + OQ * hc + l);
+    }
+    __device__ __forceinline__ double spdv(int l) const { return sm[OSPD * hc + l].x; }
+};
+
+// grad32_point's sums over the rows of R (the same arithmetic)
+template <class Rows>
+__device__ __forceinline__ void grad32_sums(const Consts &c, const Geom32 &f, int n, Rows R,
+                                            int nb, int with_delta, int i, float dx[4],
+                                            float dy[4], float qmax[4], float qmin[4],
+                                            double &min_delt) {
+    R.begin();
+    const float4 qv = R.qrow(R.self());
+    const float qi[4] = {qv.x, qv.y, qv.z, qv.w};
+#pragma unroll
+    for (int m = 0; m < 4; ++m) qmax[m] = qmin[m] = qi[m];
+    float sx[4] = {0.f, 0.f, 0.f, 0.f}, sy[4] = {0.f, 0.f, 0.f, 0.f};
+    min_delt = 1.0;
+    for (int r = 0; r < nb; ++r) {
+        const int k = R.nbr(r);
+        const float4 kv = R.qrow(k);
+        const float2 gs = R.off(r, k);
+        const float qk[4] = {kv.x, kv.y, kv.z, kv.w};
+        const float w = f.w ? __ldg(f.w + r * n + i) : 1.0f;
+#pragma unroll
+        for (int mm = 0; mm < 4; ++mm) {
+            if (qk[mm] > qmax[mm]) qmax[mm] = qk[mm];
+            if (qk[mm] < qmin[mm]) qmin[mm] = qk[mm];
+        }
+        const float wdx = w * gs.x, wdy = w * gs.y;
+#pragma unroll
+        for (int mm = 0; mm < 4; ++mm) {
+            const float dqm = qk[mm] - qi[mm];
+            sx[mm] = sx[mm] + wdx * dqm;
+            sy[mm] = sy[mm] + wdy * dqm;
+        }
+        if (with_delta) {
+            const double dist = (double)sqrtf(gs.x * gs.x + gs.y * gs.y);
+            double delta_t = dist / R.spdv(k);
+            delta_t = c.cfl * delta_t;
+            if (min_delt > delta_t) min_delt = delta_t;
+        }
+    }
+    const float4 L = __ldg(f.lsq + i);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        dx[m] = L.x * sx[m] + L.y * sy[m];
+        dy[m] = L.y * sx[m] + L.z * sy[m];
+    }
+}
+
+__global__ void __launch_bounds__(HALO32_BLOCK, HALO32_MIN_BLOCKS)
+kb_grad32_h(Geom g, Consts c, Geom32 f, Sched s, const float4 *__restrict__ q,
+            const double *__restrict__ spd, float *__restrict__ dq, float *__restrict__ qm,
+            double *__restrict__ delta, int with_delta) {
+    extern __shared__ double2 hsm[];
+    __shared__ SchedSmem ss;
+    load_sched(s, ss);
+    const int ntiles = ss.pre[ss.nact];
+    const int wpb = blockDim.x / 32, warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int half = lane / TILE, stride = gridDim.x * wpb;
+    using H = HaloRows32;
+    double2 *sm0 = hsm + (size_t)(2 * warp) * HA32 * g.hc, *sm1 = sm0 + HA32 * g.hc;
+    HaloChunk cur;
+    for (int ch = blockIdx.x * wpb + warp; 2 * ch < ntiles; ch += stride) {
+        halo_chunk(g, s, ss, ntiles, ch, lane, cur);
+        stage_array<1>(q, 16, cur.x, lane, sm0, sm1, g.hc, H::OQ);
+        stage_array<1>(g.xy, 16, cur.x, lane, sm0, sm1, g.hc, H::OXY);
+        if (with_delta) stage_array8(spd, cur.x, lane, sm0, sm1, g.hc, H::OSPD);
+        const H hr(g, half ? sm1 : sm0, cur.hn > 0 ? cur.i : -1);
+        halo_wait();
+        __syncwarp();
+        if (cur.i >= 0) {
+            float dx[4], dy[4], qmax[4], qmin[4];
+            double min_delt;
+            if (cur.hn > 0)
+                grad32_sums(c, f, g.n, hr, cur.nb, with_delta, cur.i, dx, dy, qmax, qmin,
+                            min_delt);
+            else
+                grad32_sums(c, f, g.n, GlobalRows32{g, f, q, spd, cur.i}, cur.nb,
+                            with_delta, cur.i, dx, dy, qmax, qmin, min_delt);
+            stf8(dq + 8 * (size_t)cur.i, dx, dy);
+            stf8(qm + 8 * (size_t)cur.i, qmax, qmin);
+            if (with_delta) delta[cur.i] = min_delt;
+        }
+        __syncwarp();
+    }
+}
+
 // Compensated FP32 addition (Kahan): s += v with running correction cmp.
 __device__ __forceinline__ void kahan_add(float &s, float &cmp, float v) {
     float y = __fsub_rn(v, cmp);
@@ -360,10 +497,14 @@ flux32_group(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool v
             cx0 = park[4]; cx1 = park[5]; cy0 = park[6]; cy1 = park[7];
         }
         if (used) {
+            // the list's slots of this round in slot order (lowest bit first):
+            // a lane loops over its own members only
             const unsigned long long lbits = ((L < 2) ? mx : my) >> ((L & 1) ? 32 : 0);
             const int rend = min(nb, r0 + LPP);
-            for (int rr = r0; rr < rend; ++rr) {
-                if (!((lbits >> rr) & 1ull)) continue;
+            unsigned rb = (unsigned)(lbits >> r0) & ((1u << (rend - r0)) - 1u);
+            while (rb) {
+                const int rr = r0 + __ffs(rb) - 1;
+                rb &= rb - 1u;
                 const float *ef = reinterpret_cast<const float *>(rec + (rr - r0) * FREC);
                 const float d0 = ef[4 * L + c0], d1 = ef[4 * L + c0 + 1];
                 const float sw = ef[16], nw = ef[17];
@@ -550,13 +691,32 @@ cudaError_t init_kernels32() {
                                 (int)grad32_smem_bytes(GRAD_BLOCK));
 }
 
+namespace {
+// dynamic shared memory of the halo kernels at staging stride hc
+size_t halo32_smem(int hc) { return halo_bytes(HALO32_BLOCK / 32, HA32, hc); }
+// one wave of resident blocks of a halo kernel (kind 0: D pass, 1: I pass)
+int halo32_wave(int kind, int hc) {
+    int dev = 0, sms = 1, nb = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    (void)kind;
+    cudaError_t e =
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_grad32_h, HALO32_BLOCK, halo32_smem(hc));
+    return std::max(sms, 1) * std::max(1, e == cudaSuccess ? nb : 1);
+}
+}  // namespace
+
 // the flux pass's shared memory is static (independent of the stencil size)
 size_t flux32_smem_bytes(int) { return 0; }
 
 int batch_occupancy32(int kind, int block, size_t smem) {
     int nb = 0;
     cudaError_t e = cudaErrorInvalidValue;
-    if (kind == 0) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_grad32, block, smem);
+    // the D pass: its tile-halo kernel at the largest staging stride, which
+    // every grid with halos runs
+    if (kind == 0)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_grad32_h, HALO32_BLOCK,
+                                                          halo32_smem(HALO_CAP + 1));
     else if (kind == 1)
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_inner32, block, smem);
     else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_flux32, block, smem);
@@ -575,6 +735,11 @@ int wave32(int kind, int block, size_t smem, int grid) {
 void launch_grad32(const Geom &g, const Consts &c, const Geom32 &f, const Sched &s,
                    const float4 *q, const double *spd, float *dq, float *qm, double *delta,
                    bool with_delta, int block, int grid, cudaStream_t st) {
+    if (g.hoff) {
+        kb_grad32_h<<<grid > 0 ? grid : halo32_wave(0, g.hc), HALO32_BLOCK, halo32_smem(g.hc),
+                      st>>>(g, c, f, s, q, spd, dq, qm, delta, with_delta ? 1 : 0);
+        return;
+    }
     const size_t smem = grad32_smem_bytes(block);
     kb_grad32<<<wave32(0, block, smem, grid), block, smem, st>>>(g, c, f, s, q, spd, dq, qm,
                                                                  delta, with_delta ? 1 : 0);

@@ -21,6 +21,7 @@
 #include <algorithm>
 
 #include "batch.cuh"
+#include "halo.cuh"
 #include "primal.h"
 
 namespace lskum {
@@ -234,25 +235,12 @@ struct HaloRows {
     static constexpr int OXY = nA == HA_I ? 0 : 2, ODQ = 1, OSPD = 3;
     const double2 *sm;
     int hc;
-    unsigned long long w0, w1, w2;  // the point's local row bytes (slots, then its own)
-    int own;
+    HaloLoc loc;
     // i < 0: no point (nothing is loaded)
     __device__ __forceinline__ HaloRows(const Geom &g, const double2 *sm_, int i)
-        : sm(sm_), hc(g.hc), w0(0ull), w1(0ull), w2(0ull), own(0) {
-        if (i < 0) return;
-        const unsigned long long *lw =
-            reinterpret_cast<const unsigned long long *>(g.hloc + (size_t)i * g.hkp);
-        w0 = __ldg(lw);
-        if (g.hkp > 8) w1 = __ldg(lw + 1);
-        if (g.hkp > 16) w2 = __ldg(lw + 2);
-        const unsigned long long last = g.hkp > 16 ? w2 : (g.hkp > 8 ? w1 : w0);
-        own = (int)(last >> 56);
-    }
-    __device__ __forceinline__ int self() const { return own; }
-    __device__ __forceinline__ int nbr(int r) const {
-        const unsigned long long w = r < 8 ? w0 : (r < 16 ? w1 : w2);
-        return (int)((w >> (8 * (r & 7))) & 0xffull);
-    }
+        : sm(sm_), hc(g.hc), loc(g, i) {}
+    __device__ __forceinline__ int self() const { return loc.own; }
+    __device__ __forceinline__ int nbr(int r) const { return loc.slot(r); }
     __device__ __forceinline__ double2 xy(int l) const { return sm[OXY * hc + l]; }
     __device__ __forceinline__ void qrow(int l, double v[4]) const {
         const double2 a = sm[l], b = sm[hc + l];
@@ -407,113 +395,24 @@ __device__ __forceinline__ void st8w(double *p, const double a[4], const double 
 // l + 96; a copy takes its row index from the lane holding it (a shuffle
 // whose source register is the same for the whole warp).  nA = HA_I copies
 // q, (x, y) and dq; nA = HA_D copies q, (x, y) and, with spd != nullptr, spd.
-// The row indices of a warp's two tiles: lane l holds those of pair rows l,
-// l + 32, l + 64 and l + 96 (row u of the pair being row u of the first
-// tile's halo, hrow[h0 + u], or row u - hn0 of the second's).
-struct HaloIdx {
-    int h0 = 0, hn0 = 0, h1 = 0, hn1 = 0;
-    int kr[2 * HALO_CAP / 32] = {0, 0, 0, 0};
-};
-__device__ __forceinline__ void load_halo_idx(const Geom &g, int lane, HaloIdx &x) {
-    const int hn = x.hn0 + x.hn1;
-#pragma unroll
-    for (int w = 0; w < 2 * HALO_CAP / 32; ++w) {
-        const int u = 32 * w + lane;
-        x.kr[w] = u < hn ? __ldg(g.hrow + (u < x.hn0 ? x.h0 + u : x.h1 + u - x.hn0)) : 0;
-    }
-}
-
-// Copies the halo rows of a warp's two tiles into their shared-memory arrays
-// sm0 / sm1.  Consecutive lanes copy consecutive 16-byte pieces of a row
-// array -- the pieces of one row, then those of the next row in the halo's
-// ascending order -- so that runs of neighbouring rows come in whole
-// 128-byte lines; a copy takes its row index from the lane holding it (a
-// shuffle whose source register is the same for the whole warp).  nA = HA_I
-// copies q, (x, y) and dq; nA = HA_D copies q, (x, y) and, with spd !=
-// nullptr, spd.
+// Stages a chunk's halo rows: the D pass q (two pieces a row), (x, y) and,
+// with spd != nullptr, spd; the I pass (x, y) and dq (four pieces a row).
 template <int nA>
 __device__ __forceinline__ void stage_halo(const Geom &g, const R4 *q, const double *dq,
                                            const double *spd, const HaloIdx &x, int lane,
                                            double2 *sm0, double2 *sm1) {
-    const int hc = g.hc, hn0 = x.hn0, hn = x.hn0 + x.hn1;
-    constexpr int OXY = HaloRows<nA>::OXY, ODQ = HaloRows<nA>::ODQ, OSPD = HaloRows<nA>::OSPD;
-    auto dst = [&](int u) { return u < hn0 ? sm0 + u : sm1 + (u - hn0); };
-    if (nA == HA_D) {
-        // q: two pieces a row (arrays 0 and 1)
-#pragma unroll
-        for (int t = 0; t < 2 * HALO_CAP * 2 / 32; ++t) {
-            if (32 * t >= 2 * hn) break;
-            const int pc = 32 * t + lane, u = pc >> 1, part = pc & 1;
-            const int k = __shfl_sync(0xffffffffu, x.kr[t >> 1], u & 31);
-            if (u < hn)
-                cp_async16(dst(u) + part * hc, reinterpret_cast<const double2 *>(q + k) + part);
-        }
-    }
-    // (x, y): one piece a row
-#pragma unroll
-    for (int t = 0; t < 2 * HALO_CAP / 32; ++t) {
-        if (32 * t >= hn) break;
-        const int u = 32 * t + lane;
-        if (u < hn) cp_async16(dst(u) + OXY * hc, g.xy + x.kr[t]);
-    }
-    if (nA == HA_I) {
-        // dq: four pieces a row
-#pragma unroll
-        for (int t = 0; t < 2 * HALO_CAP * 4 / 32; ++t) {
-            if (32 * t >= 4 * hn) break;
-            const int pc = 32 * t + lane, u = pc >> 2, part = pc & 3;
-            const int k = __shfl_sync(0xffffffffu, x.kr[t >> 2], u & 31);
-            if (u < hn)
-                cp_async16(dst(u) + (ODQ + part) * hc,
-                           reinterpret_cast<const double2 *>(dq + 8 * (size_t)k) + part);
-        }
-    } else if (spd) {
-        // spd: 8 bytes a row (first half of its array)
-#pragma unroll
-        for (int t = 0; t < 2 * HALO_CAP / 32; ++t) {
-            if (32 * t >= hn) break;
-            const int u = 32 * t + lane;
-            if (u < hn) cp_async8(dst(u) + OSPD * hc, spd + x.kr[t]);
-        }
-    }
+    using H = HaloRows<nA>;
+    if (nA == HA_D) stage_array<2>(q, 32, x, lane, sm0, sm1, g.hc, 0);
+    stage_array<1>(g.xy, 16, x, lane, sm0, sm1, g.hc, H::OXY);
+    if (nA == HA_I) stage_array<4>(dq, 64, x, lane, sm0, sm1, g.hc, H::ODQ);
+    else if (spd) stage_array8(spd, x, lane, sm0, sm1, g.hc, H::OSPD);
 }
 
-// The D and I passes with tile halos.  A warp takes chunks of two scheduled
-// tiles (a half-warp's points a tile): it stages both tiles' halo rows into
-// shared memory (every row the tiles read, once, with cp.async), waits, and
-// then computes one point per lane from shared memory.  A tile whose halo
-// was too large to stage (an empty halo range) gathers its rows directly.
-// No block barrier but the schedule load; the
-// lanes of a warp meet at __syncwarp before the rows are read and before
-// they are overwritten.
-struct HaloChunk {
-    HaloIdx x;
-    int i = -1, nb = 0, hn = 0;  // this lane's point, its stencil size, its tile's halo size
-};
-__device__ __forceinline__ void halo_chunk(const Geom &g, const Sched &s, const SchedSmem &ss,
-                                           int ntiles, int ch, int lane, HaloChunk &c) {
-    c = HaloChunk();
-    if (2 * ch >= ntiles) return;
-    const int half = lane / TILE, jl = lane % TILE;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int v = 2 * ch + h;
-        if (v >= ntiles) break;
-        const TileRef t = sched_tile(s, ss, v);
-        const int h0 = __ldg(g.hoff + t.tile), hn = __ldg(g.hoff + t.tile + 1) - h0;
-        if (h == 0) { c.x.h0 = h0; c.x.hn0 = hn; }
-        else { c.x.h1 = h0; c.x.hn1 = hn; }
-        if (h == half) {
-            c.hn = hn;
-            if (t.j0 + jl < t.n) {
-                c.i = t.base + t.j0 + jl;
-                c.nb = __ldg(g.nbhs + c.i);
-            }
-        }
-    }
-    load_halo_idx(g, lane, c.x);
-}
-
+// The D and I passes with tile halos (halo.cuh): a warp stages two tiles'
+// halo rows, waits, and computes one point per lane from shared memory; a
+// tile whose halo was too large to stage reads its rows directly.  No block
+// barrier but the schedule load; the lanes of a warp meet at __syncwarp
+// before the rows are read and before they are overwritten.
 __global__ void __launch_bounds__(HALO_BLOCK, HALO_MIN_BLOCKS_I)
 kb_inner_h(Geom g, Consts c, Sched s, const double *__restrict__ dq0,
            const double *__restrict__ dq_in, double *__restrict__ dq_out) {
@@ -531,7 +430,7 @@ kb_inner_h(Geom g, Consts c, Sched s, const double *__restrict__ dq0,
         const HaloRows<HA_I> hr(g, half ? sm1 : sm0, cur.hn > 0 ? cur.i : -1);
         double ax[4], ay[4];
         if (cur.i >= 0) ld8w(dq0 + 8 * (size_t)cur.i, ax, ay);
-        cp_async_wait_all();
+        halo_wait();
         __syncwarp();
         if (cur.i >= 0) {
             double dx[4], dy[4];
@@ -561,7 +460,7 @@ kb_grad_h(Geom g, Consts c, Sched s, const R4 *__restrict__ q, const double *__r
         halo_chunk(g, s, ss, ntiles, ch, lane, cur);
         stage_halo<HA_D>(g, q, nullptr, with_delta ? spd : nullptr, cur.x, lane, sm0, sm1);
         const HaloRows<HA_D> hr(g, half ? sm1 : sm0, cur.hn > 0 ? cur.i : -1);
-        cp_async_wait_all();
+        halo_wait();
         __syncwarp();
         if (cur.i >= 0) {
             double dx[4], dy[4], qmax[4], qmin[4], min_delt;
@@ -734,10 +633,14 @@ flux_group(const Geom &g, const Consts &c, const StageBufs &b, int i, bool valid
         }
         // list sums of this round's slots, in slot order
         if (used) {
+            // the list's slots of this round in slot order (lowest bit first):
+            // a lane loops over its own members only
             const unsigned long long lbits = ((L < 2) ? mx : my) >> ((L & 1) ? 32 : 0);
             const int rend = min(nb, r0 + LPP);
-            for (int rr = r0; rr < rend; ++rr) {
-                if (!((lbits >> rr) & 1ull)) continue;
+            unsigned rb = (unsigned)(lbits >> r0) & ((1u << (rend - r0)) - 1u);
+            while (rb) {
+                const int rr = r0 + __ffs(rb) - 1;
+                rb &= rb - 1u;
                 const double *e = rec + (rr - r0) * REC;
                 double dels = e[16], deln = e[17], w = e[18];
                 double dels_w = dels * w, deln_w = deln * w;
@@ -1104,7 +1007,7 @@ size_t grad_smem_bytes(int block) { return (size_t)block * STAGE_D * PAIRS_D * s
 size_t inner_smem_bytes(int) { return 0; }
 // staging memory of a block of the halo kernels: two tiles a warp
 size_t halo_smem_bytes(int kind, int hc) {
-    return (size_t)(HALO_BLOCK / 32) * 2 * (kind == 0 ? HA_D : HA_I) * hc * sizeof(double2);
+    return halo_bytes(HALO_BLOCK / 32, kind == 0 ? HA_D : HA_I, hc);
 }
 
 cudaError_t init_kernels() {
