@@ -500,8 +500,9 @@ flux32_group(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool v
             // the list's slots of this round in slot order (lowest bit first):
             // a lane loops over its own members only
             const unsigned long long lbits = ((L < 2) ? mx : my) >> ((L & 1) ? 32 : 0);
-            const int rend = min(nb, r0 + LPP);
-            unsigned rb = (unsigned)(lbits >> r0) & ((1u << (rend - r0)) - 1u);
+            // (a point with fewer slots than r0 has none in this round)
+            const int cnt = min(nb, r0 + LPP) - r0;
+            unsigned rb = cnt > 0 ? (unsigned)(lbits >> r0) & ((1u << cnt) - 1u) : 0u;
             while (rb) {
                 const int rr = r0 + __ffs(rb) - 1;
                 rb &= rb - 1u;
