@@ -225,7 +225,8 @@ kb_inner32(Geom g, Geom32 f, Sched s, const float *__restrict__ dq0,
 // and the rows from global memory (tiles without a staged halo); HaloRows32
 // reads the staged q (float4), (x, y) and spd.  (The I pass keeps its direct
 // 256-bit gathers of the 32-byte dq rows: a halo I pass staging (x, y) and dq
-// measured slower, 0.057 against 0.050 ms per C2 launch.)
+// measured slower, 0.057 against 0.050 ms per C2 launch, and so did one
+// staging only (x, y) and the row indices, 0.064 ms.)
 constexpr int HALO32_BLOCK = 128;
 constexpr int HA32 = 3;  // staged arrays
 #ifndef HALO32_MIN_BLOCKS
@@ -700,7 +701,7 @@ int halo32_wave(int kind, int hc) {
     int dev = 0, sms = 1, nb = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    (void)kind;
+    (void)kind;  // the D pass only
     cudaError_t e =
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_grad32_h, HALO32_BLOCK, halo32_smem(hc));
     return std::max(sms, 1) * std::max(1, e == cudaSuccess ? nb : 1);
