@@ -26,7 +26,7 @@ namespace {
 constexpr int GRAD_BLOCK = 256;
 constexpr int LPP = 8;
 constexpr int FLUX_BLOCK = 128;  // four independent warps
-constexpr int FREC = 9;   // dGxp..dGyn as 16 floats, then dels*w, deln*w (18 floats)
+constexpr int FREC = 10;  // dGxp..dGyn as 16 floats, then each list's slot weight c_L (20 floats)
 #ifndef FLUX32_MIN_BLOCKS
 #define FLUX32_MIN_BLOCKS 7  // <= 72 registers (8 blocks: 64 registers with spills, 0.370 against 0.364 ms on C2)
 #endif
@@ -443,13 +443,12 @@ flux32_group(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool v
     const int L = lane >> 1, c0 = (lane & 1) * 2;
     const bool used =
         valid && !((kind == KIND_WALL && L == 2) || (kind == KIND_OUTER && L == 3));
-    float fx0 = 0.f, fx1 = 0.f, fy0 = 0.f, fy1 = 0.f;
-    float cx0 = 0.f, cx1 = 0.f, cy0 = 0.f, cy1 = 0.f;
+    // Kahan sums of the lane's two list components and their corrections
+    float fx0 = 0.f, fx1 = 0.f, cx0 = 0.f, cx1 = 0.f;
     float *park = reinterpret_cast<float *>(rec + LPP * FREC) + 8 * lane;
     for (int r0 = 0; r0 < nbw; r0 += LPP) {
         if (r0 > 0) {
-            park[0] = fx0; park[1] = fx1; park[2] = fy0; park[3] = fy1;
-            park[4] = cx0; park[5] = cx1; park[6] = cy0; park[7] = cy1;
+            park[0] = fx0; park[1] = fx1; park[2] = cx0; park[3] = cx1;
         }
         const int r = r0 + lane;
         if (r < nb) {
@@ -489,13 +488,22 @@ flux32_group(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool v
                     for (int m = 0; m < 4; ++m) ef[4 * Lx + m] = (float)(Gk[m] - Gi[m]);
                 }
             }
-            ef[16] = dels * w;
-            ef[17] = deln * w;
+            {
+                // the list solves folded into the slot: list L's derivative is
+                // sum_slots d * c_L with c_L = a_L dels w + b_L deln w (x lists)
+                // or a_L deln w + b_L dels w (y lists)
+                const float sw = dels * w, nw = deln * w;
+                const float4 cx = __ldg(b.f.flsq + 2 * (size_t)i);
+                const float4 cy = __ldg(b.f.flsq + 2 * (size_t)i + 1);
+                ef[16] = cx.x * sw + cx.y * nw;
+                ef[17] = cx.z * sw + cx.w * nw;
+                ef[18] = cy.x * nw + cy.y * sw;
+                ef[19] = cy.z * nw + cy.w * sw;
+            }
         }
         __syncwarp();
         if (r0 > 0) {
-            fx0 = park[0]; fx1 = park[1]; fy0 = park[2]; fy1 = park[3];
-            cx0 = park[4]; cx1 = park[5]; cy0 = park[6]; cy1 = park[7];
+            fx0 = park[0]; fx1 = park[1]; cx0 = park[2]; cx1 = park[3];
         }
         if (used) {
             // the list's slots of this round in slot order (lowest bit first):
@@ -509,29 +517,17 @@ flux32_group(const Geom &g, const Consts &c, const StageBufs32 &b, int i, bool v
                 rb &= rb - 1u;
                 const float *ef = reinterpret_cast<const float *>(rec + (rr - r0) * FREC);
                 const float d0 = ef[4 * L + c0], d1 = ef[4 * L + c0 + 1];
-                const float sw = ef[16], nw = ef[17];
-                kahan_add(fx0, cx0, d0 * sw);
-                kahan_add(fy0, cy0, d0 * nw);
-                kahan_add(fx1, cx1, d1 * sw);
-                kahan_add(fy1, cy1, d1 * nw);
+                const float cl = ef[16 + L];
+                kahan_add(fx0, cx0, d0 * cl);
+                kahan_add(fx1, cx1, d1 * cl);
             }
         }
         __syncwarp();  // the next round overwrites the records
     }
     double Gv0 = 0.0, Gv1 = 0.0;
     if (used) {
-        // the list's precomputed solve: x lists a Sx + b Sy, y lists a Sy + b Sx
-        const float4 co = __ldg(b.f.flsq + 2 * (size_t)i + (L >> 1));
-        const double a = (L & 1) ? co.z : co.x, bb = (L & 1) ? co.w : co.y;
-        const double X0 = (double)fx0 - cx0, X1 = (double)fx1 - cx1;
-        const double Y0 = (double)fy0 - cy0, Y1 = (double)fy1 - cy1;
-        if (L < 2) {
-            Gv0 = a * X0 + bb * Y0;
-            Gv1 = a * X1 + bb * Y1;
-        } else {
-            Gv0 = a * Y0 + bb * X0;
-            Gv1 = a * Y1 + bb * X1;
-        }
+        Gv0 = (double)fx0 - cx0;
+        Gv1 = (double)fx1 - cx1;
     }
     // lane 2L+h holds G[L][2h], G[L][2h+1]
     Gout[2 * lane] = Gv0;
