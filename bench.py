@@ -66,12 +66,14 @@ def workload_config(name: str, grid, flow: dict) -> dict:
 
 def algorithmic_bytes(kbar: float, m: int, rks: int = 4) -> dict:
     """Minimal dataflow bytes per point: each pass reads and writes every
-    array it touches once (split lists derive from conn)."""
+    array it touches once (split lists derive from conn).  The I pass in its
+    rearranged form reads the D pass's dq0 (64 B) in place of q (32 B)."""
     t = 92 + 4 * kbar
     d = 180 + 4 * kbar
+    i = 212 + 4 * kbar
     f = 280 + 4 * kbar
-    return {"flux_pass": f, "grad_pass": d, "inner_pass": d, "step_pass": t,
-            "iteration": t + rks * ((1 + m) * d + f)}
+    return {"flux_pass": f, "grad_pass": d, "inner_pass": i, "step_pass": t,
+            "iteration": t + rks * (d + m * i + f)}
 
 
 def measured_peaks() -> dict:
@@ -593,7 +595,7 @@ def main():
     roofline.update({
         "kernel": "kb_flux (flux residual + state update, one SSPRK stage)",
         "fp64_pipe_active_frac": _profile_value("fp64_pipe_active_frac"),
-        "note": ("kb_flux is bound by FP64 issue (exp/erf/log/div chains), not by HBM: "
+        "note": ("kb_flux is bound by FP64 latency (exp/erf/div chains), not by HBM: "
                  "achieved/peak is its FP64 work rate against the measured FMA peak; "
                  "the hbm object gives its algorithmic bytes against the copy peak")})
     iter_bytes = ab["iteration"] * grid.n
