@@ -809,19 +809,38 @@ kb_flux(Geom g, Consts c, Sched s, StageBufs b, int rk, int last) {
 #undef FLUX_TILE
 }
 
-// fpi_solver.F90:57-70: res_new = sqrt(sum res_sqr)/plen and the residue.
-// Partials are summed in a fixed order (deterministic).
-// Whole block of 1024 threads; the residue is returned on thread 0.
-__device__ __forceinline__ double residual_block(const double *__restrict__ part, int nparts,
-                                                 Ctl *ctl, double *hist, double *s) {
-    double acc = 0.0;
-    for (int t = threadIdx.x; t < nparts; t += blockDim.x) acc = acc + part[t];
-    s[threadIdx.x] = acc;
+// Sum of nparts tile partials in a fixed order (deterministic, independent
+// of the launch shape of the passes that wrote them): thread t of a block of
+// 1024 keeps eight accumulators over partials t + 1024 j (j mod 8 picks the
+// accumulator, so the loads of one thread are independent), adds them
+// pairwise, and a tree over the block adds the threads.  The result is in
+// s[0] for every thread.
+__device__ __forceinline__ void sum_parts_block(const double *__restrict__ part, int nparts,
+                                                double *s) {
+    constexpr int U = 8;
+    const int T = blockDim.x;
+    double acc[U] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    int t = threadIdx.x;
+    for (; t + (U - 1) * T < nparts; t += U * T) {
+#pragma unroll
+        for (int j = 0; j < U; ++j) acc[j] = acc[j] + __ldg(part + t + j * T);
+    }
+#pragma unroll
+    for (int j = 0; j < U; ++j)
+        if (t + j * T < nparts) acc[j] = acc[j] + __ldg(part + t + j * T);
+    s[threadIdx.x] = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
     __syncthreads();
     for (int w = blockDim.x / 2; w > 0; w >>= 1) {
         if (threadIdx.x < w) s[threadIdx.x] = s[threadIdx.x] + s[threadIdx.x + w];
         __syncthreads();
     }
+}
+
+// fpi_solver.F90:57-70: res_new = sqrt(sum res_sqr)/plen and the residue.
+// Whole block of 1024 threads; the residue is returned on thread 0.
+__device__ __forceinline__ double residual_block(const double *__restrict__ part, int nparts,
+                                                 Ctl *ctl, double *hist, double *s) {
+    sum_parts_block(part, nparts, s);
     if (threadIdx.x == 0) {
         double res_new = sqrt(s[0]) / ctl->plen;
         int it = ctl->it;
@@ -847,14 +866,7 @@ __device__ __forceinline__ double residual_block(const double *__restrict__ part
 __global__ void __launch_bounds__(1024)
 k_sum_parts(const double *__restrict__ part, int nparts, double *out) {
     __shared__ double s[1024];
-    double acc = 0.0;
-    for (int t = threadIdx.x; t < nparts; t += blockDim.x) acc = acc + part[t];
-    s[threadIdx.x] = acc;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) s[threadIdx.x] = s[threadIdx.x] + s[threadIdx.x + w];
-        __syncthreads();
-    }
+    sum_parts_block(part, nparts, s);
     if (threadIdx.x == 0) *out = s[0];
 }
 
