@@ -803,11 +803,9 @@ static int create_handle(const mfcfd_grid *grid, const mfcfd_params *params, int
     ALLOC(h->d_my, n);
     {
         lskum_host::build_halo(n, kp, hconn.data(), hnb.data(), {{0, nl}}, halo);
-        if (halo.hc > 0) {
-            ALLOC(h->d_hoff, halo.off.size());
-            ALLOC(h->d_hrow, halo.rows.size());
-            ALLOC(h->d_hloc, halo.loc.size());
-        }
+        ALLOC(h->d_hoff, halo.off.size());
+        ALLOC(h->d_hrow, halo.rows.size());
+        ALLOC(h->d_hloc, halo.loc.size());
     }
     if (!h->fp32) {
         for (int b = 0; b < 2; ++b) {

@@ -565,11 +565,9 @@ int mfcfd_batch_create(int n_inst, const mfcfd_grid *const *grids, const mfcfd_p
         std::vector<std::pair<int, int>> ranges;
         for (int i = 0; i < n_inst; ++i) ranges.emplace_back(b->inst[i].base, info[i].n);
         lskum_host::build_halo(N, kp, conn.data(), nbhs.data(), ranges, halo);
-        if (halo.hc > 0) {
-            BALLOC(b->d_hoff, halo.off.size());
-            BALLOC(b->d_hrow, halo.rows.size());
-            BALLOC(b->d_hloc, halo.loc.size());
-        }
+        BALLOC(b->d_hoff, halo.off.size());
+        BALLOC(b->d_hrow, halo.rows.size());
+        BALLOC(b->d_hloc, halo.loc.size());
     }
     if (!b->fp32) {
         for (int k = 0; k < 2; ++k) {

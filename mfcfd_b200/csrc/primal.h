@@ -131,17 +131,11 @@ int flux_grid_blocks(int n);
 // the FP32-mixed kernels)
 int batch_occupancy(int kind, bool fp32, int block, size_t smem);
 int batch_occupancy32(int kind, int block, size_t smem);
-// dynamic shared memory of the D and I passes (their staging buffers) for
-// blocks of `block` threads
-size_t grad_smem_bytes(int block);
-size_t inner_smem_bytes(int block);
-size_t grad32_smem_bytes(int block);
-size_t inner32_smem_bytes(int block);
 // dynamic shared memory of the flux passes for stencils of kp slots
 size_t flux_smem_bytes(int kp);
 size_t flux32_smem_bytes(int kp);
 // blocks of one wave of resident blocks of a pass on device dev (for the
-// point passes the staging memory of `block` replaces `smem`)
+// point passes their own staging memory replaces `smem`)
 int wave_blocks(int dev, int kind, int block, size_t smem, bool fp32);
 // threads per block of the point passes (their staging buffers take up to
 // 512 B of shared memory a thread)

@@ -33,13 +33,6 @@ constexpr int FREC = 10;  // dGxp..dGyn as 16 floats, then each list's slot weig
 constexpr double OBT = 1.0 / 3.0;
 constexpr double TBT = 2.0 / 3.0;
 
-__device__ __forceinline__ void ldf8(const float *p, float a[4], float b[4]) {
-    const float4 *v = reinterpret_cast<const float4 *>(p);
-    float4 x = __ldg(v), y = __ldg(v + 1);
-    a[0] = x.x; a[1] = x.y; a[2] = x.z; a[3] = x.w;
-    b[0] = y.x; b[1] = y.y; b[2] = y.z; b[3] = y.w;
-}
-
 // A 32-byte row (dq or qm of one point) in one 256-bit read-only load
 // (ld.global.nc.v8.f32, sm_100); the rows are 32-byte aligned.
 __device__ __forceinline__ void ldf8w(const float *p, float a[4], float b[4]) {
@@ -49,120 +42,12 @@ __device__ __forceinline__ void ldf8w(const float *p, float a[4], float b[4]) {
         : "l"(p));
 }
 
-__device__ __forceinline__ void stf8(float *p, const float a[4], const float b[4]) {
-    float4 *v = reinterpret_cast<float4 *>(p);
-    v[0] = make_float4(a[0], a[1], a[2], a[3]);
-    v[1] = make_float4(b[0], b[1], b[2], b[3]);
-}
-
-// Staged neighbour gathers of the D pass, as in the FP64 D pass: a thread copies
-// the rows of a round of stencil slots into its own shared-memory slots with
-// cp.async (no registers held while the copies fly), waits once, and sums in
-// slot order from shared memory.  16-byte units, thread-minor
-// (sb[unit * blockDim + thread]).  D pass units: the neighbour's q row, then
-// (slot offset dx dy, neighbour spd).  (The I pass gathers one 32-byte dq
-// row per slot in a 256-bit load; staging it was measured slower.)
-#ifndef STAGE32
-#define STAGE32 8    // slots per round, D pass
-#endif
-constexpr int UNITS32_D = 2;
-
-__device__ __forceinline__ void cp16(void *dst, const void *src) {
-    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp8(void *dst, const void *src) {
-    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_wait_all() {
-    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-}
-
-// eval_q_derivatives (q_variables.F90:41-112) with FP32 sums and the
-// precomputed inverse normal matrix, and func_delta (state_update.F90:190-236)
-// with each neighbour's distance from the slot's FP32 offset (FP32 geometry,
-// read anyway) and the division and minimum in FP64.
-__device__ __forceinline__ void
-grad32_point(const Geom &g, const Consts &c, const Geom32 &f, const float4 *__restrict__ q,
-             const double *__restrict__ spd, float *__restrict__ dq, float *__restrict__ qm,
-             double *__restrict__ delta, int with_delta, int i, float4 *sb) {
-    const int T = blockDim.x;
-    const float4 qv = __ldg(q + i);
-    const float qi[4] = {qv.x, qv.y, qv.z, qv.w};
-    float qmax[4] = {qi[0], qi[1], qi[2], qi[3]};
-    float qmin[4] = {qi[0], qi[1], qi[2], qi[3]};
-    float sx[4] = {0.f, 0.f, 0.f, 0.f}, sy[4] = {0.f, 0.f, 0.f, 0.f};
-    double min_delt = 1.0;
-    const int nb = g.nbhs[i];
-    for (int r0 = 0; r0 < nb; r0 += STAGE32) {
-        const int m = min(STAGE32, nb - r0);
-        int kk[STAGE32];
-#pragma unroll
-        for (int t = 0; t < STAGE32; ++t) kk[t] = t < m ? __ldg(g.conn + (r0 + t) * g.n + i) : 0;
-#pragma unroll
-        for (int t = 0; t < STAGE32; ++t) {
-            if (t < m) {
-                float4 *d = sb + t * UNITS32_D * T;
-                cp16(d, q + kk[t]);
-                cp8(d + T, f.dxy + (r0 + t) * g.n + i);
-                if (with_delta) cp8(reinterpret_cast<char *>(d + T) + 8, spd + kk[t]);
-            }
-        }
-        cp_wait_all();
-        for (int t = 0; t < m; ++t) {
-            const float4 *d = sb + t * UNITS32_D * T;
-            const float4 kv = d[0], gs = d[T];
-            const float qk[4] = {kv.x, kv.y, kv.z, kv.w};
-            const int r = r0 + t;
-            const float w = f.w ? __ldg(f.w + r * g.n + i) : 1.0f;
-#pragma unroll
-            for (int mm = 0; mm < 4; ++mm) {
-                if (qk[mm] > qmax[mm]) qmax[mm] = qk[mm];
-                if (qk[mm] < qmin[mm]) qmin[mm] = qk[mm];
-            }
-            const float wdx = w * gs.x, wdy = w * gs.y;
-#pragma unroll
-            for (int mm = 0; mm < 4; ++mm) {
-                const float dqm = qk[mm] - qi[mm];
-                sx[mm] = sx[mm] + wdx * dqm;
-                sy[mm] = sy[mm] + wdy * dqm;
-            }
-            if (with_delta) {
-                const double sk = __hiloint2double(__float_as_int(gs.w), __float_as_int(gs.z));
-                const double dist = (double)sqrtf(gs.x * gs.x + gs.y * gs.y);
-                double delta_t = dist / sk;
-                delta_t = c.cfl * delta_t;
-                if (min_delt > delta_t) min_delt = delta_t;
-            }
-        }
-    }
-    const float4 L = __ldg(f.lsq + i);
-    float dx[4], dy[4];
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-        dx[m] = L.x * sx[m] + L.y * sy[m];
-        dy[m] = L.y * sx[m] + L.z * sy[m];
-    }
-    stf8(dq + 8 * (size_t)i, dx, dy);
-    stf8(qm + 8 * (size_t)i, qmax, qmin);
-    if (with_delta) delta[i] = min_delt;
-}
-
-__global__ void __launch_bounds__(GRAD_BLOCK)
-kb_grad32(Geom g, Consts c, Geom32 f, Sched s, const float4 *__restrict__ q,
-          const double *__restrict__ spd, float *__restrict__ dq, float *__restrict__ qm,
-          double *__restrict__ delta, int with_delta) {
-    extern __shared__ float4 sbd32[];
-    __shared__ SchedSmem ss;
-    load_sched(s, ss);
-    const int total = ss.pre[ss.nact] * TILE;
-    for (int vp = blockIdx.x * blockDim.x + threadIdx.x; vp < total;
-         vp += gridDim.x * blockDim.x) {
-        const int i = sched_point(s, ss, vp);
-        if (i >= 0)
-            grad32_point(g, c, f, q, spd, dq, qm, delta, with_delta, i, sbd32 + threadIdx.x);
-    }
+// A 32-byte row in one 256-bit store (st.global.v8.f32, sm_100).
+__device__ __forceinline__ void stf8w(float *p, const float a[4], const float b[4]) {
+    asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p),
+                 "f"(a[0]), "f"(a[1]), "f"(a[2]), "f"(a[3]), "f"(b[0]), "f"(b[1]), "f"(b[2]),
+                 "f"(b[3])
+                 : "memory");
 }
 
 // eval_q_inner_loop + eval_update_innerloop (q_variables.F90:115-227) with
@@ -193,8 +78,8 @@ inner32_point(const Geom &g, const Geom32 &f, const float *__restrict__ dq0,
         }
     }
     float dxi[4], dyi[4], dx0[4], dy0[4];
-    ldf8(dq_in + 8 * (size_t)i, dxi, dyi);
-    ldf8(dq0 + 8 * (size_t)i, dx0, dy0);
+    ldf8w(dq_in + 8 * (size_t)i, dxi, dyi);
+    ldf8w(dq0 + 8 * (size_t)i, dx0, dy0);
     const float4 L = __ldg(f.lsq + i);
     float dx[4], dy[4];
 #pragma unroll
@@ -202,7 +87,7 @@ inner32_point(const Geom &g, const Geom32 &f, const float *__restrict__ dq0,
         dx[m] = dx0[m] + 0.5f * dxi[m] - 0.5f * (L.x * tx[m] + L.y * ty[m]);
         dy[m] = dy0[m] + 0.5f * dyi[m] - 0.5f * (L.y * tx[m] + L.z * ty[m]);
     }
-    stf8(dq_out + 8 * (size_t)i, dx, dy);
+    stf8w(dq_out + 8 * (size_t)i, dx, dy);
 }
 
 __global__ void __launch_bounds__(GRAD_BLOCK)
@@ -345,8 +230,8 @@ kb_grad32_h(Geom g, Consts c, Geom32 f, Sched s, const float4 *__restrict__ q,
             else
                 grad32_sums(c, f, g.n, GlobalRows32{g, f, q, spd, cur.i}, cur.nb,
                             with_delta, cur.i, dx, dy, qmax, qmin, min_delt);
-            stf8(dq + 8 * (size_t)cur.i, dx, dy);
-            stf8(qm + 8 * (size_t)cur.i, qmax, qmin);
+            stf8w(dq + 8 * (size_t)cur.i, dx, dy);
+            stf8w(qm + 8 * (size_t)cur.i, qmax, qmin);
             if (with_delta) delta[cur.i] = min_delt;
         }
         __syncwarp();
@@ -681,12 +566,11 @@ inline int nblk(int n, int b) { return (n + b - 1) / b; }
 
 }  // namespace
 
-size_t grad32_smem_bytes(int block) { return (size_t)block * STAGE32 * UNITS32_D * 16; }
-size_t inner32_smem_bytes(int) { return 0; }
 
 cudaError_t init_kernels32() {
-    return cudaFuncSetAttribute(kb_grad32, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)grad32_smem_bytes(GRAD_BLOCK));
+    // the FP32 halo D pass stays below the default 48 KB of dynamic shared
+    // memory (at most 25 KB); nothing to set
+    return cudaSuccess;
 }
 
 namespace {
@@ -733,14 +617,9 @@ int wave32(int kind, int block, size_t smem, int grid) {
 void launch_grad32(const Geom &g, const Consts &c, const Geom32 &f, const Sched &s,
                    const float4 *q, const double *spd, float *dq, float *qm, double *delta,
                    bool with_delta, int block, int grid, cudaStream_t st) {
-    if (g.hoff) {
-        kb_grad32_h<<<grid > 0 ? grid : halo32_wave(0, g.hc), HALO32_BLOCK, halo32_smem(g.hc),
-                      st>>>(g, c, f, s, q, spd, dq, qm, delta, with_delta ? 1 : 0);
-        return;
-    }
-    const size_t smem = grad32_smem_bytes(block);
-    kb_grad32<<<wave32(0, block, smem, grid), block, smem, st>>>(g, c, f, s, q, spd, dq, qm,
-                                                                 delta, with_delta ? 1 : 0);
+    (void)block;  // the halo kernel's blocks are HALO32_BLOCK threads
+    kb_grad32_h<<<grid > 0 ? grid : halo32_wave(0, g.hc), HALO32_BLOCK, halo32_smem(g.hc), st>>>(
+        g, c, f, s, q, spd, dq, qm, delta, with_delta ? 1 : 0);
 }
 
 void launch_inner32(const Geom &g, const Consts &c, const Geom32 &f, const Sched &s,

@@ -1,8 +1,9 @@
 // FP64 kernels of the LSKUM pseudo-time loop on sm_100a.
 //
 // Per pseudo-time stage (fpi_solver.F90:27-53):
-//   kb_grad   D pass  -- eval_q_derivatives (+ func_delta on the first stage)
-//   kb_inner  I pass  -- eval_q_inner_loop + eval_update_innerloop (ping-pong)
+//   kb_grad_h   D pass  -- eval_q_derivatives (+ func_delta on the first stage)
+//   kb_inner_h  I pass  -- eval_q_inner_loop + eval_update_innerloop, rearranged
+//                          (dq buffers rotate; the D pass's result is kept)
 //   kb_flux   F pass  -- cal_flux_residual + state_update + eval_q_variables of
 //                        the new state (+ res_sqr partials on the last stage)
 // and per iteration kb_residual (fpi_solver.F90:57-70).
@@ -28,7 +29,7 @@ namespace lskum {
 
 namespace {
 
-constexpr int GRAD_BLOCK = 256;
+constexpr int GRAD_BLOCK = 256;  // blocks of the per-point set-up kernels
 constexpr int LPP = 8;                   // lanes per point in the flux pass
 constexpr int FLUX_BLOCK = 128;          // four independent warps
 constexpr int REC = 19;                  // dGxp[4] dGxn[4] dGyp[4] dGyn[4] dels deln w
@@ -38,19 +39,11 @@ constexpr int REC = 19;                  // dGxp[4] dGxn[4] dGyp[4] dGyn[4] dels
 constexpr double OBT = 1.0 / 3.0;        // state_update.F90:19-20
 constexpr double TBT = 2.0 / 3.0;
 
-__device__ __forceinline__ void st8(double *p, const double a[4], const double b[4]) {
-    double2 *v = reinterpret_cast<double2 *>(p);
-    v[0] = make_double2(a[0], a[1]);
-    v[1] = make_double2(a[2], a[3]);
-    v[2] = make_double2(b[0], b[1]);
-    v[3] = make_double2(b[2], b[3]);
-}
-
-// Rows in 256-bit read-only loads (ld.global.nc.v4.f64, sm_100) for the
-// thread-per-point gathers of the D and I passes: a 32-byte q row in one
-// load, a 64-byte dq row in two.  R4 rows and dq rows are 32-byte aligned.
-// The flux pass uses them for its 64-byte dq and qm rows only: its 32-byte
-// q rows in the wide form made it spill at its 96-register cap.
+// Rows in 256-bit read-only loads (ld.global.nc.v4.f64, sm_100): a 32-byte
+// q row in one load, a 64-byte dq row in two (the D and I passes' rows of
+// tiles without a staged halo, the I pass's dq0 row).  R4 rows and dq rows
+// are 32-byte aligned.  The flux pass uses them for its 64-byte dq and qm
+// rows only: its 32-byte q rows in the wide form made it spill.
 __device__ __forceinline__ R4 ld4w(const R4 *p) {
     R4 r;
     asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
@@ -64,129 +57,6 @@ __device__ __forceinline__ void ld8w(const double *p, double a[4], double b[4]) 
     const R4 v = ld4w(reinterpret_cast<const R4 *>(p + 4));
     a[0] = u.a; a[1] = u.b; a[2] = u.c; a[3] = u.d;
     b[0] = v.a; b[1] = v.b; b[2] = v.c; b[3] = v.d;
-}
-
-// ---------------------------------------------------------------------------
-// Staged neighbour gathers of the D and I passes.
-//
-// A thread owns one point.  Its stencil is read in rounds of STAGE slots:
-// the round's conn entries are loaded first (independent, coalesced loads),
-// then every neighbour row the round needs is copied into the thread's own
-// shared-memory slots with cp.async (16-byte asynchronous copies that hold no
-// registers while in flight), and one wait covers them all.  The per-point
-// sums then run in slot order -- the reference's loop order -- from shared
-// memory.  The serial chain of the plain loop (conn -> row -> sums, once per
-// neighbour) becomes one chain per round, with every row of the round in
-// flight at once.  Shared memory is laid out thread-minor
-// (sb[pair * blockDim + thread], a pair = 16 bytes) so the copies and the
-// reads of a warp hit distinct banks.  Each thread reads only what it
-// copied, so no block barrier is needed.
-#ifndef STAGE_D
-#define STAGE_D 4  // slots per round, D pass (4: 0.099 ms per C2 launch, 8: 0.107)
-#endif
-constexpr int PAIRS_D = 4;  // q[0..1], q[2..3], (x, y), (spd, -)
-
-__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
-    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
-    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
-}
-// Waits for every cp.async this thread issued.
-__device__ __forceinline__ void cp_async_wait_all() {
-    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-}
-
-// q_variables.F90:41-112 eval_q_derivatives, and state_update.F90:190-236
-// func_delta (spd[k] = |u_k| + 3 sqrt(p_k/rho_k) of the neighbour's state).
-__device__ __forceinline__ void
-grad_point(const Geom &g, const Consts &c, const R4 *__restrict__ q, const double *__restrict__ spd,
-           double *__restrict__ dq, double *__restrict__ qm, double *__restrict__ delta,
-           int with_delta, int i, double2 *sb) {
-    const int T = blockDim.x;
-    const int nb = g.nbhs[i];
-    double2 pi_ = g.xy[i];
-    R4 qv = ld4w(q + i);
-    double qi[4] = {qv.a, qv.b, qv.c, qv.d};
-    double qmax[4] = {qi[0], qi[1], qi[2], qi[3]};
-    double qmin[4] = {qi[0], qi[1], qi[2], qi[3]};
-    double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0;
-    double sdxq[4] = {0.0, 0.0, 0.0, 0.0}, sdyq[4] = {0.0, 0.0, 0.0, 0.0};
-    double min_delt = 1.0;
-    for (int r0 = 0; r0 < nb; r0 += STAGE_D) {
-        const int m = min(STAGE_D, nb - r0);
-        int kk[STAGE_D];
-#pragma unroll
-        for (int t = 0; t < STAGE_D; ++t) kk[t] = t < m ? __ldg(g.conn + (r0 + t) * g.n + i) : 0;
-#pragma unroll
-        for (int t = 0; t < STAGE_D; ++t) {
-            if (t < m) {
-                double2 *d = sb + t * PAIRS_D * T;
-                const double2 *row = reinterpret_cast<const double2 *>(q + kk[t]);
-                cp_async16(d, row);
-                cp_async16(d + T, row + 1);
-                cp_async16(d + 2 * T, g.xy + kk[t]);
-                if (with_delta) cp_async8(d + 3 * T, spd + kk[t]);
-            }
-        }
-        cp_async_wait_all();
-        for (int t = 0; t < m; ++t) {
-            const double2 *d = sb + t * PAIRS_D * T;
-            const double2 a = d[0], b = d[T], pk = d[2 * T];
-            double qk[4] = {a.x, a.y, b.x, b.y};
-#pragma unroll
-            for (int mm = 0; mm < 4; ++mm) {
-                if (qk[mm] > qmax[mm]) qmax[mm] = qk[mm];
-                if (qk[mm] < qmin[mm]) qmin[mm] = qk[mm];
-            }
-            double delx = pk.x - pi_.x, dely = pk.y - pi_.y;
-            double dist = sqrt(delx * delx + dely * dely);
-            double w = c.power_zero ? 1.0 : pow(dist, c.power);
-            sdx2 = sdx2 + delx * delx * w;
-            sdy2 = sdy2 + dely * dely * w;
-            sdxy = sdxy + delx * dely * w;
-#pragma unroll
-            for (int mm = 0; mm < 4; ++mm) {
-                sdxq[mm] = sdxq[mm] + w * delx * (qk[mm] - qi[mm]);
-                sdyq[mm] = sdyq[mm] + w * dely * (qk[mm] - qi[mm]);
-            }
-            if (with_delta) {
-                double delta_t = dist / d[3 * T].x;
-                delta_t = c.cfl * delta_t;
-                if (min_delt > delta_t) min_delt = delta_t;
-            }
-        }
-    }
-    double det = sdx2 * sdy2 - sdxy * sdxy;
-    double one_by_det = 1.0 / det;
-    double dx[4], dy[4];
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-        dx[m] = (sdxq[m] * sdy2 - sdyq[m] * sdxy) * one_by_det;
-        dy[m] = (sdyq[m] * sdx2 - sdxq[m] * sdxy) * one_by_det;
-    }
-    st8(dq + 8 * (size_t)i, dx, dy);
-    st8(qm + 8 * (size_t)i, qmax, qmin);
-    if (with_delta) delta[i] = min_delt;
-}
-
-// D pass: grid-stride over the points of the scheduled instances (a single
-// grid is the one-instance case).  Dynamic shared memory: grad_smem_bytes.
-__global__ void __launch_bounds__(GRAD_BLOCK)
-kb_grad(Geom g, Consts c, Sched s, const R4 *__restrict__ q, const double *__restrict__ spd,
-        double *__restrict__ dq, double *__restrict__ qm, double *__restrict__ delta,
-        int with_delta) {
-    extern __shared__ double2 sbd[];
-    __shared__ SchedSmem ss;
-    load_sched(s, ss);
-    const int total = ss.pre[ss.nact] * TILE;
-    for (int vp = blockIdx.x * blockDim.x + threadIdx.x; vp < total;
-         vp += gridDim.x * blockDim.x) {
-        const int i = sched_point(s, ss, vp);
-        if (i >= 0) grad_point(g, c, q, spd, dq, qm, delta, with_delta, i, sbd + threadIdx.x);
-    }
 }
 
 // Row sources of the per-point sums of the D and I passes: the rows of a
@@ -353,25 +223,6 @@ __device__ __forceinline__ void inner_sums(const Consts &c, const Rows &R, int n
         const double Ly = one_by_det * (sB[m] * sdx2 - sA[m] * sdxy);
         dx[m] = (dq0x[m] + 0.5 * dxi[m]) - 0.5 * Lx;
         dy[m] = (dq0y[m] + 0.5 * dyi[m]) - 0.5 * Ly;
-    }
-}
-
-// I pass without tile halos: a thread per point with its neighbour rows in
-// 256-bit loads.
-__global__ void __launch_bounds__(GRAD_BLOCK)
-kb_inner(Geom g, Consts c, Sched s, const double *__restrict__ dq0,
-         const double *__restrict__ dq_in, double *__restrict__ dq_out) {
-    __shared__ SchedSmem ss;
-    load_sched(s, ss);
-    const int total = ss.pre[ss.nact] * TILE;
-    for (int vp = blockIdx.x * blockDim.x + threadIdx.x; vp < total;
-         vp += gridDim.x * blockDim.x) {
-        const int i = sched_point(s, ss, vp);
-        if (i < 0) continue;
-        double ax[4], ay[4], dx[4], dy[4];
-        ld8w(dq0 + 8 * (size_t)i, ax, ay);
-        inner_sums(c, GlobalRows{g, nullptr, dq_in, nullptr, i}, g.nbhs[i], ax, ay, dx, dy);
-        st8(dq_out + 8 * (size_t)i, dx, dy);
     }
 }
 
@@ -1019,19 +870,14 @@ int flux_blocks(int n) { return nblk(n, TILE); }
 // blocks that give every warp of the flux pass one chunk of two tiles
 int flux_grid_blocks(int n) { return nblk(nblk(n, TILE), 2 * FLUX_WARPS); }
 
-size_t grad_smem_bytes(int block) { return (size_t)block * STAGE_D * PAIRS_D * sizeof(double2); }
-size_t inner_smem_bytes(int) { return 0; }
 // staging memory of a block of the halo kernels: two tiles a warp
 size_t halo_smem_bytes(int kind, int hc) {
     return halo_bytes(HALO_BLOCK / 32, kind == 0 ? HA_D : HA_I, hc);
 }
 
 cudaError_t init_kernels() {
-    cudaError_t e = cudaFuncSetAttribute(kb_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)grad_smem_bytes(GRAD_BLOCK));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(kb_grad_h, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)halo_smem_bytes(0, HALO_CAP + 1));
+    cudaError_t e = cudaFuncSetAttribute(kb_grad_h, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)halo_smem_bytes(0, HALO_CAP + 1));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(kb_inner_h, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)halo_smem_bytes(1, HALO_CAP + 1));
@@ -1039,9 +885,9 @@ cudaError_t init_kernels() {
 }
 
 int wave_blocks(int dev, int kind, int block, size_t smem, bool fp32) {
-    // the D and I passes size their staging buffers by the block
-    if (kind == 0) smem = fp32 ? grad32_smem_bytes(block) : grad_smem_bytes(block);
-    if (kind == 1) smem = fp32 ? inner32_smem_bytes(block) : inner_smem_bytes(block);
+    // the D and I passes: their own staging memory (the halo kernels' at the
+    // largest stride; the FP32 I pass none)
+    if (kind == 0 || kind == 1) smem = 0;
     int sms = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     return std::max(sms, 1) * std::max(1, batch_occupancy(kind, fp32, block, smem));
@@ -1091,24 +937,16 @@ int halo_wave(int kind, int hc) {
 void launch_grad(const Geom &g, const Consts &c, const Sched &s, const R4 *q, const double *spd,
                  double *dq, double *qm, double *delta, bool with_delta, int block, int grid,
                  cudaStream_t st) {
-    if (g.hoff) {
-        kb_grad_h<<<grid > 0 ? grid : halo_wave(0, g.hc), HALO_BLOCK, halo_smem_bytes(0, g.hc),
-                    st>>>(g, c, s, q, spd, dq, qm, delta, with_delta ? 1 : 0);
-        return;
-    }
-    const size_t smem = grad_smem_bytes(block);
-    kb_grad<<<wave(0, block, smem, grid), block, smem, st>>>(g, c, s, q, spd, dq, qm, delta,
-                                                             with_delta ? 1 : 0);
+    (void)block;  // the halo kernels' blocks are HALO_BLOCK threads
+    kb_grad_h<<<grid > 0 ? grid : halo_wave(0, g.hc), HALO_BLOCK, halo_smem_bytes(0, g.hc), st>>>(
+        g, c, s, q, spd, dq, qm, delta, with_delta ? 1 : 0);
 }
 
 void launch_inner(const Geom &g, const Consts &c, const Sched &s, const double *dq0,
                   const double *dq_in, double *dq_out, int block, int grid, cudaStream_t st) {
-    if (g.hoff) {
-        kb_inner_h<<<grid > 0 ? grid : halo_wave(1, g.hc), HALO_BLOCK, halo_smem_bytes(1, g.hc),
-                     st>>>(g, c, s, dq0, dq_in, dq_out);
-        return;
-    }
-    kb_inner<<<wave(1, block, 0, grid), block, 0, st>>>(g, c, s, dq0, dq_in, dq_out);
+    (void)block;
+    kb_inner_h<<<grid > 0 ? grid : halo_wave(1, g.hc), HALO_BLOCK, halo_smem_bytes(1, g.hc), st>>>(
+        g, c, s, dq0, dq_in, dq_out);
 }
 
 void launch_flux(const Geom &g, const Consts &c, const Sched &s, const StageBufs &b, int rk,
