@@ -321,8 +321,8 @@ void lskum_host::build_halo(int n, int kp, const int *conn, const int *nbhs,
     out.off[ntile] = (int)out.rows.size();
     // the staging stride: one more than a multiple of eight rows, so that a
     // row's 16-byte pieces in consecutive arrays fall on different banks
-    // (C2 I pass: 0.091 ms; 0.109 with no padding, 0.097 / 0.101 at two /
-    // four more than a multiple of eight)
+    // (C2 I pass: 0.091 ms; 0.109 with no padding, 0.097 - 0.101 at two to
+    // seven more than a multiple of eight)
     if (out.hc > 0) out.hc += (9 - out.hc % 8) % 8;
 }
 
