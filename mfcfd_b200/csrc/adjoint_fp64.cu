@@ -42,6 +42,14 @@ __device__ __forceinline__ void ld8a(const double *p, double a[4], double b[4]) 
     b[0] = t2.x; b[1] = t2.y; b[2] = t3.x; b[3] = t3.y;
 }
 
+// Four doubles in one 256-bit read-only load (ld.global.nc.v4.f64, sm_100);
+// p is 32-byte aligned and not written by the kernel that reads it.
+__device__ __forceinline__ void ld4nc(const double *p, double v[4]) {
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+        : "l"(p));
+}
+
 __device__ __forceinline__ void kst_store(double *e, const KState &s) {
     e[0] = s.rho; e[1] = s.ut; e[2] = s.un; e[3] = s.pbr; e[4] = s.usq;
     e[5] = s.B1; e[6] = s.B2; e[7] = s.e1; e[8] = s.e2;
@@ -227,15 +235,11 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
             KState si, sk;
             if (kst) {
                 // the forward re-run taped both reconstructions of this slot
-                const double2 *tp =
-                    reinterpret_cast<const double2 *>(kst + ((size_t)i * g.kp + r) * KS_TAPE);
+                // (128 contiguous bytes, in four 256-bit loads)
+                const double *tp = kst + ((size_t)i * g.kp + r) * KS_TAPE;
                 double v[KS_TAPE];
 #pragma unroll
-                for (int hh = 0; hh < KS_TAPE / 2; ++hh) {
-                    const double2 t2 = __ldg(tp + hh);
-                    v[2 * hh] = t2.x;
-                    v[2 * hh + 1] = t2.y;
-                }
+                for (int hh = 0; hh < KS_TAPE / 4; ++hh) ld4nc(tp + 4 * hh, v + 4 * hh);
                 si = kst_taped(v, nx, ny);
                 sk = kst_taped(v + 8, nx, ny);
                 e_[0] = v[6]; e_[1] = v[7]; e_[2] = si.rho; e_[3] = si.rho * si.pbr;
@@ -298,8 +302,12 @@ k_flux_b(Geom g, Consts c, const R4 *__restrict__ q_in, const double *__restrict
     double sdx2 = 0.0, sdy2 = 0.0, sdxy = 0.0, fx[2] = {0.0, 0.0}, fy[2] = {0.0, 0.0};
     double obd = 0.0;
     if (used) {
-        for (int r = 0; r < nb; ++r) {
-            if (!((lbits >> r) & 1ull)) continue;
+        // the list's slots in slot order (lowest bit first): a lane loops
+        // over its own members only (nb <= 20)
+        unsigned rb = (unsigned)lbits & ((1u << nb) - 1u);
+        while (rb) {
+            const int r = __ffs(rb) - 1;
+            rb &= rb - 1u;
             const double *e = rec + r * BREC;
             const double dels = e[16], deln = e[17];
             sdx2 = sdx2 + dels * dels;
