@@ -9,7 +9,8 @@ share, so that staged and unstaged tiles meet in the same warps -- and check
 the CUDA path against the oracle on the same shuffled grid (FP64: 1e-10
 relative in prim, residue history 1e-9 absolute), the FP32-mixed path
 against the FP64 path, and batches holding shuffled and ring-ordered
-instances against single runs bit for bit.
+instances against single runs bit for bit; and stencils of up to 20 slots
+(a point's local row bytes in three 8-byte words) against the oracle.
 """
 import numpy as np
 import pytest
@@ -72,8 +73,31 @@ def base_grid():
     return naca_ogrid(64, 24, seed=5, first_spacing=5e-3)
 
 
+def wide_stencil_grid():
+    """An O-grid whose 40 seeded interior points take their nearest other
+    points up to 18-20 stencil slots: local row bytes in three words."""
+    g = naca_ogrid(48, 16, seed=3, first_spacing=5e-3)
+    rng = np.random.default_rng(0)
+    for p in rng.choice(np.where(g.flag_1 == INTERIOR)[0], 40, replace=False):
+        have = set((g.conn[: g.nbhs[p], p] - 1).tolist()) | {int(p)}
+        want = 18 + int(rng.integers(0, 3))
+        for k in np.argsort(np.hypot(g.x - g.x[p], g.y - g.y[p])):
+            if g.nbhs[p] >= want:
+                break
+            if int(k) not in have:
+                g.conn[g.nbhs[p], p] = k + 1
+                g.nbhs[p] += 1
+                have.add(int(k))
+    return g
+
+
 def test_ring_order_stages_every_tile():
     assert unstaged_share(base_grid()) == 0.0
+
+
+def test_wide_stencils_reach_twenty_slots():
+    g = wide_stencil_grid()
+    assert g.nbhs.max() == 20 and int((g.nbhs >= 16).sum()) == 40
 
 
 def test_shuffled_orders_give_unstaged_tiles():
@@ -92,6 +116,20 @@ def test_unstaged_tiles_match_the_oracle(gpu, frac):
     with Solver(g, **FLOW) as s:
         res = s.run(6)
         assert max_rel(s.get_state(), o.prim()) < 1e-10
+    o.close()
+    assert np.allclose(res, res_ref, rtol=0, atol=1e-9)
+
+
+@pytest.mark.gpu
+def test_wide_stencils_match_the_oracle(gpu):
+    g = wide_stencil_grid()
+    o = oracle.Oracle(g, **FLOW)
+    res_ref = o.run(6)
+    with Solver(g, **FLOW) as s, Solver(g, precision="fp32_mixed", **FLOW) as s32:
+        res = s.run(6)
+        s32.run(6)
+        assert max_rel(s.get_state(), o.prim()) < 1e-10
+        assert max_rel(s32.get_state(), s.get_state()) < 1e-3
     o.close()
     assert np.allclose(res, res_ref, rtol=0, atol=1e-9)
 
