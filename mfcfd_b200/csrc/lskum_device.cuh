@@ -163,9 +163,9 @@ __device__ __forceinline__ KStateT<T> kstate(T u1, T u2, T rho, T pr, T nx, T ny
 // erf(x) given exp(-x*x).  FP64: the library erf.  FP32: Abramowitz &
 // Stegun 7.1.26 (after Hastings), erf(|x|) = 1 - t (a1 + t (a2 + t (a3 + t
 // (a4 + t a5)))) exp(-x^2), t = 1 / (1 + p |x|), absolute error below
-// 1.5e-7 -- the split fluxes use erf only in 1 +- erf, so the absolute error
-// is what counts -- reusing the exponential the Maxwellian moments take
-// anyway (C2: FP32 flux pass 0.316 -> 0.304 ms; |dCl| against the FP64
+// 1.5e-7 (5.3e-7 evaluated in FP32; tests/test_erf32.py) -- the split
+// fluxes use erf only in 1 +- erf, so the absolute error is what counts --
+// reusing the exponential the Maxwellian moments take anyway (C2: FP32 flux pass 0.316 -> 0.304 ms; |dCl| against the FP64
 // loop after 50 iterations 1.0e-7 with the library erff, 6e-9 with this).
 template <class T>
 __device__ __forceinline__ T erf_with_exp(T x, T) {
